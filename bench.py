@@ -1,0 +1,414 @@
+"""Benchmark: ABMC-ICCG to relative residual 1e-8 on one B200.
+
+Workload (one step = one full solve of one system):
+  3D 7-point Laplacian, 128^3 grid (n = 2,097,152, nnz = 14,581,760),
+  coefficients 1, 1, 0.01; ABMC with block size 16 (breadth-first blocks,
+  greedy block coloring), b = A x*, x* ~ U(-1,1) from splitmix64(0); x0 = 0;
+  IC(0) preconditioner; A and L stored in FP32, x / r / p / z and all inner
+  products in FP64, FP64 residual replacement every 50 iterations; converged
+  when the FP64 true relative residual is below 1e-8.
+
+Prints ONE JSON line (rank 0).  `value` is the device time per solve
+(CUDA events around the timed steps, max over ranks); `e2e` repeats the
+measurement through the C ABI with host (pinned) buffers, copies included.
+`--impl reference` times the reference's own OpenMP CPU code (compiled from
+its sources into oracle/_ref) on the same problem.
+
+Multi-GPU: one process per GPU (torchrun); each rank solves its own replica
+of the system (independent solves, no data-path collective: weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SIDE = 128
+BLOCK = 16
+TOL = 1e-8
+RR = 50
+METRIC = "ICCG ms to resid 1e-8 (ABMC B=16, 3D 7-pt 128^3 aniso, FP32 storage / FP64 recurrences)"
+WORKLOAD = "abmc_iccg_laplace3d_aniso_128"
+
+
+def _env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = max(mx, float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_problem():
+    import iccg_b200.problems as pb
+    t0 = time.perf_counter()
+    P = pb.config_abmc_aniso(SIDE, BLOCK, "bfs", seed=0)
+    return P, time.perf_counter() - t0
+
+
+def bytes_model(P, storage_bytes: int):
+    """Algorithmic bytes (compulsory traffic) of the kernels of one PCG iteration."""
+    n = P.A_run.n
+    nnz = P.A_run.nnz
+    nnzS = (nnz - n) // 2                   # strict lower (= strict upper) entries of L
+    sv = storage_bytes
+    S_A = nnz * (sv + 4) + 4 * (n + 1)
+    S_L = nnzS * (sv + 4) + 4 * (n + 1) + sv * n   # strict part + row pointers + diagonal
+    return {
+        "spmv": S_A + 16 * n,                 # A, p gathered (compulsory once), Ap written
+        "fwd_sweep": S_L + 16 * n,            # r read, y written
+        "bwd_sweep": S_L + 24 * n,            # y read, z written, r read for r.z
+        "iteration": S_A + 2 * S_L + 16 * 8 * n,
+    }
+
+
+def run_gpu(args):
+    import torch
+    import iccg_b200 as ib
+
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    local = _env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    P, setup_s = build_problem()
+    n = P.A_run.n
+    ctx = ib.Context(local)
+    t0 = time.perf_counter()
+    ctx.upload(P.A_run)
+    ctx.set_schedule(P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    factor_s = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    dev = torch.device("cuda", local)
+    b_d = torch.from_numpy(P.b_run).to(dev)
+    x_d = torch.zeros(n, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+
+    def solve(storage, mode=ib.MODE_FUSED):
+        with torch.cuda.stream(stream):
+            x_d.zero_()
+        return ctx.solve_dev(b_d.data_ptr(), x_d.data_ptr(), 10000, TOL, mode=mode, storage=storage, rr_interval=RR)
+
+    # FP64 reference solution on the device (for the error report)
+    r64 = solve(ib.STORE_FP64)
+    x64 = x_d.cpu().numpy().copy()
+    for _ in range(args.warmup):
+        solve(ib.STORE_FP32)
+    # timed region
+    clocks = ClockSampler(local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = ctx.launches
+    results = []
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+    for _ in range(args.steps):
+        results.append(solve(ib.STORE_FP32))
+    with torch.cuda.stream(stream):
+        e1.record(stream)
+    torch.cuda.synchronize()
+    launches = ctx.launches - launches0
+    clk = clocks.stop()
+    if dist:
+        dist.barrier()
+    total_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per = total_ms / args.steps
+    r32 = results[-1]
+    x32 = x_d.cpu().numpy()
+    err = float(np.linalg.norm(x32 - x64) / np.linalg.norm(x64))
+    per_solve = [r.solve_ms for r in results]
+
+    # plain FP64 path (one kernel per reference op, host-checked) and fused FP64, untimed by the contract
+    plain = solve(ib.STORE_FP64, ib.MODE_PLAIN)
+    fused64 = solve(ib.STORE_FP64, ib.MODE_FUSED)
+
+    # per-kernel device time: one more solve with every launch bracketed by
+    # CUDA events on the context's stream
+    ctx.profile(True)
+    rp = solve(ib.STORE_FP32)
+    prof = {}
+    names = {0: "spmv", 1: "fwd_sweep", 2: "bwd_sweep", 3: "vector", 4: "residual"}
+    for cls, nm in names.items():
+        msum, cnt = ctx.profile_read(cls)
+        prof[nm] = (msum, cnt)
+    ctx.profile(False)
+    iters = rp.iters
+    bm = bytes_model(P, 4)
+    peak, peak_kind = _peaks()
+    kernels = {}
+    for nm, key in (("spmv", "spmv"), ("fwd_sweep", "fwd_sweep"), ("bwd_sweep", "bwd_sweep")):
+        msum, cnt = prof[nm]
+        if nm == "spmv":
+            per_launch_ms = msum / max(cnt, 1)
+            units = "launch"
+        else:
+            per_launch_ms = msum / max(iters + 1, 1)   # one sweep = nc color launches
+            units = "sweep"
+        gbs = bm[key] / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else 0.0
+        kernels[nm] = {"ms": round(per_launch_ms, 5), "per": units, "bytes": bm[key], "GB/s": round(gbs, 1),
+                       "frac": round(gbs / peak, 4), "launches": cnt}
+    kernels["vector"] = {"ms_total": round(prof["vector"][0], 4), "launches": prof["vector"][1]}
+    kernels["residual_replacement"] = {"ms_total": round(prof["residual"][0], 4), "launches": prof["residual"][1]}
+    dom = kernels["spmv"]
+    traffic = _traffic_from_profiles()
+
+    # e2e: through the C ABI with host (pinned) buffers, H2D of b and x0 and D2H of x inside the timed region
+    pin_b = torch.from_numpy(P.b_run).pin_memory()
+    pin_x = torch.zeros(n, dtype=torch.float64).pin_memory()
+    xb = pin_x.numpy()
+    e2e = []
+    for _ in range(max(1, min(args.steps, 5))):
+        xb[:] = 0.0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.solve(pin_b.numpy(), xb, 10000, TOL, storage=ib.STORE_FP32, rr_interval=RR)
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = statistics.median(e2e)
+    if dist:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(P, samples=args.cpu_samples)
+
+    line = {
+        "metric": METRIC,
+        "value": round(ms_per, 4),
+        "unit": "ms",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_per, 4),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "storage": "fp32 A and L, fp64 vectors and reductions",
+        "data": "synthetic",
+        "config": {
+            "workload": WORKLOAD, "n": n, "nnz": P.A_run.nnz, "grid": f"{SIDE}^3", "coeffs": [1, 1, 0.01],
+            "block_size": BLOCK, "blocking": "bfs", "nb": P.nb, "colors": P.nc, "tol": TOL, "rr_interval": RR,
+            "x0": "zeros", "rhs": "b = A x*, x* ~ U(-1,1) splitmix64(0)",
+            "l2": "inputs larger than L2: ~0.5 GB streamed per iteration vs 126 MB L2",
+            "parallelism": f"replicas x{world}",
+        },
+        "solves_per_s": round(world * 1000.0 / ms_per, 3),
+        "iters": r32.iters,
+        "true_rel_resid": r32.true_rel_resid,
+        "residual_replacements": r32.n_replacements,
+        "err_vs_fp64_solution": err,
+        "per_solve_ms": {"p50": round(statistics.median(per_solve), 4), "max": round(max(per_solve), 4)},
+        "fp64": {"fused_ms": round(fused64.solve_ms, 4), "fused_iters": fused64.iters,
+                 "plain_ms": round(plain.solve_ms, 4), "plain_iters": plain.iters,
+                 "true_rel_resid": r64.true_rel_resid},
+        "speedup_vs_plain_fp64": round(plain.solve_ms / ms_per, 3),
+        "speedup_vs_fused_fp64": round(fused64.solve_ms / ms_per, 3),
+        "roofline": {"bound": "hbm", "kernel": "spmv (FP32 values, FP64 x)", "achieved": dom["GB/s"],
+                     "peak": peak, "unit": "GB/s", "frac": dom["frac"], "peak_source": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes": dom["bytes"]},
+        "kernels": kernels,
+        "iteration_bytes": bm["iteration"],
+        "iteration_GBps": round(bm["iteration"] * iters / (rp.solve_ms * 1e-3) / 1e9, 1) if rp.solve_ms else None,
+        "gpu_launches": int(launches),
+        "e2e": {"value": round(e2e_ms, 4), "unit": "ms", "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 8 * n},
+        "setup_s": {"host": round(setup_s, 3), "upload_and_device_ic0": round(factor_s, 3)},
+        "clocks": clk,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def _traffic_from_profiles():
+    """DRAM bytes per SpMV launch from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "ncu_spmv_abmc128.txt"
+    if not p.exists():
+        return None
+    for ln in p.read_text().splitlines():
+        if ln.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(ln.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_baseline(P, samples=3):
+    """The reference's OpenMP CG (compiled from its sources) on the same
+    problem, all host cores; or the oracle port on one core if the compiled
+    reference is absent."""
+    from oracle import bindings as ob
+    n = P.A.n
+    if ob.ref() is not None:
+        cores = os.cpu_count() or 1
+        ob.ref().ref_set_threads(cores)
+        R = ob.RefProblem(4, n, P.A.rowptr, P.A.colind, P.A.val, P.block_of_old, P.nb, P.block_color, P.nc)
+        times, iters = [], 0
+        for _ in range(samples):
+            x, it, rel, cv, us = R.cg(P.b_run, np.zeros(n), 10000, TOL)
+            times.append(us / 1e3)
+            iters = it
+        return {"value": round(statistics.median(times), 3), "unit": "ms", "cores": cores, "kind": "reference",
+                "sample": f"{samples} full ABMC-ICCG solves of the same 128^3 system (median), {iters} iterations, "
+                          f"conjugate_gradient only (cg_crs.cpp:507-510)"}
+    rp, ci, v = P.A_run.rowptr, P.A_run.colind, P.A_run.val
+    ic0 = ob.OracleIC0(n, rp, ci, v, 0.0)
+    t0 = time.perf_counter()
+    x, it, rel, cv, _ = ob.cg(n, rp, ci, v, P.b_run, np.zeros(n), 2, 10000, TOL, ic0, P.sched)
+    ms = (time.perf_counter() - t0) * 1e3
+    return {"value": round(ms, 3), "unit": "ms", "cores": 1, "kind": "port",
+            "sample": f"1 full solve by the C restatement ({it} iterations)"}
+
+
+def run_reference(args):
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    if rank != 0:
+        return
+    from oracle import bindings as ob
+    if ob.ref() is None:
+        print(json.dumps({"impl": "reference", "unavailable": "compiled reference (oracle/_ref) not present"}))
+        return
+    P, _ = build_problem()
+    n = P.A.n
+    cores = os.cpu_count() or 1
+    ob.ref().ref_set_threads(cores)
+    R = ob.RefProblem(4, n, P.A.rowptr, P.A.colind, P.A.val, P.block_of_old, P.nb, P.block_color, P.nc)
+    for _ in range(args.warmup):
+        R.cg(P.b_run, np.zeros(n), 10000, TOL)
+    times, iters, rel = [], 0, 0.0
+    for _ in range(args.steps):
+        x, it, rel, cv, us = R.cg(P.b_run, np.zeros(n), 10000, TOL)
+        times.append(us / 1e3)
+        iters = it
+    ms = statistics.mean(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": n, "nnz": P.A.nnz, "block_size": BLOCK, "tol": TOL,
+                   "parallelism": f"OpenMP x{cores} host threads"},
+        "iters": iters, "rel_resid": rel,
+        "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": cores, "kind": "reference",
+                         "sample": f"{args.steps} full solves (mean), conjugate_gradient only"},
+        "e2e": {"value": round(ms, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="iccg_b200", choices=["iccg_b200", "reference"])
+    ap.add_argument("--cpu-samples", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

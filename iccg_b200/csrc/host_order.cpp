@@ -1,0 +1,521 @@
+// host_order.cpp -- file formats, permutations, P^T A P and schedules.
+//
+// New implementations (counting sorts, flat buckets) that reproduce the
+// reference's results bit for bit; each function cites the reference
+// routine whose output it must equal.
+#include <algorithm>
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <numeric>
+#include <sstream>
+
+#include "host.hpp"
+#include "../../include/iccg.h"
+
+namespace iccg {
+
+namespace {
+
+// whole-file reader
+std::string slurp(const std::string& path)
+{
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) throw Error(ICCG_ERR_IO, "Failed to open: " + path);
+    std::string s;
+    std::fseek(f, 0, SEEK_END);
+    long sz = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    if (sz > 0) {
+        s.resize((size_t)sz);
+        size_t got = std::fread(&s[0], 1, (size_t)sz, f);
+        s.resize(got);
+    }
+    std::fclose(f);
+    return s;
+}
+
+inline bool is_ws(char c) { return c == ' ' || c == '\t' || c == '\r' || c == '\v' || c == '\f'; }
+
+// Sequential line cursor over a buffer (getline semantics: the last line may
+// lack a newline; a trailing newline does not produce an extra empty line).
+struct Lines {
+    const char* p;
+    const char* end;
+    bool next(const char*& b, const char*& e)
+    {
+        if (p >= end) return false;
+        b = p;
+        const char* nl = (const char*)std::memchr(p, '\n', (size_t)(end - p));
+        e = nl ? nl : end;
+        p = nl ? nl + 1 : end;
+        return true;
+    }
+};
+
+// token reader within [p, e)
+bool next_token(const char*& p, const char* e, std::string& tok)
+{
+    while (p < e && is_ws(*p)) ++p;
+    if (p >= e) return false;
+    const char* s = p;
+    while (p < e && !is_ws(*p)) ++p;
+    tok.assign(s, p);
+    return true;
+}
+
+bool parse_ll(const char*& p, const char* e, long long& v)
+{
+    while (p < e && is_ws(*p)) ++p;
+    if (p >= e) return false;
+    char buf[64];
+    size_t len = 0;
+    while (p + len < e && !is_ws(p[len]) && len < 63) { buf[len] = p[len]; ++len; }
+    buf[len] = 0;
+    char* q;
+    errno = 0;
+    v = std::strtoll(buf, &q, 10);
+    if (q == buf) return false;
+    p += (q - buf);
+    return true;
+}
+
+bool parse_double(const char*& p, const char* e, double& v)
+{
+    while (p < e && is_ws(*p)) ++p;
+    if (p >= e) return false;
+    char buf[128];
+    size_t len = 0;
+    while (p + len < e && !is_ws(p[len]) && len < 127) { buf[len] = p[len]; ++len; }
+    buf[len] = 0;
+    char* q;
+    v = std::strtod(buf, &q);
+    if (q == buf) return false;
+    p += (q - buf);
+    return true;
+}
+
+std::string lower(std::string s)
+{
+    for (auto& c : s) c = (char)std::tolower((unsigned char)c);
+    return s;
+}
+
+}  // namespace
+
+// read_matrix_market_crs (crs_io.cpp:73-159) with coo_to_crs (crs_io.cpp:19-70).
+// Same accepted formats and error cases; parsing is a single pass over the
+// file in memory.  Duplicate entries are summed in file order.
+CRS read_matrix_market_crs(const std::string& path)
+{
+    std::string buf = slurp(path);
+    Lines L{buf.data(), buf.data() + buf.size()};
+    const char *b, *e;
+    if (!L.next(b, e)) throw Error(ICCG_ERR_IO, "Empty file");
+    std::string banner, mtx, storage, field, symmetry;
+    {
+        const char* p = b;
+        if (!(next_token(p, e, banner) && next_token(p, e, mtx) && next_token(p, e, storage) &&
+              next_token(p, e, field) && next_token(p, e, symmetry)))
+            throw Error(ICCG_ERR_IO, "Invalid MatrixMarket header");
+        if (banner != "%%MatrixMarket") throw Error(ICCG_ERR_IO, "Not a MatrixMarket file");
+        mtx = lower(mtx); storage = lower(storage); field = lower(field); symmetry = lower(symmetry);
+        if (mtx != "matrix" || storage != "coordinate")
+            throw Error(ICCG_ERR_IO, "Only 'matrix coordinate' is supported");
+        if (!(field == "real" || field == "integer" || field == "pattern"))
+            throw Error(ICCG_ERR_IO, "Unsupported field: " + field);
+        if (!(symmetry == "general" || symmetry == "symmetric"))
+            throw Error(ICCG_ERR_IO, "Unsupported symmetry: " + symmetry);
+    }
+    // skip comment lines, then the size line
+    bool got = false;
+    while (L.next(b, e)) {
+        if (e > b && *b == '%') continue;
+        got = true;
+        break;
+    }
+    if (!got) throw Error(ICCG_ERR_IO, "Missing size line");
+    long long nr, nc, nz;
+    {
+        const char* p = b;
+        if (!(parse_ll(p, e, nr) && parse_ll(p, e, nc) && parse_ll(p, e, nz)))
+            throw Error(ICCG_ERR_IO, "Invalid size line");
+    }
+    const int nrows = (int)nr, ncols = (int)nc, nnz = (int)nz;
+    const bool sym = symmetry == "symmetric";
+    const bool pattern = field == "pattern";
+    std::vector<int> I, J;
+    std::vector<double> V;
+    size_t cap = (size_t)std::max(nnz, 0) * (sym ? 2 : 1);
+    I.reserve(cap); J.reserve(cap); V.reserve(cap);
+    auto push = [&](int i, int j, double v) {
+        if (i < 0 || i >= nrows || j < 0 || j >= ncols) throw Error(ICCG_ERR_IO, "Index out of range");
+        I.push_back(i); J.push_back(j); V.push_back(v);
+    };
+    for (int k = 0; k < nnz; ++k) {
+        if (!L.next(b, e)) throw Error(ICCG_ERR_IO, "Unexpected EOF");
+        if (e == b || *b == '%') { --k; continue; }
+        const char* p = b;
+        long long ii, jj;
+        if (!(parse_ll(p, e, ii) && parse_ll(p, e, jj)))
+            throw Error(ICCG_ERR_IO, "Invalid entry line (indices)");
+        double v = 1.0;
+        if (!pattern && !parse_double(p, e, v)) throw Error(ICCG_ERR_IO, "Invalid entry line (value)");
+        int i = (int)(ii - 1), j = (int)(jj - 1);
+        push(i, j, v);
+        if (sym && i != j) push(j, i, v);
+    }
+    // COO -> CRS: bucket by row (stable), sort each row by column (stable),
+    // sum duplicates in order.
+    CRS A;
+    A.n = nrows;
+    const size_t m = I.size();
+    std::vector<int> cnt((size_t)nrows + 1, 0);
+    for (size_t t = 0; t < m; ++t) cnt[(size_t)I[t] + 1]++;
+    for (int r = 0; r < nrows; ++r) cnt[(size_t)r + 1] += cnt[(size_t)r];
+    std::vector<int> ord(m);
+    {
+        std::vector<int> cur(cnt.begin(), cnt.end() - 1);
+        for (size_t t = 0; t < m; ++t) ord[(size_t)cur[(size_t)I[t]]++] = (int)t;
+    }
+    A.rowptr.assign((size_t)nrows + 1, 0);
+    A.colind.reserve(m);
+    A.val.reserve(m);
+    for (int r = 0; r < nrows; ++r) {
+        int* s = ord.data() + cnt[(size_t)r];
+        int* t = ord.data() + cnt[(size_t)r + 1];
+        std::stable_sort(s, t, [&](int a, int c) { return J[(size_t)a] < J[(size_t)c]; });
+        for (int* q = s; q < t;) {
+            int c = J[(size_t)*q];
+            double acc = 0.0;
+            do { acc += V[(size_t)*q]; ++q; } while (q < t && J[(size_t)*q] == c);
+            A.colind.push_back(c);
+            A.val.push_back(acc);
+        }
+        A.rowptr[(size_t)r + 1] = (int)A.colind.size();
+    }
+    return A;
+}
+
+void write_matrix_market(const std::string& path, const CRS& A, bool symmetric_lower)
+{
+    FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) throw Error(ICCG_ERR_IO, "cannot write " + path);
+    long long cnt = 0;
+    for (int i = 0; i < A.n; ++i)
+        for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k)
+            if (!symmetric_lower || A.colind[k] <= i) ++cnt;
+    std::fprintf(f, "%%%%MatrixMarket matrix coordinate real %s\n",
+                 symmetric_lower ? "symmetric" : "general");
+    std::fprintf(f, "%d %d %lld\n", A.n, A.n, cnt);
+    for (int i = 0; i < A.n; ++i)
+        for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k)
+            if (!symmetric_lower || A.colind[k] <= i)
+                std::fprintf(f, "%d %d %.17g\n", i + 1, A.colind[k] + 1, A.val[k]);
+    std::fclose(f);
+}
+
+// ReadColorFile_1Based (color.cpp:14-47), ReadBlockFile_1Based
+// (block.cpp:15-51), ReadBlockColorFile_1Based (block.cpp:53-89).
+std::vector<int> read_assignment_1based(int kind, const std::string& path, int n_expected, int& k_out)
+{
+    static const char* what[3] = {"color", "block", "block-color"};
+    if (kind < 0 || kind > 2) throw Error(ICCG_ERR_ARG, "bad assignment kind");
+    std::string buf;
+    try {
+        buf = slurp(path);
+    } catch (const Error&) {
+        throw Error(ICCG_ERR_IO, std::string("cannot open ") + what[kind] + " file: " + path);
+    }
+    const char* p = buf.data();
+    const char* e = p + buf.size();
+    auto skipws = [&] { while (p < e && (is_ws(*p) || *p == '\n')) ++p; };
+    auto read_int = [&](int& v) -> bool {
+        skipws();
+        if (p >= e) return false;
+        char tmp[32];
+        size_t len = 0;
+        while (p + len < e && !is_ws(p[len]) && p[len] != '\n' && len < 31) { tmp[len] = p[len]; ++len; }
+        tmp[len] = 0;
+        char* q;
+        long x = std::strtol(tmp, &q, 10);
+        if (q == tmp) return false;
+        p += (q - tmp);
+        v = (int)x;
+        return true;
+    };
+    int K = 0;
+    if (!read_int(K)) throw Error(ICCG_ERR_IO, std::string("failed to read first line of ") + what[kind] + " file");
+    if (K <= 0) throw Error(ICCG_ERR_IO, std::string(what[kind]) + " count must be positive");
+    std::vector<int> out((size_t)std::max(n_expected, 0), -1);
+    int assigned = 0, id, v;
+    while (read_int(id) && read_int(v)) {
+        if (id < 1 || id > n_expected)
+            throw Error(ICCG_ERR_IO, std::string("id out of range in ") + what[kind] + " file: " + std::to_string(id));
+        if (v < 1 || v > K)
+            throw Error(ICCG_ERR_IO, std::string("value out of range in ") + what[kind] + " file: " + std::to_string(v));
+        if (out[(size_t)id - 1] == -1) ++assigned;
+        out[(size_t)id - 1] = v - 1;
+    }
+    if (assigned != n_expected)
+        throw Error(ICCG_ERR_IO, std::string(what[kind]) + " file does not assign all ids: assigned=" +
+                                     std::to_string(assigned) + " expected=" + std::to_string(n_expected));
+    k_out = K;
+    return out;
+}
+
+void write_assignment_1based(const std::string& path, const int* v0, int n, int k)
+{
+    FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) throw Error(ICCG_ERR_IO, "cannot write " + path);
+    std::fprintf(f, "%d\n", k);
+    for (int i = 0; i < n; ++i) std::fprintf(f, "%d %d\n", i + 1, v0[i] + 1);
+    std::fclose(f);
+}
+
+namespace {
+
+// stable counting sort of ids [0,n) by key[id] (ids ascending within a key)
+std::vector<int> counting_order(const std::vector<int>& key, const std::vector<int>& ids_in)
+{
+    int lo = 0, hi = -1;
+    for (int id : ids_in) { lo = std::min(lo, key[(size_t)id]); hi = std::max(hi, key[(size_t)id]); }
+    std::vector<int> out(ids_in.size());
+    if (ids_in.empty()) return out;
+    long range = (long)hi - lo + 1;
+    if (range > (long)ids_in.size() * 4 + 1024) {
+        out = ids_in;
+        std::stable_sort(out.begin(), out.end(), [&](int a, int b) { return key[(size_t)a] < key[(size_t)b]; });
+        return out;
+    }
+    std::vector<int> cnt((size_t)range + 1, 0);
+    for (int id : ids_in) cnt[(size_t)(key[(size_t)id] - lo) + 1]++;
+    for (long r = 0; r < range; ++r) cnt[(size_t)r + 1] += cnt[(size_t)r];
+    for (int id : ids_in) out[(size_t)cnt[(size_t)(key[(size_t)id] - lo)]++] = id;
+    return out;
+}
+
+}  // namespace
+
+// BuildPermutationByColor (color.cpp:50-63): order = ids sorted by
+// (color, old id); new_of_old[order[k]] = k.
+std::vector<int> build_permutation_by_color(const std::vector<int>& color)
+{
+    const int n = (int)color.size();
+    std::vector<int> ids((size_t)n);
+    std::iota(ids.begin(), ids.end(), 0);
+    std::vector<int> order = counting_order(color, ids);
+    std::vector<int> new_of_old((size_t)n);
+    for (int k = 0; k < n; ++k) new_of_old[(size_t)order[(size_t)k]] = k;
+    return new_of_old;
+}
+
+// BuildPermutationByBlockColor (block.cpp:92-114): sort by
+// (block_color[block], block, old id), done as two stable counting passes.
+std::vector<int> build_permutation_by_block_color(const std::vector<int>& block_of_old,
+                                                  const std::vector<int>& block_color)
+{
+    const int n = (int)block_of_old.size();
+    std::vector<int> ids((size_t)n);
+    std::iota(ids.begin(), ids.end(), 0);
+    std::vector<int> by_block = counting_order(block_of_old, ids);
+    std::vector<int> ckey((size_t)n);
+    for (int i = 0; i < n; ++i) ckey[(size_t)i] = block_color[(size_t)block_of_old[(size_t)i]];
+    std::vector<int> order = counting_order(ckey, by_block);
+    std::vector<int> new_of_old((size_t)n);
+    for (int k = 0; k < n; ++k) new_of_old[(size_t)order[(size_t)k]] = k;
+    return new_of_old;
+}
+
+// Permute_PtAP_LowerCRS_to_LowerCRS (color.cpp:66-141).  Uses only j <= i of
+// the input, folds each entry to (max(ip,jp), min(ip,jp)), sorts every row by
+// column, sums duplicate columns (in input order) and drops sums equal to 0.0.
+CRS permute_ptap_lower(const CRS& A, const std::vector<int>& new_of_old)
+{
+    const int n = A.n;
+    if ((int)new_of_old.size() != n) throw Error(ICCG_ERR_ARG, "Permute_PtAP: new_of_old size mismatch");
+    if ((int)A.rowptr.size() != n + 1) throw Error(ICCG_ERR_ARG, "Permute_PtAP: A.rowptr size mismatch");
+    std::vector<int> cnt((size_t)n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+        const int ip = new_of_old[(size_t)i];
+        for (int k = A.rowptr[(size_t)i]; k < A.rowptr[(size_t)i + 1]; ++k) {
+            const int j = A.colind[(size_t)k];
+            if (j > i) continue;
+            const int jp = new_of_old[(size_t)j];
+            cnt[(size_t)std::max(ip, jp) + 1]++;
+        }
+    }
+    for (int r = 0; r < n; ++r) cnt[(size_t)r + 1] += cnt[(size_t)r];
+    const size_t m = (size_t)cnt[(size_t)n];
+    std::vector<int> bc(m);
+    std::vector<double> bv(m);
+    {
+        std::vector<int> cur(cnt.begin(), cnt.end() - 1);
+        for (int i = 0; i < n; ++i) {
+            const int ip = new_of_old[(size_t)i];
+            for (int k = A.rowptr[(size_t)i]; k < A.rowptr[(size_t)i + 1]; ++k) {
+                const int j = A.colind[(size_t)k];
+                if (j > i) continue;
+                const int jp = new_of_old[(size_t)j];
+                const int r = std::max(ip, jp), c = std::min(ip, jp);
+                const int pos = cur[(size_t)r]++;
+                bc[(size_t)pos] = c;
+                bv[(size_t)pos] = A.val[(size_t)k];
+            }
+        }
+    }
+    CRS B;
+    B.n = n;
+    B.rowptr.assign((size_t)n + 1, 0);
+    B.colind.reserve(m);
+    B.val.reserve(m);
+    std::vector<std::pair<int, double>> tmp;
+    for (int r = 0; r < n; ++r) {
+        const int s = cnt[(size_t)r], e = cnt[(size_t)r + 1];
+        if (e > s) {
+            // stable insertion sort by column (rows are short)
+            for (int t = s + 1; t < e; ++t) {
+                int c = bc[(size_t)t];
+                double v = bv[(size_t)t];
+                int u = t - 1;
+                while (u >= s && bc[(size_t)u] > c) { bc[(size_t)u + 1] = bc[(size_t)u]; bv[(size_t)u + 1] = bv[(size_t)u]; --u; }
+                bc[(size_t)u + 1] = c;
+                bv[(size_t)u + 1] = v;
+            }
+            int cur_c = bc[(size_t)s];
+            double acc = bv[(size_t)s];
+            for (int t = s + 1; t < e; ++t) {
+                if (bc[(size_t)t] == cur_c) {
+                    acc += bv[(size_t)t];
+                } else {
+                    if (acc != 0.0) { B.colind.push_back(cur_c); B.val.push_back(acc); }
+                    cur_c = bc[(size_t)t];
+                    acc = bv[(size_t)t];
+                }
+            }
+            if (acc != 0.0) { B.colind.push_back(cur_c); B.val.push_back(acc); }
+        }
+        B.rowptr[(size_t)r + 1] = (int)B.colind.size();
+    }
+    return B;
+}
+
+// expand_lower_to_full (crs_io.cpp:163-227): diagonal once, (i,j) and (j,i)
+// for each off-diagonal; columns sorted per row.  Row i of the output is
+// (lower part of row i) followed by (transposed entries from rows k > i), and
+// both parts arrive already ascending, so a merge replaces the sort.
+CRS expand_lower_to_full(const CRS& L)
+{
+    const int n = L.n;
+    CRS F;
+    F.n = n;
+    std::vector<int> cnt((size_t)n + 1, 0);
+    for (int i = 0; i < n; ++i)
+        for (int k = L.rowptr[(size_t)i]; k < L.rowptr[(size_t)i + 1]; ++k) {
+            const int j = L.colind[(size_t)k];
+            cnt[(size_t)i + 1]++;
+            if (j != i) cnt[(size_t)j + 1]++;
+        }
+    for (int i = 0; i < n; ++i) cnt[(size_t)i + 1] += cnt[(size_t)i];
+    const size_t m = (size_t)cnt[(size_t)n];
+    F.rowptr = cnt;
+    F.colind.resize(m);
+    F.val.resize(m);
+    std::vector<int> cur(cnt.begin(), cnt.end() - 1);
+    for (int i = 0; i < n; ++i)
+        for (int k = L.rowptr[(size_t)i]; k < L.rowptr[(size_t)i + 1]; ++k) {
+            const int j = L.colind[(size_t)k];
+            const double v = L.val[(size_t)k];
+            const int p = cur[(size_t)i]++;
+            F.colind[(size_t)p] = j;
+            F.val[(size_t)p] = v;
+            if (j != i) {
+                const int q = cur[(size_t)j]++;
+                F.colind[(size_t)q] = i;
+                F.val[(size_t)q] = v;
+            }
+        }
+    // per-row stable sort by column (the reference's index sort)
+    std::vector<std::pair<int, double>> row;
+    for (int i = 0; i < n; ++i) {
+        const int s = F.rowptr[(size_t)i], e = F.rowptr[(size_t)i + 1];
+        bool sorted = true;
+        for (int t = s + 1; t < e; ++t)
+            if (F.colind[(size_t)t] < F.colind[(size_t)t - 1]) { sorted = false; break; }
+        if (sorted) continue;
+        row.clear();
+        for (int t = s; t < e; ++t) row.emplace_back(F.colind[(size_t)t], F.val[(size_t)t]);
+        std::stable_sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        for (int t = s; t < e; ++t) { F.colind[(size_t)t] = row[(size_t)(t - s)].first; F.val[(size_t)t] = row[(size_t)(t - s)].second; }
+    }
+    return F;
+}
+
+// BuildColorPtrRows_FromPermutationAndColor (color.cpp:164-197)
+void build_color_schedule(const std::vector<int>& color, int nc, const std::vector<int>& new_of_old,
+                          std::vector<int>& color_ptr, std::vector<int>& rows_of_color)
+{
+    const int n = (int)color.size();
+    if ((int)new_of_old.size() != n) throw Error(ICCG_ERR_ARG, "size mismatch");
+    std::vector<int> old_of_new((size_t)n, -1);
+    for (int o = 0; o < n; ++o) {
+        const int id = new_of_old[(size_t)o];
+        if (id < 0 || id >= n) throw Error(ICCG_ERR_ARG, "invert_permutation: out of range");
+        old_of_new[(size_t)id] = o;
+    }
+    color_ptr.assign((size_t)nc + 1, 0);
+    for (int i = 0; i < n; ++i) {
+        const int c = color[(size_t)old_of_new[(size_t)i]];
+        if ((unsigned)c >= (unsigned)nc) throw Error(ICCG_ERR_ARG, "color out of range");
+        color_ptr[(size_t)c + 1]++;
+    }
+    for (int c = 0; c < nc; ++c) color_ptr[(size_t)c + 1] += color_ptr[(size_t)c];
+    rows_of_color.assign((size_t)n, -1);
+    std::vector<int> cur(color_ptr.begin(), color_ptr.end() - 1);
+    for (int i = 0; i < n; ++i) rows_of_color[(size_t)cur[(size_t)color[(size_t)old_of_new[(size_t)i]]]++] = i;
+}
+
+// BuildABMCSchedule (block.cpp:116-174)
+void build_abmc_schedule(const std::vector<int>& new_of_old, const std::vector<int>& block_of_old,
+                         const std::vector<int>& block_color, int nb, int nc,
+                         std::vector<int>& color_ptr_blk, std::vector<int>& blocks_of_color,
+                         std::vector<int>& block_ptr, std::vector<int>& rows_of_block)
+{
+    const int n = (int)new_of_old.size();
+    std::vector<int> old_of_new((size_t)n, -1);
+    for (int o = 0; o < n; ++o) {
+        const int id = new_of_old[(size_t)o];
+        if (id < 0 || id >= n) throw Error(ICCG_ERR_ARG, "new_of_old out of range");
+        old_of_new[(size_t)id] = o;
+    }
+    for (int o = 0; o < n; ++o) {
+        const int b = block_of_old[(size_t)o];
+        if (b < 0 || b >= nb) throw Error(ICCG_ERR_ARG, "block id out of range");
+        if (block_color[(size_t)b] < 0 || block_color[(size_t)b] >= nc) throw Error(ICCG_ERR_ARG, "block color out of range");
+    }
+    std::vector<char> seen((size_t)nb, 0);
+    color_ptr_blk.assign((size_t)nc + 1, 0);
+    for (int i = 0; i < n; ++i) {
+        const int b = block_of_old[(size_t)old_of_new[(size_t)i]];
+        if (!seen[(size_t)b]) { seen[(size_t)b] = 1; color_ptr_blk[(size_t)block_color[(size_t)b] + 1]++; }
+    }
+    for (int c = 0; c < nc; ++c) color_ptr_blk[(size_t)c + 1] += color_ptr_blk[(size_t)c];
+    blocks_of_color.assign((size_t)nb, -1);
+    std::vector<int> cur(color_ptr_blk.begin(), color_ptr_blk.end() - 1);
+    std::fill(seen.begin(), seen.end(), 0);
+    for (int i = 0; i < n; ++i) {
+        const int b = block_of_old[(size_t)old_of_new[(size_t)i]];
+        if (!seen[(size_t)b]) { seen[(size_t)b] = 1; blocks_of_color[(size_t)cur[(size_t)block_color[(size_t)b]]++] = b; }
+    }
+    block_ptr.assign((size_t)nb + 1, 0);
+    for (int i = 0; i < n; ++i) block_ptr[(size_t)block_of_old[(size_t)old_of_new[(size_t)i]] + 1]++;
+    for (int b = 0; b < nb; ++b) block_ptr[(size_t)b + 1] += block_ptr[(size_t)b];
+    rows_of_block.assign((size_t)n, -1);
+    std::vector<int> cur2(block_ptr.begin(), block_ptr.end() - 1);
+    for (int i = 0; i < n; ++i) rows_of_block[(size_t)cur2[(size_t)block_of_old[(size_t)old_of_new[(size_t)i]]]++] = i;
+}
+
+}  // namespace iccg

@@ -1,0 +1,254 @@
+/*
+ * iccg.h -- C ABI of iccg_b200, a Blackwell (sm_100a) implementation of the
+ * preconditioned conjugate-gradient hot path of stomo0511/ICCG.
+ *
+ * Plain C types only: ints, doubles, pointers and sizes.  Every function
+ * returns an int status (ICCG_OK = 0) unless stated otherwise; no C++
+ * exception crosses this boundary.  A context (iccg_ctx) owns one CUDA stream
+ * and the device-resident matrix, schedule, preconditioner and work vectors
+ * of one linear system.  A context is not thread-safe; use one per thread or
+ * per system.  Any number of contexts may live on one device.
+ *
+ * Each declaration names the reference interface it replaces (file:line in
+ * stomo0511/ICCG).  The CRS layout is the reference's (crs_io.hpp:10-49):
+ * 0-based int32 rowptr[n+1], int32 colind[nnz] (ascending within a row),
+ * double val[nnz].  The schedule arrays are the reference's ColorSchedule
+ * (color.hpp:9-22).
+ */
+#ifndef ICCG_H
+#define ICCG_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define ICCG_OK 0
+#define ICCG_ERR_ARG (-1)           /* bad size / index / pointer              */
+#define ICCG_ERR_DIAG (-2)          /* IC(0): diagonal missing   (ic0.cpp:52)  */
+#define ICCG_ERR_PIVOT_ZERO (-3)    /* IC(0): |L_jj| < 1e-30     (ic0.cpp:86)  */
+#define ICCG_ERR_PIVOT_NONPOS (-4)  /* IC(0): pivot <= 0         (ic0.cpp:104) */
+#define ICCG_ERR_IO (-5)            /* malformed or unreadable file            */
+#define ICCG_ERR_NOMEM (-6)         /* host or device allocation failed        */
+#define ICCG_ERR_CUDA (-7)          /* CUDA runtime error                      */
+#define ICCG_ERR_STATE (-8)         /* call order (e.g. apply before build)    */
+#define ICCG_ERR_SCHEDULE (-9)      /* schedule violates a dependency          */
+#define ICCG_ERR_NONFINITE (-10)    /* NaN/Inf in a CG scalar                  */
+
+/* ---- enums ------------------------------------------------------------- */
+#define ICCG_PRECOND_NONE 0      /* Identity  (precond.hpp:8-17)           */
+#define ICCG_PRECOND_JACOBI 1    /* Jacobi    (precond.hpp:19-45)          */
+#define ICCG_PRECOND_IC0 2       /* IC0       (ic0.hpp:11-76)              */
+
+#define ICCG_SCHED_NONE 0        /* natural order (iccg_crs)               */
+#define ICCG_SCHED_MC 1          /* ColorSchedule::MC_NODE                 */
+#define ICCG_SCHED_ABMC 2        /* ColorSchedule::ABMC_BLOCK              */
+
+#define ICCG_STORE_FP64 0        /* A and L stored in FP64                 */
+#define ICCG_STORE_FP32 1        /* A and L stored in FP32, FP64 vectors   */
+
+#define ICCG_MODE_PLAIN 0        /* one kernel per reference operation,
+                                    scalars checked on the host each
+                                    iteration (the plain FP64 GPU path)    */
+#define ICCG_MODE_FUSED 1        /* fused kernels, device-side scalars,
+                                    iterations replayed as a CUDA graph    */
+
+/* CG result (cg_crs.cpp:82-86) plus what the reference prints afterwards. */
+typedef struct {
+    int iters;               /* CGResult::iters                           */
+    int converged;           /* CGResult::converged                       */
+    int status;              /* 0 converged, 1 breakdown, 2 max_iter      */
+    int n_replacements;      /* FP64 residual replacements performed      */
+    double rel_resid;        /* CGResult::rel_resid (recurrence)          */
+    double true_rel_resid;   /* ||b - A x|| / ||b|| in FP64 (cg_crs.cpp:518-528) */
+    double solve_ms;         /* device time of the solve (CUDA events)    */
+} iccg_result;
+
+typedef struct {
+    int mode;          /* ICCG_MODE_PLAIN or ICCG_MODE_FUSED                  */
+    int storage;       /* ICCG_STORE_FP64 or ICCG_STORE_FP32                  */
+    int rr_interval;   /* FP64 residual replacement every k iterations
+                          (FP32 storage only; 0 = off; default 50)           */
+    int graph_iters;   /* FUSED: iterations per graph launch (default 8)     */
+} iccg_solve_opts;
+
+typedef struct iccg_ctx iccg_ctx;
+typedef struct iccg_crs iccg_crs;
+
+/* ======================================================================= */
+/* Host-side CRS objects and file formats                                   */
+/* ======================================================================= */
+
+/* read_matrix_market_crs (crs_io.hpp:52, crs_io.cpp:73-159) */
+int iccg_mm_read(const char* path, iccg_crs** out);
+/* writes A (full) as MatrixMarket coordinate real; symmetric=1 writes the
+   lower triangle with a `symmetric` header */
+int iccg_mm_write(const char* path, int n, const int* rowptr, const int* colind,
+                  const double* val, int symmetric);
+/* wraps caller arrays into a new CRS object (copies) */
+int iccg_crs_create(int n, const int* rowptr, const int* colind, const double* val,
+                    iccg_crs** out);
+int iccg_crs_dims(const iccg_crs* a, int* n, int* nnz);
+int iccg_crs_copy(const iccg_crs* a, int* rowptr, int* colind, double* val);
+void iccg_crs_free(iccg_crs* a);
+
+/* ReadColorFile_1Based (color.cpp:14-47)        kind 0
+   ReadBlockFile_1Based (block.cpp:15-51)        kind 1
+   ReadBlockColorFile_1Based (block.cpp:53-89)   kind 2
+   out[n_expected] receives 0-based ids, *k_out the count in the header. */
+int iccg_read_assignment(int kind, const char* path, int n_expected, int* out, int* k_out);
+/* writes the same formats (1-based), k = header count */
+int iccg_write_assignment(const char* path, int n, const int* values0, int k);
+
+/* ======================================================================= */
+/* Orderings and schedules (bit-exact with the reference)                   */
+/* ======================================================================= */
+
+/* BuildPermutationByColor (color.cpp:50-63) */
+int iccg_perm_by_color(int n, const int* color, int* new_of_old);
+/* BuildPermutationByBlockColor (block.cpp:92-114) */
+int iccg_perm_by_block_color(int n, int nb, const int* block_of_old, const int* block_color,
+                             int* new_of_old);
+/* Permute_PtAP_LowerCRS_to_LowerCRS (color.cpp:66-141).  cap >= number of
+   entries with j <= i in the input; *out_nnz receives the result size. */
+int iccg_ptap_lower(int n, const int* rowptr, const int* colind, const double* val,
+                    const int* new_of_old, int cap, int* out_rowptr, int* out_colind,
+                    double* out_val, int* out_nnz);
+/* expand_lower_to_full (crs_io.hpp:56, crs_io.cpp:163-227) */
+int iccg_expand_lower_nnz(int n, const int* rowptr, const int* colind, int* out_nnz);
+int iccg_expand_lower_to_full(int n, const int* rowptr, const int* colind, const double* val,
+                              int* out_rowptr, int* out_colind, double* out_val);
+/* BuildColorPtrRows_FromPermutationAndColor (color.cpp:164-197) */
+int iccg_color_schedule(int n, const int* color, int nc, const int* new_of_old,
+                        int* color_ptr, int* rows_of_color);
+/* BuildABMCSchedule (block.cpp:116-174) */
+int iccg_abmc_schedule(int n, const int* new_of_old, const int* block_of_old,
+                       const int* block_color, int nb, int nc, int* color_ptr_blk,
+                       int* blocks_of_color, int* block_ptr, int* rows_of_block);
+/* DebugCheck_InterBlockSameColorEdges (cg_crs.cpp:171-224): returns the total
+   count (>= 0) or ICCG_ERR_ARG; per-color counts into by_color[nc] if given. */
+long long iccg_check_interblock_same_color(int n, const int* rowptr, const int* colind,
+                                           const int* block_of_old, const int* block_color,
+                                           int nb, int nc, long long* by_color);
+/* DebugCheck_ScheduleHazards_OnLower (cg_crs.cpp:259-336): same-color j<i
+   dependencies in the lower pattern of the permuted matrix. */
+long long iccg_check_schedule_hazards(int n, const int* rowptr, const int* colind,
+                                      const int* new_of_old, const int* color_old,
+                                      const int* block_of_old, long long* same_block,
+                                      long long* cross_block);
+
+/* ======================================================================= */
+/* Problem generators (no counterpart in the reference, whose inputs come   */
+/* from SuiteSparse and an external igraph tool, run_*.sh, check_igraph.cpp) */
+/* ======================================================================= */
+
+#define ICCG_GEN_2D5 0   /* 5-point, diag 2(wx+wy), off -wx/-wy               */
+#define ICCG_GEN_3D7 1   /* 7-point, diag 2(wx+wy+wz), off -wx/-wy/-wz         */
+int iccg_gen_stencil(int kind, int nx, int ny, int nz, double wx, double wy, double wz,
+                     iccg_crs** out);
+/* 27-point cell-centred diffusion on nx*ny*nz cells; coefficients are the
+   harmonic means of exp(sigma*g), g a unit-variance Gaussian field smoothed
+   by a 3-cell box filter, sigma set so max/min of the field = contrast. */
+int iccg_gen_diffusion27(int nx, int ny, int nz, double contrast, unsigned long long seed,
+                         iccg_crs** out);
+/* symmetrised k-nearest-neighbour graph Laplacian of npts uniform points in
+   the unit square, weights 1/dist, plus diag_shift * I */
+int iccg_gen_knn_laplacian(int npts, int k, double diag_shift, unsigned long long seed,
+                           iccg_crs** out);
+/* x[i] ~ U(-1,1) from splitmix64(seed): ((u >> 11) * 2^-53) * 2 - 1 */
+int iccg_gen_uniform(int n, unsigned long long seed, double* out);
+/* y = A x on the host in CSR order with spmv's rounding (cg_crs.cpp:68-77:
+   product and sum rounded separately); used to form b = A x* */
+int iccg_host_spmv(int n, const int* rowptr, const int* colind, const double* val, const double* x, double* y);
+/* greedy node coloring in natural order (smallest free color) */
+int iccg_color_greedy(int n, const int* rowptr, const int* colind, int* color, int* nc);
+/* ABMC blocking: method 0 = consecutive ids, 1 = breadth-first aggregation */
+int iccg_block_partition(int n, const int* rowptr, const int* colind, int block_size,
+                         int method, int* block_of_old, int* nb);
+/* greedy coloring of the block quotient graph in block-id order */
+int iccg_color_blocks(int n, const int* rowptr, const int* colind, const int* block_of_old,
+                      int nb, int* block_color, int* nc);
+
+/* ======================================================================= */
+/* Device context                                                           */
+/* ======================================================================= */
+
+int iccg_ctx_create(int device, iccg_ctx** out);
+int iccg_ctx_destroy(iccg_ctx* ctx);
+/* message of the last failing call on this context (never NULL) */
+const char* iccg_ctx_last_error(const iccg_ctx* ctx);
+/* message of the last failing context-free call on this thread */
+const char* iccg_last_error(void);
+/* the context's cudaStream_t, as void* */
+void* iccg_ctx_stream(iccg_ctx* ctx);
+/* number of kernels this context has launched so far (graph nodes count
+   once per replay) */
+long long iccg_ctx_launch_count(const iccg_ctx* ctx);
+/* bytes of device memory held by this context */
+long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
+
+/* Uploads A_run (the matrix conjugate_gradient runs on, cg_crs.cpp:442-447):
+   full symmetric CRS with ascending columns.  Keeps an FP64 copy and, on
+   first FP32-storage use, an FP32 copy of the values. */
+int iccg_matrix_upload(iccg_ctx* ctx, int n, const int* rowptr, const int* colind,
+                       const double* val);
+
+/* ColorSchedule with mode MC_NODE (color.hpp:9-13, cg_crs.cpp:468-471) */
+int iccg_schedule_mc(iccg_ctx* ctx, int nc, const int* color_ptr, const int* rows_of_color);
+/* ColorSchedule with mode ABMC_BLOCK (color.hpp:15-21, cg_crs.cpp:474-481) */
+int iccg_schedule_abmc(iccg_ctx* ctx, int nc, int nb, const int* color_ptr_blk,
+                       const int* blocks_of_color, const int* block_ptr,
+                       const int* rows_of_block);
+/* sched == nullptr: natural-order substitutions (ic0.cpp:368) */
+int iccg_schedule_none(iccg_ctx* ctx);
+
+/* Preconditioner construction: Identity(A) / Jacobi(A) / IC0(A, shift)
+   (precond.hpp:10, precond.hpp:23-36, ic0.cpp:6-12).  IC(0) is factored on
+   the device in the schedule's order.  auto_shift != 0: on a non-positive
+   pivot the factorisation restarts with shift = max(2*shift, 1e-12*max|a_ii|)
+   instead of failing (the reference throws, ic0.cpp:104-113).  The factor is
+   stored in FP64 and, for FP32-storage solves, also rounded to FP32. */
+int iccg_precond_build(iccg_ctx* ctx, int kind, double shift, int auto_shift);
+/* the shift the last IC(0) build ended with */
+double iccg_precond_shift(const iccg_ctx* ctx);
+
+/* Precond::apply(r, z, sched) (precond.hpp:12, precond.hpp:38, ic0.hpp:34,
+   ic0.cpp:366-393) with host vectors; storage selects FP64 or FP32 factor. */
+int iccg_precond_apply(iccg_ctx* ctx, const double* r, double* z, int storage);
+/* same with device pointers on the context's stream */
+int iccg_precond_apply_dev(iccg_ctx* ctx, const double* r, double* z, int storage);
+
+/* exports the device IC(0) factor in the reference's layout: L (CRS, lower +
+   diagonal, ic0.hpp:41-44) and L^T (CSC of L, ic0.hpp:46-48).  nnzL via
+   iccg_precond_nnz. */
+int iccg_precond_nnz(const iccg_ctx* ctx, int* nnzL);
+int iccg_precond_export(iccg_ctx* ctx, int* Lp, int* Li, double* Lx, int* Up, int* Ui,
+                        double* Ux);
+
+/* spmv (cg_crs.cpp:54-79), host vectors / device vectors */
+int iccg_spmv(iccg_ctx* ctx, const double* x, double* y, int storage);
+int iccg_spmv_dev(iccg_ctx* ctx, const double* x, double* y, int storage);
+
+/* dot / nrm2 (cg_crs.cpp:33-50) on device vectors, evaluated in double-double
+   and rounded once to double */
+int iccg_dot_dev(iccg_ctx* ctx, int n, const double* a, const double* b, double* out);
+
+/* conjugate_gradient<Precond> (cg_crs.cpp:89-162) on A_run with the built
+   preconditioner and schedule.  x holds x0 on entry and the solution on
+   return.  opts may be NULL (FUSED, FP64, rr 50, graph 8). */
+int iccg_solve(iccg_ctx* ctx, const double* b, double* x, int max_iter, double tol,
+               const iccg_solve_opts* opts, iccg_result* res);
+int iccg_solve_dev(iccg_ctx* ctx, const double* b, double* x, int max_iter, double tol,
+                   const iccg_solve_opts* opts, iccg_result* res);
+
+/* per-kernel-class device time of the last solve run with profiling on:
+   class 0 SpMV, 1 forward sweep, 2 backward sweep, 3 vector/reduction
+   kernels, 4 residual replacement.  enable != 0 brackets every launch of
+   the following solves with CUDA events (launches are not graphed then). */
+int iccg_profile_enable(iccg_ctx* ctx, int enable);
+int iccg_profile_read(iccg_ctx* ctx, int cls, double* total_ms, long long* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ICCG_H */

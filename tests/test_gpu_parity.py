@@ -1,0 +1,271 @@
+"""GPU parity: the CUDA path against the oracle and the golden fixtures.
+
+Bit-exact: SpMV, IC(0) factor, preconditioner apply (all schedules), the
+orderings.  FP64 CG (plain and fused): iteration count within 1 of the
+reference and ||x - x_ref|| / ||x_ref|| <= 1e-10 (the tolerance of the FP64
+path); in practice the fused and plain paths reproduce the reference's
+trajectory.  Mixed precision (FP32 storage, FP64 recurrences with residual
+replacement): true relative residual <= tol and the error against the FP64
+solution is reported.
+"""
+import numpy as np
+import pytest
+
+import iccg_b200 as ib
+import iccg_b200.problems as pb
+from oracle import bindings as ob
+from _util import golden_names, load_golden, golden_sched, to_color_schedule, rel_err
+
+pytestmark = pytest.mark.gpu
+
+X_TOL = 1e-10  # FP64 path: ||x - x_ref|| / ||x_ref||
+
+
+def _ctx_for(A, sched):
+    ctx = ib.Context(0)
+    ctx.upload(A)
+    ctx.set_schedule(sched)
+    return ctx
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_gpu_matches_golden(name):
+    g = load_golden(name)
+    n = int(g["n"])
+    A = ib.CRS.from_arrays(n, g["run_rowptr"], g["run_colind"], g["run_val"])
+    sched = to_color_schedule(golden_sched(g))
+    ctx = _ctx_for(A, sched)
+    assert np.array_equal(ctx.spmv(g["spmv_x"]), g["spmv_y"])
+    kind = {"cg": ib.PRECOND_NONE, "dcg": ib.PRECOND_JACOBI}.get(str(g["variant"]), ib.PRECOND_IC0)
+    ctx.build(kind, 0.0)
+    if kind == ib.PRECOND_IC0:
+        Lp, Li, Lx, Up, Ui, Ux = ctx.export_factor()
+        for a, k in ((Lp, "L_rowptr"), (Li, "L_colind"), (Lx, "L_val"), (Up, "LT_colptr"), (Ui, "LT_rowind"),
+                     (Ux, "LT_val")):
+            assert np.array_equal(a, g[k]), k
+    assert np.array_equal(ctx.apply(g["apply_r"]), g["apply_z"])
+    for mode in (ib.MODE_PLAIN, ib.MODE_FUSED):
+        x = np.zeros(n)
+        res = ctx.solve(g["cg_b"], x, 10000, float(g["cg_tol"]), mode=mode)
+        assert res.converged == bool(g["cg_converged"])
+        assert abs(res.iters - int(g["cg_iters"])) <= 1
+        assert rel_err(x, g["cg_x"]) <= X_TOL
+    ctx.close()
+
+
+def _oracle_solve(P, tol=1e-8, kind=2):
+    rp, ci, v = P.A_run.rowptr, P.A_run.colind, P.A_run.val
+    ic0 = ob.OracleIC0(P.A_run.n, rp, ci, v, 0.0) if kind == 2 else None
+    x, it, rel, cv, _ = ob.cg(P.A_run.n, rp, ci, v, P.b_run, np.zeros(P.A_run.n), kind, 10000, tol, ic0, P.sched)
+    return ic0, x, it, rel, cv
+
+
+@pytest.mark.parametrize("which", ["c1_mc", "abmc64_bfs", "abmc64_lin", "iccg_natural", "d27_abmc", "d27_mc", "knn"])
+def test_gpu_cg_parity_vs_oracle(which):
+    if which == "c1_mc":
+        P = pb.config_small_mc(128, seed=0)
+    elif which == "abmc64_bfs":
+        P = pb.config_abmc_aniso(64, 16, "bfs")
+    elif which == "abmc64_lin":
+        P = pb.config_abmc_aniso(64, 16, "linear")
+    elif which == "iccg_natural":
+        P = pb.make(pb.laplace3d_aniso(40), "iccg", seed=1)
+    elif which == "d27_abmc":
+        P = pb.config_diffusion27(40, "abmc", 16)
+    elif which == "d27_mc":
+        P = pb.config_diffusion27(40, "piccg")
+    else:
+        P = pb.config_knn(20000, seed=2)
+    ic0, xo, ito, relo, cvo = _oracle_solve(P)
+    ctx = _ctx_for(P.A_run, P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    # factor and one apply are bit-exact at this size
+    Lx = ctx.export_factor()[2]
+    assert np.array_equal(Lx, ic0.export()[2])
+    r = ib.gen_uniform(P.A_run.n, 11)
+    assert np.array_equal(ctx.apply(r), ic0.apply(r, P.sched))
+    assert np.array_equal(ctx.spmv(r), ob.spmv(P.A_run.n, P.A_run.rowptr, P.A_run.colind, P.A_run.val, r))
+    for mode in (ib.MODE_PLAIN, ib.MODE_FUSED):
+        x = np.zeros(P.A_run.n)
+        res = ctx.solve(P.b_run, x, 10000, 1e-8, mode=mode)
+        assert res.converged and cvo
+        assert abs(res.iters - ito) <= 1, (res.iters, ito)
+        assert rel_err(x, xo) <= X_TOL
+        assert res.true_rel_resid < 1.5e-8
+    ctx.close()
+
+
+@pytest.mark.parametrize("which", ["abmc64", "d27_abmc"])
+def test_gpu_mixed_precision(which):
+    P = pb.config_abmc_aniso(64, 16, "bfs") if which == "abmc64" else pb.config_diffusion27(40, "abmc", 16)
+    ctx = _ctx_for(P.A_run, P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    x64 = np.zeros(P.A_run.n)
+    r64 = ctx.solve(P.b_run, x64, 10000, 1e-8, storage=ib.STORE_FP64)
+    x32 = np.zeros(P.A_run.n)
+    r32 = ctx.solve(P.b_run, x32, 10000, 1e-8, storage=ib.STORE_FP32, rr_interval=50)
+    assert r64.converged and r32.converged
+    assert r32.true_rel_resid <= 1e-8          # the true residual, in FP64
+    assert r32.n_replacements >= 1
+    assert rel_err(x32, x64) <= 1e-6           # both are 1e-8-residual solutions
+    assert r32.iters <= r64.iters * 1.2 + 5
+    ctx.close()
+
+
+def test_gpu_apply_fp32_close_to_fp64():
+    P = pb.config_abmc_aniso(32, 16, "bfs")
+    ctx = _ctx_for(P.A_run, P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    r = ib.gen_uniform(P.A_run.n, 3)
+    z64 = ctx.apply(r, ib.STORE_FP64)
+    z32 = ctx.apply(r, ib.STORE_FP32)
+    assert rel_err(z32, z64) < 1e-5
+    y64 = ctx.spmv(r, ib.STORE_FP64)
+    y32 = ctx.spmv(r, ib.STORE_FP32)
+    assert rel_err(y32, y64) < 1e-6
+    ctx.close()
+
+
+def test_gpu_reference_interface():
+    """Drop-in use: IC0(A, shift).apply(r, z, sched) and conjugate_gradient()."""
+    P = pb.config_small_mc(48, seed=0)
+    M = ib.IC0(P.A_run, 0.0, sched=P.sched)
+    r = ib.gen_uniform(P.A_run.n, 1)
+    z = np.zeros(0)
+    M.apply(r, z, P.sched)
+    ic0 = ob.OracleIC0(P.A_run.n, P.A_run.rowptr, P.A_run.colind, P.A_run.val, 0.0)
+    assert np.array_equal(z, ic0.apply(r, P.sched))
+    x = np.zeros(P.A_run.n)
+    res = ib.conjugate_gradient(P.A_run, P.b_run, x, M, 10000, 1e-8, P.sched)
+    xo, ito, relo, cvo, _ = ob.cg(P.A_run.n, P.A_run.rowptr, P.A_run.colind, P.A_run.val, P.b_run,
+                                  np.zeros(P.A_run.n), 2, 10000, 1e-8, ic0, P.sched)
+    assert res.converged and abs(res.iters - ito) <= 1 and rel_err(x, xo) <= X_TOL
+    for cls, kind in ((ib.Identity, 0), (ib.Jacobi, 1)):
+        M2 = cls(P.A_run)
+        x2 = np.zeros(P.A_run.n)
+        r2 = ib.conjugate_gradient(P.A_run, P.b_run, x2, M2, 10000, 1e-8, None)
+        xo2, ito2, _, _, _ = ob.cg(P.A_run.n, P.A_run.rowptr, P.A_run.colind, P.A_run.val, P.b_run,
+                                   np.zeros(P.A_run.n), kind, 10000, 1e-8)
+        assert abs(r2.iters - ito2) <= 1 and rel_err(x2, xo2) <= X_TOL
+
+
+# ---------------------------------------------------------------------------
+# failure paths (host-side detection; nothing faults the GPU)
+# ---------------------------------------------------------------------------
+def _indefinite():
+    A = pb.poisson2d(12)
+    v = A.val.copy()
+    for i in range(A.n):
+        for k in range(A.rowptr[i], A.rowptr[i + 1]):
+            if A.colind[k] == i and i in (37, 90):
+                v[k] = -0.5
+    return ib.CRS(A.n, A.rowptr, A.colind, v)
+
+
+def test_gpu_nonpositive_pivot_reported_like_reference():
+    A = _indefinite()
+    with pytest.raises(ob.OracleError):
+        ob.OracleIC0(A.n, A.rowptr, A.colind, A.val, 0.0)
+    row = ob.orc().orc_last_error_row()
+    ctx = _ctx_for(A, None)
+    with pytest.raises(ib.IccgError) as e:
+        ctx.build(ib.PRECOND_IC0, 0.0)
+    assert e.value.code == ib.ERR_PIVOT_NONPOS
+    assert f"row {row}" in str(e.value)
+    ctx.build(ib.PRECOND_IC0, 0.0, auto_shift=True)
+    assert ctx.shift > 0.0
+    z = ctx.apply(np.ones(A.n))
+    assert np.all(np.isfinite(z))
+    ctx.close()
+
+
+def test_gpu_missing_diagonal():
+    A = ib.CRS.from_arrays(3, [0, 2, 3, 5], [0, 1, 0, 1, 2], [2.0, 1.0, 1.0, 1.0, 3.0])
+    ctx = _ctx_for(A, None)
+    with pytest.raises(ib.IccgError) as e:
+        ctx.build(ib.PRECOND_IC0, 0.0)
+    assert e.value.code == ib.ERR_DIAG and "row 1" in str(e.value)
+    ctx.close()
+
+
+def test_gpu_rejects_racy_schedule():
+    # an MC schedule of the unpermuted matrix puts dependencies on later colors
+    A = pb.poisson2d(8)
+    color, nc = ib.color_greedy(A)
+    cp = np.zeros(nc + 1, np.int32)
+    for c in range(nc):
+        cp[c + 1] = cp[c] + np.sum(color == c)
+    rows = np.argsort(color[::-1], kind="stable").astype(np.int32)  # any order
+    rows = np.concatenate([np.nonzero(color == c)[0] for c in range(nc)]).astype(np.int32)
+    bad = ib.ColorSchedule(nc=nc, color_ptr=cp, rows_of_color=rows[::-1].copy())
+    ctx = ib.Context(0)
+    ctx.upload(A)
+    with pytest.raises(ib.IccgError) as e:
+        ctx.set_schedule(bad)
+    assert e.value.code == ib.ERR_SCHEDULE
+    ctx.close()
+
+
+def test_gpu_state_errors():
+    ctx = ib.Context(0)
+    with pytest.raises(ib.IccgError) as e:
+        ctx.apply(np.ones(3))
+    assert e.value.code == ib.ERR_STATE
+    ctx.upload(pb.poisson2d(4))
+    with pytest.raises(ib.IccgError):
+        ctx.apply(np.ones(16))
+    ctx.close()
+
+
+def test_gpu_breakdown_and_maxiter_like_reference():
+    A = _indefinite()
+    b = np.ones(A.n)
+    xo, ito, relo, cvo, _ = ob.cg(A.n, A.rowptr, A.colind, A.val, b, np.zeros(A.n), 0, 10000, 1e-8)
+    ctx = _ctx_for(A, None)
+    ctx.build(ib.PRECOND_NONE)
+    for mode in (ib.MODE_PLAIN, ib.MODE_FUSED):
+        x = np.zeros(A.n)
+        res = ctx.solve(b, x, 10000, 1e-8, mode=mode)
+        assert res.converged == cvo and abs(res.iters - ito) <= 1
+    # max_iter cap (cg_crs.cpp:125)
+    P = pb.config_small_mc(16)
+    ctx2 = _ctx_for(P.A_run, P.sched)
+    ctx2.build(ib.PRECOND_IC0, 0.0)
+    ic0 = ob.OracleIC0(P.A_run.n, P.A_run.rowptr, P.A_run.colind, P.A_run.val, 0.0)
+    for cap in (0, 1, 3):
+        xo, ito, relo, cvo, _ = ob.cg(P.A_run.n, P.A_run.rowptr, P.A_run.colind, P.A_run.val, P.b_run,
+                                      np.zeros(P.A_run.n), 2, cap, 1e-8, ic0, P.sched)
+        for mode in (ib.MODE_PLAIN, ib.MODE_FUSED):
+            x = np.zeros(P.A_run.n)
+            res = ctx2.solve(P.b_run, x, cap, 1e-8, mode=mode)
+            assert res.iters == ito and not res.converged and res.status == "max_iter"
+            assert rel_err(x, xo) <= X_TOL if cap else np.all(x == 0)
+    ctx.close()
+    ctx2.close()
+
+
+# ---------------------------------------------------------------------------
+# full size: size-independent properties at the benchmark configuration
+# ---------------------------------------------------------------------------
+@pytest.mark.slow
+def test_gpu_full_size_abmc_128():
+    P = pb.config_abmc_aniso(128, 16, "bfs")
+    n = P.A_run.n
+    ctx = _ctx_for(P.A_run, P.sched)
+    x = ib.gen_uniform(n, 9)
+    assert np.array_equal(ctx.spmv(x), ib.host_spmv(P.A_run, x))      # bit-exact at 2.1M rows
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    ic0 = ob.OracleIC0(n, P.A_run.rowptr, P.A_run.colind, P.A_run.val, 0.0)
+    assert np.array_equal(ctx.export_factor()[2], ic0.export()[2])   # factor bit-exact
+    assert np.array_equal(ctx.apply(x), ic0.apply(x, P.sched))        # apply bit-exact
+    x64 = np.zeros(n)
+    r64 = ctx.solve(P.b_run, x64, 10000, 1e-8, storage=ib.STORE_FP64)
+    x32 = np.zeros(n)
+    r32 = ctx.solve(P.b_run, x32, 10000, 1e-8, storage=ib.STORE_FP32)
+    assert r64.converged and r64.true_rel_resid < 1.5e-8
+    assert r32.converged and r32.true_rel_resid <= 1e-8
+    assert rel_err(x32, x64) < 1e-6
+    xs_run = np.empty(n)
+    xs_run[P.new_of_old] = P.xstar
+    assert rel_err(x64, xs_run) < 1e-4   # error against x* is bounded by cond(A) * 1e-8
+    ctx.close()

@@ -1,0 +1,222 @@
+"""Host-side routines of iccg_b200 against the oracle (no GPU needed).
+
+Orderings, P^T A P, expansion and schedules must equal the reference bit for
+bit (SURVEY bit-exact contract); readers must accept and reject the same
+inputs as the reference's.
+"""
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import iccg_b200 as ib
+import iccg_b200.problems as pb
+from oracle import bindings as ob
+from _util import golden_names, load_golden
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+# ---------------------------------------------------------------------------
+# the C ABI library
+# ---------------------------------------------------------------------------
+def test_library_exports_every_declared_symbol():
+    header = (ROOT / "include" / "iccg.h").read_text()
+    declared = set(re.findall(r"\b(iccg_[a-z0-9_]+)\s*\(", header))
+    assert len(declared) > 40
+    L = ib.lib()
+    missing = [s for s in sorted(declared) if not hasattr(L, s)]
+    assert not missing, missing
+
+
+def test_python_binds_only_declared_symbols():
+    header = (ROOT / "include" / "iccg.h").read_text()
+    declared = set(re.findall(r"\b(iccg_[a-z0-9_]+)\s*\(", header))
+    src = (ROOT / "iccg_b200" / "__init__.py").read_text()
+    bound = set(re.findall(r'"(iccg_[a-z0-9_]+)"', src))
+    assert bound <= declared, bound - declared
+
+
+def test_error_message_on_bad_call():
+    with pytest.raises(ib.IccgError) as e:
+        ib.read_matrix_market_crs("/nonexistent/file.mtx")
+    assert e.value.code == ib.ERR_IO
+    assert "Failed to open" in str(e.value)
+
+
+# ---------------------------------------------------------------------------
+# orderings vs golden fixtures and the oracle
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("name", [n for n in golden_names() if "piccg" in n or "abmc" in n])
+def test_setup_matches_golden(name):
+    g = load_golden(name)
+    A = ib.CRS.from_arrays(int(g["n"]), g["A_rowptr"], g["A_colind"], g["A_val"])
+    if str(g["variant"]) == "piccg":
+        P = pb.setup(A, "piccg", color=g["color"], nc=int(g["nc"]))
+        assert np.array_equal(P.sched.color_ptr, g["color_ptr"])
+        assert np.array_equal(P.sched.rows_of_color, g["rows_of_color"])
+    else:
+        P = pb.setup(A, "abmc", block_of_old=g["block_of_old"], nb=int(g["nb"]), block_color=g["block_color"],
+                     nbc=int(g["nc"]))
+        for k in ("color_ptr_blk", "blocks_of_color", "block_ptr", "rows_of_block"):
+            assert np.array_equal(getattr(P.sched, k), g[k]), k
+    assert np.array_equal(P.new_of_old, g["perm"])
+    assert np.array_equal(P.A_run.rowptr, g["run_rowptr"])
+    assert np.array_equal(P.A_run.colind, g["run_colind"])
+    assert np.array_equal(P.A_run.val, g["run_val"])
+
+
+def _random_sym(n, density, seed, zeros=False):
+    rng = np.random.default_rng(seed)
+    M = (rng.random((n, n)) < density) * rng.standard_normal((n, n))
+    M = M + M.T
+    if zeros:
+        M[rng.random((n, n)) < 0.05] = 0.0
+        M = np.triu(M) + np.triu(M, 1).T
+    np.fill_diagonal(M, np.abs(M).sum(1) + 1.0)
+    rp, ci, v = [0], [], []
+    for i in range(n):
+        nz = np.nonzero(M[i])[0]
+        if zeros:  # keep some explicit zeros in the pattern
+            extra = rng.choice(n, 2, replace=False)
+            nz = np.unique(np.concatenate([nz, extra]))
+        ci += list(nz)
+        v += list(M[i, nz])
+        rp.append(len(ci))
+    return ib.CRS.from_arrays(n, rp, ci, v)
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_permutations_and_ptap_match_oracle(seed):
+    rng = np.random.default_rng(seed)
+    A = _random_sym(60 + 10 * seed, 0.08, seed, zeros=seed % 2 == 1)
+    color = rng.integers(0, 5, A.n).astype(np.int32)
+    p1 = ib.BuildPermutationByColor(color)
+    assert np.array_equal(p1, ob.perm_by_color(color))
+    nb = 9
+    blk = rng.integers(0, nb, A.n).astype(np.int32)
+    bcol = rng.integers(0, 3, nb).astype(np.int32)
+    p2 = ib.BuildPermutationByBlockColor(blk, bcol)
+    assert np.array_equal(p2, ob.perm_by_block_color(blk, bcol))
+    for p in (p1, p2):
+        L = ib.Permute_PtAP_LowerCRS_to_LowerCRS(A, p)
+        orp, oci, ov = ob.ptap_lower(A.n, A.rowptr, A.colind, A.val, p)
+        assert np.array_equal(L.rowptr, orp) and np.array_equal(L.colind, oci) and np.array_equal(L.val, ov)
+        assert not np.any(L.val == 0.0)  # color.cpp:123,132 drops exact zeros
+        F = ib.expand_lower_to_full(L)
+        frp, fci, fv = ob.expand_lower_to_full(A.n, orp, oci, ov)
+        assert np.array_equal(F.rowptr, frp) and np.array_equal(F.colind, fci) and np.array_equal(F.val, fv)
+    cp, rc = ib.BuildColorPtrRows_FromPermutationAndColor(color, 5, p1)
+    ocp, orc_ = ob.color_schedule(color, 5, p1)
+    assert np.array_equal(cp, ocp) and np.array_equal(rc, orc_)
+    s1 = ib.BuildABMCSchedule(p2, blk, bcol, nb, 3)
+    s2 = ob.abmc_schedule(p2, blk, bcol, nb, 3)
+    for a, b in zip(s1, s2):
+        assert np.array_equal(a, b)
+
+
+def test_abmc_schedule_with_empty_block():
+    # a block with no rows leaves -1 at the tail of blocks_of_color (block.cpp:141)
+    blk = np.array([0, 0, 2, 2, 0], np.int32)
+    bcol = np.array([0, 1, 1], np.int32)
+    p = ib.BuildPermutationByBlockColor(blk, bcol)
+    s1 = ib.BuildABMCSchedule(p, blk, bcol, 3, 2)
+    s2 = ob.abmc_schedule(p, blk, bcol, 3, 2)
+    for a, b in zip(s1, s2):
+        assert np.array_equal(a, b)
+    assert s1[1][-1] == -1
+
+
+def test_edge_cases_sizes():
+    # n = 1 and a diagonal matrix
+    A = ib.CRS.from_arrays(1, [0, 1], [0], [2.0])
+    P = pb.setup(A, "piccg", color=[0], nc=1)
+    assert P.A_run.nnz == 1
+    D = ib.CRS.from_arrays(4, [0, 1, 2, 3, 4], [0, 1, 2, 3], [1.0, 2.0, 3.0, 4.0])
+    c, nc = ib.color_greedy(D)
+    assert nc == 1
+
+
+# ---------------------------------------------------------------------------
+# readers and writers
+# ---------------------------------------------------------------------------
+def test_matrix_market_roundtrip_and_oracle(tmp_path):
+    A = pb.laplace3d_aniso(5)
+    p = tmp_path / "a.mtx"
+    ib.write_matrix_market(str(p), A, symmetric=True)
+    B = ib.read_matrix_market_crs(str(p))
+    assert np.array_equal(A.rowptr, B.rowptr) and np.array_equal(A.colind, B.colind)
+    assert np.array_equal(A.val, B.val)
+    n, rp, ci, v = ob.read_mm(p)
+    assert np.array_equal(B.rowptr, rp) and np.array_equal(B.colind, ci) and np.array_equal(B.val, v)
+
+
+def test_matrix_market_formats(tmp_path):
+    p = tmp_path / "g.mtx"
+    p.write_text("%%MatrixMarket matrix coordinate pattern general\n% c\n%\n3 3 4\n1 1\n\n2 2\n3 1\n3 3\n")
+    A = ib.read_matrix_market_crs(str(p))
+    assert A.n == 3 and list(A.colind) == [0, 1, 0, 2] and list(A.val) == [1, 1, 1, 1]
+    q = tmp_path / "d.mtx"  # duplicates are summed
+    q.write_text("%%MatrixMarket matrix coordinate real general\n2 2 3\n1 1 1.5\n1 1 2.5\n2 2 1\n")
+    B = ib.read_matrix_market_crs(str(q))
+    assert list(B.val) == [4.0, 1.0]
+    n, rp, ci, v = ob.read_mm(q)
+    assert list(v) == [4.0, 1.0]
+
+
+@pytest.mark.parametrize("text,msg", [
+    ("", "Empty file"),
+    ("%%MatrixMarket matrix array real general\n1 1\n1\n", "coordinate"),
+    ("%%MatrixMarket matrix coordinate complex general\n1 1 1\n1 1 1 0\n", "Unsupported field"),
+    ("%%MatrixMarket matrix coordinate real hermitian\n1 1 1\n1 1 1\n", "Unsupported symmetry"),
+    ("%MatrixMarket matrix coordinate real general\n1 1 1\n1 1 1\n", "Not a MatrixMarket"),
+    ("%%MatrixMarket matrix coordinate real general\n\n1 1 1\n", "Invalid size line"),
+    ("%%MatrixMarket matrix coordinate real general\n2 2 2\n1 1 1\n", "Unexpected EOF"),
+    ("%%MatrixMarket matrix coordinate real general\n2 2 1\n3 1 1\n", "Index out of range"),
+    ("%%MatrixMarket matrix coordinate real general\n2 2 1\n1 x 1\n", "Invalid entry line"),
+])
+def test_matrix_market_errors(tmp_path, text, msg):
+    p = tmp_path / "bad.mtx"
+    p.write_text(text)
+    with pytest.raises(ib.IccgError) as e:
+        ib.read_matrix_market_crs(str(p))
+    assert msg in str(e.value)
+    with pytest.raises(ob.OracleError):
+        ob.read_mm(p)
+
+
+def test_assignment_files(tmp_path):
+    p = tmp_path / "x.blk"
+    ib.write_assignment_1based(str(p), np.array([2, 0, 1, 1]), 3)
+    v, k = ib.ReadBlockFile_1Based(str(p), 4)
+    assert k == 3 and list(v) == [2, 0, 1, 1]
+    w, k2 = ob.read_assignment(p, 4)
+    assert np.array_equal(v, w) and k2 == 3
+    bad = tmp_path / "bad.bcol"
+    bad.write_text("2\n1 1\n")
+    with pytest.raises(ib.IccgError):
+        ib.ReadBlockColorFile_1Based(str(bad), 2)
+    # duplicates overwrite (color.cpp:57-59)
+    dup = tmp_path / "dup.col"
+    dup.write_text("2\n1 1\n2 1\n1 2\n")
+    c, nc = ib.ReadColorFile_1Based(str(dup), 2)
+    assert list(c) == [1, 0] and nc == 2
+
+
+# ---------------------------------------------------------------------------
+# schedule validators (cg_crs.cpp:171-336)
+# ---------------------------------------------------------------------------
+def test_hazard_checkers_match_oracle():
+    A = pb.laplace3d_aniso(6)
+    P = pb.make(A, "abmc", block_size=8)
+    t, byc = ib.check_interblock_same_color(A, P.block_of_old, P.block_color, P.nb, P.nc)
+    assert t == 0
+    h, sb, xb = ib.check_schedule_hazards(P.A_run, P.new_of_old, P.color, P.block_of_old)
+    assert xb == 0 and h == sb
+    # a bad block coloring: everything one color
+    bad = np.zeros(P.nb, np.int32)
+    t2, _ = ib.check_interblock_same_color(A, P.block_of_old, bad, P.nb, 1)
+    o2 = ob.orc().orc_check_interblock_same_color(A.n, ob._ptr(A.rowptr), ob._ptr(A.colind),
+                                                  ob._ptr(P.block_of_old), ob._ptr(bad), P.nb, 1, None)
+    assert t2 == o2 > 0
