@@ -2,8 +2,9 @@
 
 Workload (one step = one full solve of one system):
   3D 7-point Laplacian, 128^3 grid (n = 2,097,152, nnz = 14,581,760),
-  coefficients 1, 1, 0.01; ABMC with block size 16 (breadth-first blocks,
-  greedy block coloring), b = A x*, x* ~ U(-1,1) from splitmix64(0); x0 = 0;
+  coefficients 1, 1, 0.01; ABMC with block size 16 (16 consecutive rows per
+  block, greedy block coloring: 2 colors), b = A x*, x* ~ U(-1,1) from
+  splitmix64(0); x0 = 0;
   IC(0) preconditioner; A and L stored in FP32, x / r / p / z and all inner
   products in FP64, FP64 residual replacement every 50 iterations; converged
   when the FP64 true relative residual is below 1e-8.
@@ -36,6 +37,7 @@ sys.path.insert(0, str(ROOT))
 
 SIDE = 128
 BLOCK = 16
+BLOCKING = "linear"   # 16 consecutive rows per block: 2 block colors on this grid
 TOL = 1e-8
 RR = 50
 METRIC = "ICCG ms to resid 1e-8 (ABMC B=16, 3D 7-pt 128^3 aniso, FP32 storage / FP64 recurrences)"
@@ -120,7 +122,7 @@ class ClockSampler:
 def build_problem():
     import iccg_b200.problems as pb
     t0 = time.perf_counter()
-    P = pb.config_abmc_aniso(SIDE, BLOCK, "bfs", seed=0)
+    P = pb.config_abmc_aniso(SIDE, BLOCK, BLOCKING, seed=0)
     return P, time.perf_counter() - t0
 
 
@@ -281,7 +283,7 @@ def run_gpu(args):
         "data": "synthetic",
         "config": {
             "workload": WORKLOAD, "n": n, "nnz": P.A_run.nnz, "grid": f"{SIDE}^3", "coeffs": [1, 1, 0.01],
-            "block_size": BLOCK, "blocking": "bfs", "nb": P.nb, "colors": P.nc, "tol": TOL, "rr_interval": RR,
+            "block_size": BLOCK, "blocking": BLOCKING, "nb": P.nb, "colors": P.nc, "tol": TOL, "rr_interval": RR,
             "x0": "zeros", "rhs": "b = A x*, x* ~ U(-1,1) splitmix64(0)",
             "l2": "inputs larger than L2: ~0.5 GB streamed per iteration vs 126 MB L2",
             "parallelism": f"replicas x{world}",

@@ -49,6 +49,7 @@ ERR_IO, ERR_NOMEM, ERR_CUDA, ERR_STATE, ERR_SCHEDULE, ERR_NONFINITE = -5, -6, -7
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_IC0 = 0, 1, 2
 STORE_FP64, STORE_FP32 = 0, 1
 MODE_PLAIN, MODE_FUSED = 0, 1
+OPT_TILED = 0
 STATUS_NAMES = {0: "converged", 1: "breakdown", 2: "max_iter", 3: "nonfinite"}
 
 
@@ -118,6 +119,7 @@ def lib() -> C.CDLL:
         "iccg_ctx_stream": (_P, [_P]),
         "iccg_ctx_launch_count": (C.c_longlong, [_P]),
         "iccg_ctx_device_bytes": (C.c_longlong, [_P]),
+        "iccg_ctx_set_option": (_I, [_P, _I, C.c_longlong]),
         "iccg_matrix_upload": (_I, [_P, _I, _P, _P, _P]),
         "iccg_schedule_mc": (_I, [_P, _I, _P, _P]),
         "iccg_schedule_abmc": (_I, [_P, _I, _I, _P, _P, _P, _P]),
@@ -474,6 +476,13 @@ class Context:
     @property
     def device_bytes(self) -> int:
         return int(lib().iccg_ctx_device_bytes(self.h))
+
+    def set_option(self, option: int, value: int):
+        self._ck(lib().iccg_ctx_set_option(self.h, option, value))
+
+    def use_tiled(self, on: bool):
+        """Select the shared-memory tiled kernels (default) or the simple ones."""
+        self.set_option(OPT_TILED, int(on))
 
     def upload(self, A: CRS):
         self._A = A

@@ -374,6 +374,195 @@ __global__ void __launch_bounds__(256) k_sweep(SweepArgs a, int u0, int u1, int 
 }
 
 // ---------------------------------------------------------------------------
+// Tiled kernels.
+//
+// A CTA tile is a range of at most 256 consecutive rows whose CSR entries
+// [rowptr[R0], rowptr[R1]) are contiguous in memory.  The CTA first copies
+// that segment (column indices and values) into shared memory with 16-byte
+// vector loads marked streaming (evict-first: the matrix is read once per
+// iteration and should not push the vectors out of L2), then one thread per
+// row runs the row's arithmetic from shared memory in the reference's order.
+// Segments start at the 4-entry boundary at or below rowptr[R0]; every
+// device array carries 16 entries of padding, so the rounded-up tail of the
+// last tile stays inside the allocation.
+// ---------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ void stage_segment(const int* __restrict__ gcol, const T* __restrict__ gval, int ea,
+                                              int cnt, int* s_col, T* s_val)
+{
+    const int nv = (cnt + 3) >> 2;  // 4-entry groups
+    const int4* c4 = reinterpret_cast<const int4*>(gcol + ea);
+    int4* sc4 = reinterpret_cast<int4*>(s_col);
+    for (int v = threadIdx.x; v < nv; v += blockDim.x) sc4[v] = __ldcs(c4 + v);
+    if (sizeof(T) == 4) {
+        const float4* v4 = reinterpret_cast<const float4*>(gval + ea);
+        float4* sv4 = reinterpret_cast<float4*>(s_val);
+        for (int v = threadIdx.x; v < nv; v += blockDim.x) sv4[v] = __ldcs(v4 + v);
+    } else {
+        const double2* v2 = reinterpret_cast<const double2*>(gval + ea);
+        double2* sv2 = reinterpret_cast<double2*>(s_val);
+        for (int v = threadIdx.x; v < 2 * nv; v += blockDim.x) sv2[v] = __ldcs(v2 + v);
+    }
+}
+
+// SpMV over CTA tiles (tile_row: ntiles+1 row boundaries); same arithmetic as
+// k_spmv.  Dynamic shared memory: cap * (4 + sizeof(T)) bytes.
+template <class T, int FIN>
+__global__ void __launch_bounds__(256) k_spmv_tiled(int ntiles, const int* __restrict__ tile_row,
+                                                    const int* __restrict__ rp, const int* __restrict__ ci,
+                                                    const T* __restrict__ v, int cap,
+                                                    const double* __restrict__ x, double* __restrict__ y,
+                                                    SolverState* st, RedBuf red, unsigned int* ticket)
+{
+    if (st_done(st)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* s_val = reinterpret_cast<T*>(smem_raw);
+    int* s_col = reinterpret_cast<int*>(smem_raw + (size_t)cap * sizeof(T));
+    acc2 a[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int R0 = tile_row[t], R1 = tile_row[t + 1];
+        const int e0 = rp[R0], e1 = rp[R1];
+        const int ea = e0 & ~3;
+        stage_segment<T>(ci, v, ea, e1 - ea, s_col, s_val);
+        const int i = R0 + threadIdx.x;
+        int rs = 0, re = 0;
+        if (i < R1) {
+            rs = rp[i] - ea;
+            re = rp[i + 1] - ea;
+        }
+        __syncthreads();
+        if (i < R1) {
+            double sum = 0.0;
+            for (int k = rs; k < re; ++k) sum = sum + (double)s_val[k] * __ldg(x + s_col[k]);
+            y[i] = sum;
+            if (FIN == FIN_PAP) {
+                const double xi = __ldg(x + i);
+                acc2_fma(a[0], xi, sum);
+                acc2_fma(a[1], xi, xi);
+                acc2_fma(a[2], sum, sum);
+            }
+        }
+        __syncthreads();
+    }
+    if (FIN == FIN_PAP) reduce_finish<3, FIN_PAP>(a, red, st, ticket, blockIdx.x, gridDim.x);
+}
+
+// Warp tile of a substitution level: `nrows` (<= 32) consecutive rows from
+// `row0`, made of whole units (blocks); bit l of `mask` is set where lane l
+// starts a unit; `nsteps` is the longest unit.  Eight warp tiles form one CTA
+// tile (rows contiguous across them; empty ones pad the end of a level).
+struct WarpTile {
+    int row0;
+    int nrows;
+    unsigned int mask;
+    int nsteps;
+};
+
+// Forward (L y = r, FWD) or backward (L^T z = y) substitution over the CTA
+// tiles [ct0, ct1) of one level of a contiguous schedule.  Lane l owns row
+// i = row0 + l of its warp tile; its unit spans lanes [us, ue).
+//
+// Forward: the entries of row i with column below the unit's first row
+// (earlier levels, final) are applied first, fully in parallel -- they come
+// first in the reference's column order; the unit's own entries follow, one
+// step per row of the unit: at step s the lane with position s in its unit
+// applies its in-unit entries (their y values are in the shared tile) and
+// divides.  Backward: in-unit entries come first in column order, so at its
+// step (units run in descending row order) a lane applies its in-unit
+// entries from the shared tile, then the later-level entries, whose values
+// (and matrix entries) were fetched into registers before the steps began.
+// The operation order per row equals the reference's sequential sweep.
+template <class T, bool FWD, int KX, int FIN>
+__global__ void __launch_bounds__(256) k_sweep_tiled(int ct0, int ct1, const WarpTile* __restrict__ wt,
+                                                     const int* __restrict__ Sp, const int* __restrict__ Si,
+                                                     const T* __restrict__ Sx, const T* __restrict__ dg,
+                                                     int cap, const double* __restrict__ in, double* out,
+                                                     const double* __restrict__ rdot, int slot0, int nslots,
+                                                     SolverState* st, RedBuf red, unsigned int* ticket)
+{
+    if (st_done(st)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* s_y = reinterpret_cast<double*>(smem_raw);                       // 256 rows
+    T* s_val = reinterpret_cast<T*>(smem_raw + 256 * sizeof(double));
+    int* s_col = reinterpret_cast<int*>(smem_raw + 256 * sizeof(double) + (size_t)cap * sizeof(T));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    acc2 rz[1] = {{0.0, 0.0}};
+    for (int ct = ct0 + blockIdx.x; ct < ct1; ct += gridDim.x) {
+        // padding warp tiles start at the end row with nrows = 0
+        const int R0 = wt[(size_t)ct * 8].row0;
+        const WarpTile w7 = wt[(size_t)ct * 8 + 7];
+        const int R1 = w7.row0 + w7.nrows;
+        const int e0 = Sp[R0], e1 = Sp[R1];
+        const int ea = e0 & ~3;
+        stage_segment<T>(Si, Sx, ea, e1 - ea, s_col, s_val);
+        const WarpTile w = wt[(size_t)ct * 8 + warp];
+        const bool valid = lane < w.nrows;
+        const int i = w.row0 + lane;
+        // unit of this lane: lanes [us, ue)
+        const unsigned int below = w.mask & (0xffffffffu >> (31 - lane));
+        const int us = 31 - __clz(below);
+        const unsigned int above = w.mask & ~(0xffffffffu >> (31 - lane));
+        const int ue = above ? (__ffs(above) - 1) : w.nrows;
+        const int pos = FWD ? (lane - us) : (ue - 1 - lane);
+        const int urow0 = w.row0 + us, urow1 = w.row0 + ue;
+        double acc = 0.0, dv = 1.0;
+        int k = 0, ke = 0;
+        if (valid) {
+            acc = in[i];
+            dv = (double)dg[i];
+            k = Sp[i] - ea;
+            ke = Sp[i + 1] - ea;
+        }
+        __syncthreads();
+        double xv[KX > 0 ? KX : 1];
+        T lv[KX > 0 ? KX : 1];
+        int kin = k, nx = 0;
+        if (valid) {
+            if (FWD) {
+                // earlier-level entries: parallel part of the chain
+                while (k < ke && s_col[k] < urow0) {
+                    acc = fma(-(double)s_val[k], out[s_col[k]], acc);
+                    ++k;
+                }
+            } else {
+                while (kin < ke && s_col[kin] < urow1) ++kin;
+#pragma unroll
+                for (int q = 0; q < KX; ++q) {
+                    if (kin + q < ke) {
+                        lv[q] = s_val[kin + q];
+                        xv[q] = out[s_col[kin + q]];
+                        ++nx;
+                    }
+                }
+            }
+        }
+        double v = 0.0;
+        for (int s = 0; s < w.nsteps; ++s) {
+            if (valid && pos == s) {
+                if (FWD) {
+                    for (; k < ke; ++k) acc = fma(-(double)s_val[k], s_y[s_col[k] - R0], acc);
+                } else {
+                    for (int q = k; q < kin; ++q) acc = fma(-(double)s_val[q], s_y[s_col[q] - R0], acc);
+#pragma unroll
+                    for (int q = 0; q < KX; ++q)
+                        if (q < nx) acc = fma(-(double)lv[q], xv[q], acc);
+                    for (int q = kin + nx; q < ke; ++q) acc = fma(-(double)s_val[q], out[s_col[q]], acc);
+                }
+                v = acc / dv;
+                s_y[i - R0] = v;
+            }
+            __syncwarp();
+        }
+        if (valid) {
+            out[i] = v;
+            if (FIN != FIN_NONE) acc2_fma(rz[0], rdot[i], v);
+        }
+        __syncthreads();
+    }
+    if (FIN != FIN_NONE) reduce_finish<1, FIN>(rz, red, st, ticket, slot0 + blockIdx.x, nslots);
+}
+
+// ---------------------------------------------------------------------------
 // IC(0) factorisation of one level (ic0.cpp:56-115), one thread per unit,
 // rows of a unit in order.  Failures record (row << 34 | code << 32 | report
 // row) with atomicMin, so the smallest failing row -- the one the reference's

@@ -186,6 +186,12 @@ void* iccg_ctx_stream(iccg_ctx* ctx);
 long long iccg_ctx_launch_count(const iccg_ctx* ctx);
 /* bytes of device memory held by this context */
 long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
+/* context options: ICCG_OPT_TILED (default 1) selects the shared-memory
+   tiled SpMV and substitution kernels where the matrix and schedule allow
+   them; 0 forces the one-thread-per-row / per-block kernels.  Both give the
+   same bits. */
+#define ICCG_OPT_TILED 0
+int iccg_ctx_set_option(iccg_ctx* ctx, int option, long long value);
 
 /* Uploads A_run (the matrix conjugate_gradient runs on, cg_crs.cpp:442-447):
    full symmetric CRS with ascending columns.  Keeps an FP64 copy and, on
@@ -205,8 +211,10 @@ int iccg_schedule_none(iccg_ctx* ctx);
 /* Preconditioner construction: Identity(A) / Jacobi(A) / IC0(A, shift)
    (precond.hpp:10, precond.hpp:23-36, ic0.cpp:6-12).  IC(0) is factored on
    the device in the schedule's order.  auto_shift != 0: on a non-positive
-   pivot the factorisation restarts with shift = max(2*shift, 1e-12*max|a_ii|)
-   instead of failing (the reference throws, ic0.cpp:104-113).  The factor is
+   pivot the factorisation restarts with shift = max(2*shift, 1e-3*max|a_ii|)
+   (at most 40 restarts) instead of failing (the reference throws,
+   ic0.cpp:104-113).  The shift is added to every pivot, as the reference's
+   shift argument is (ic0.cpp:103).  The factor is
    stored in FP64 and, for FP32-storage solves, also rounded to FP32. */
 int iccg_precond_build(iccg_ctx* ctx, int kind, double shift, int auto_shift);
 /* the shift the last IC(0) build ended with */
