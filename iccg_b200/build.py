@@ -21,7 +21,7 @@ LIB = LIBDIR / "libiccg_b200.so"
 
 CUDA_SOURCES = ["ctx.cu"]
 HOST_SOURCES = ["host_order.cpp", "host_gen.cpp", "host_capi.cpp"]
-HEADERS = ["dd.cuh", "kernels.cuh", "host.hpp"]
+HEADERS = ["dd.cuh", "kernels.cuh", "host.hpp", "devbuf.hpp", "context.hpp", "plan.inl", "factor.inl", "qsys.inl", "solver.inl"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -65,7 +65,7 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     if cxx:
         cmd += ["-ccbin", cxx]
     cmd += [str(CSRC / s) for s in CUDA_SOURCES + HOST_SOURCES]
-    cmd += ["-o", str(LIB), "-lcudart"]
+    cmd += ["-o", str(LIB), "--cudart=static"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

@@ -1,0 +1,182 @@
+// context.hpp -- the device context behind iccg_ctx.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "devbuf.hpp"
+#include "kernels.cuh"
+
+namespace iccg {
+
+constexpr int kThreads = 256;
+
+// A substitution / factorisation schedule in A_run row numbering: levels of
+// independent units, each unit a sequence of rows done in order.
+struct Plan {
+    int nlevels = 0;
+    std::vector<int> level_ptr;  // units per level (host)
+    std::vector<int> grid;       // CTAs per level launch (simple kernels)
+    std::vector<int> slot0;      // first reduction slot of each launch
+    int nslots = 0;
+    bool unit_is_row = true;
+    Buf<int> unit_ptr, rows;
+    std::vector<int> h_unit_ptr, h_rows;
+};
+
+// IC(0) factor in the reference's layout (L rows, A_run numbering) plus the
+// strict-lower / strict-upper split used by the substitutions.
+struct Factor {
+    bool built = false;
+    int nnzL = 0;
+    double shift = 0.0;
+    std::vector<int> Lp, Li, dpos, Up, Ui, ut_src, Sp, Si, s_src, Tp, Ti, t_src;
+    Buf<int> dLp, dLi, ddpos;
+    Buf<double> dLx;
+    // simple-path arrays (A_run numbering)
+    Buf<int> dSp, dSi, dTp, dTi;
+    Buf<double> S64, T64, d64;
+    Buf<float> S32, T32, d32;
+    bool has32 = false;
+    void reset()
+    {
+        built = false;
+        has32 = false;
+        nnzL = 0;
+        shift = 0.0;
+        for (auto* v : {&Lp, &Li, &dpos, &Up, &Ui, &ut_src, &Sp, &Si, &s_src, &Tp, &Ti, &t_src}) v->clear();
+        for (auto* b : {&dLp, &dLi, &ddpos, &dSp, &dSi, &dTp, &dTi}) b->free();
+        for (auto* b : {&dLx, &S64, &T64, &d64}) b->free();
+        for (auto* b : {&S32, &T32, &d32}) b->free();
+    }
+};
+
+// A SELL-32 matrix over Q rows (see kernels.cuh, "Lane-interleaved kernels").
+struct SellDev {
+    Buf<int> ptr, col, len;
+    Buf<double> v64;
+    Buf<float> v32;
+    bool has32 = false;
+    long long slots = 0;
+    std::vector<int> src;  // host: CRS value index of each slot (-1: padding)
+    SellMat view(bool fp32) const
+    {
+        return SellMat{ptr.get(), col.get(), fp32 ? (const void*)v32.get() : (const void*)v64.get(), len.get()};
+    }
+    void reset()
+    {
+        for (auto* b : {&ptr, &col, &len}) b->free();
+        v64.free();
+        v32.free();
+        has32 = false;
+        slots = 0;
+        src.clear();
+    }
+};
+
+// The lane-interleaved device system.
+struct QSys {
+    bool ok = false;
+    int version = -1;         // schedule version it was built for
+    int factor_version = -1;  // factor build it holds
+    std::vector<int> q2r, r2q;
+    Buf<int> dq2r;
+    // sweep groups
+    int nlevels = 0, ngroups = 0;
+    std::vector<int> level_g;   // groups per level (nlevels+1)
+    std::vector<int> fgrid, bslot0;
+    int bnslots = 0;
+    Buf<int> gbase, glen, sl0;
+    std::vector<int> h_gbase, h_glen, h_sl0;
+    std::vector<std::pair<int, int>> steps;  // step slices: (first Q row, rows)
+    // matrices
+    SellDev A, S, T;
+    Buf<double> d64, inv_diag;
+    Buf<float> d32;
+    bool d32_ok = false;
+    void reset()
+    {
+        ok = false;
+        version = factor_version = -1;
+        q2r.clear();
+        r2q.clear();
+        dq2r.free();
+        nlevels = ngroups = 0;
+        level_g.clear();
+        fgrid.clear();
+        bslot0.clear();
+        bnslots = 0;
+        gbase.free();
+        glen.free();
+        sl0.free();
+        h_gbase.clear();
+        h_glen.clear();
+        h_sl0.clear();
+        steps.clear();
+        A.reset();
+        S.reset();
+        T.reset();
+        d64.free();
+        inv_diag.free();
+        d32.free();
+        d32_ok = false;
+    }
+};
+
+}  // namespace iccg
+
+struct iccg_ctx {
+    int device = 0;
+    int nsm = 148;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    long long launches = 0;
+    long long dev_bytes = 0;
+    // A_run
+    int n = 0, nnz = 0;
+    std::vector<int> h_rowptr, h_colind;
+    std::vector<double> h_val;
+    iccg::Buf<int> rowptr, colind;
+    iccg::Buf<double> val64;
+    iccg::Buf<float> val32;
+    bool has_val32 = false;
+    // schedule
+    int sched_kind = ICCG_SCHED_NONE;
+    int sched_version = 0;
+    iccg::Plan fwd, bwd;
+    // lane-interleaved system (default) or the simple one-thread-per-row path
+    bool use_q = true;
+    iccg::QSys Q;
+    // preconditioner
+    int pc_kind = -1;
+    int factor_version = 0;
+    iccg::Buf<double> inv_diag;
+    iccg::Factor F;
+    // vectors: A_run-order staging (vb, vx) and work vectors (path order)
+    iccg::Buf<double> vb, vx, qb, qx, vr, vp, vz, vy, vAp, vtmp;
+    // reductions / state
+    iccg::Buf<iccg::dd> partials;
+    iccg::Buf<unsigned int> ticket;
+    iccg::Buf<double> scalars;
+    iccg::Buf<iccg::SolverState> state;
+    iccg::Buf<unsigned long long> errword;
+    iccg::SolverState* h_state = nullptr;  // pinned
+    double* h_scalars = nullptr;           // pinned
+    int* h_status = nullptr;               // pinned, 2 slots
+    size_t partial_slots = 0;
+    // graph of the fused iteration
+    cudaGraphExec_t gexec = nullptr;
+    long long gkey = -1;
+    int gkernels = 0;
+    // events
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evs[2] = {nullptr, nullptr};
+    // profiling
+    bool profile = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
+    size_t ev_used = 0;
+    std::vector<int> ev_cls;
+    double prof_ms[5] = {0, 0, 0, 0, 0};
+    long long prof_n[5] = {0, 0, 0, 0, 0};
+};

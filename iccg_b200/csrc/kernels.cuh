@@ -374,66 +374,67 @@ __global__ void __launch_bounds__(256) k_sweep(SweepArgs a, int u0, int u1, int 
 }
 
 // ---------------------------------------------------------------------------
-// Tiled kernels.
+// Lane-interleaved kernels (the default path).
 //
-// A CTA tile is a range of at most 256 consecutive rows whose CSR entries
-// [rowptr[R0], rowptr[R1]) are contiguous in memory.  The CTA first copies
-// that segment (column indices and values) into shared memory with 16-byte
-// vector loads marked streaming (evict-first: the matrix is read once per
-// iteration and should not push the vectors out of L2), then one thread per
-// row runs the row's arithmetic from shared memory in the reference's order.
-// Segments start at the 4-entry boundary at or below rowptr[R0]; every
-// device array carries 16 entries of padding, so the rounded-up tail of the
-// last tile stays inside the allocation.
+// The device keeps the system in an internal row order Q built from the
+// schedule: within each level (color), the units (ABMC blocks; single rows
+// for MC and level sets) are taken 32 at a time, longest first, and their
+// rows are numbered (step r, unit u) -- the r-th row of every unit of the
+// group, then the (r+1)-th, ...  A warp owns a group and lane u owns unit u,
+// so one warp step advances 32 independent chains by one row each, and rows
+// of one step are consecutive.
+//
+// Matrices are stored as SELL-32 over Q: a slice holds up to 32 consecutive
+// Q rows, entry j of the slice's lane l at ptr[slice] + 32 j + l, so every
+// load of a warp step is one coalesced 128-byte line per array.  Each row
+// keeps the reference's entry order (column indices are relabelled to Q, not
+// re-sorted), so every row's chain of operations is the reference's and the
+// results keep its bits.  Vectors live in Q order; they are permuted only at
+// the API boundary.
 // ---------------------------------------------------------------------------
-template <class T>
-__device__ __forceinline__ void stage_segment(const int* __restrict__ gcol, const T* __restrict__ gval, int ea,
-                                              int cnt, int* s_col, T* s_val)
-{
-    const int nv = (cnt + 3) >> 2;  // 4-entry groups
-    const int4* c4 = reinterpret_cast<const int4*>(gcol + ea);
-    int4* sc4 = reinterpret_cast<int4*>(s_col);
-    for (int v = threadIdx.x; v < nv; v += blockDim.x) sc4[v] = __ldcs(c4 + v);
-    if (sizeof(T) == 4) {
-        const float4* v4 = reinterpret_cast<const float4*>(gval + ea);
-        float4* sv4 = reinterpret_cast<float4*>(s_val);
-        for (int v = threadIdx.x; v < nv; v += blockDim.x) sv4[v] = __ldcs(v4 + v);
-    } else {
-        const double2* v2 = reinterpret_cast<const double2*>(gval + ea);
-        double2* sv2 = reinterpret_cast<double2*>(s_val);
-        for (int v = threadIdx.x; v < 2 * nv; v += blockDim.x) sv2[v] = __ldcs(v2 + v);
-    }
-}
+struct SellMat {
+    const int* ptr;       // first slot of each slice
+    const int* col;       // column (Q index) per slot
+    const void* val;      // value per slot (float or double)
+    const int* len;       // entries of each Q row
+};
 
-// SpMV over CTA tiles (tile_row: ntiles+1 row boundaries); same arithmetic as
-// k_spmv.  Dynamic shared memory: cap * (4 + sizeof(T)) bytes.
+// y = A x over regular 32-row slices (slice s = Q rows [32 s, 32 s + 32)),
+// product and sum rounded separately as in spmv (cg_crs.cpp:73-75).
 template <class T, int FIN>
-__global__ void __launch_bounds__(256) k_spmv_tiled(int ntiles, const int* __restrict__ tile_row,
-                                                    const int* __restrict__ rp, const int* __restrict__ ci,
-                                                    const T* __restrict__ v, int cap,
-                                                    const double* __restrict__ x, double* __restrict__ y,
-                                                    SolverState* st, RedBuf red, unsigned int* ticket)
+__global__ void __launch_bounds__(256) k_spmv_q(int n, SellMat A, const double* __restrict__ x,
+                                                double* __restrict__ y, SolverState* st, RedBuf red,
+                                                unsigned int* ticket)
 {
     if (st_done(st)) return;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* s_val = reinterpret_cast<T*>(smem_raw);
-    int* s_col = reinterpret_cast<int*>(smem_raw + (size_t)cap * sizeof(T));
+    const T* __restrict__ val = (const T*)A.val;
+    const int* __restrict__ col = A.col;
     acc2 a[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int R0 = tile_row[t], R1 = tile_row[t + 1];
-        const int e0 = rp[R0], e1 = rp[R1];
-        const int ea = e0 & ~3;
-        stage_segment<T>(ci, v, ea, e1 - ea, s_col, s_val);
-        const int i = R0 + threadIdx.x;
-        int rs = 0, re = 0;
-        if (i < R1) {
-            rs = rp[i] - ea;
-            re = rp[i + 1] - ea;
-        }
-        __syncthreads();
-        if (i < R1) {
+    const int lane = threadIdx.x & 31;
+    const int nslices = (n + 31) >> 5;
+    for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nslices; s += (gridDim.x * blockDim.x) >> 5) {
+        const int i = (s << 5) + lane;
+        if (i < n) {
+            const int L = A.len[i];
+            const int p0 = A.ptr[s] + lane;
             double sum = 0.0;
-            for (int k = rs; k < re; ++k) sum = sum + (double)s_val[k] * __ldg(x + s_col[k]);
+            int j = 0;
+            for (; j + 4 <= L; j += 4) {
+                const int pa = p0 + 32 * j;
+                const int c0 = __ldcs(col + pa), c1 = __ldcs(col + pa + 32), c2 = __ldcs(col + pa + 64),
+                          c3 = __ldcs(col + pa + 96);
+                const double v0 = (double)__ldcs(val + pa), v1 = (double)__ldcs(val + pa + 32),
+                             v2 = (double)__ldcs(val + pa + 64), v3 = (double)__ldcs(val + pa + 96);
+                const double x0 = __ldg(x + c0), x1 = __ldg(x + c1), x2 = __ldg(x + c2), x3 = __ldg(x + c3);
+                sum = sum + v0 * x0;
+                sum = sum + v1 * x1;
+                sum = sum + v2 * x2;
+                sum = sum + v3 * x3;
+            }
+            for (; j < L; ++j) {
+                const int pa = p0 + 32 * j;
+                sum = sum + (double)__ldcs(val + pa) * __ldg(x + __ldcs(col + pa));
+            }
             y[i] = sum;
             if (FIN == FIN_PAP) {
                 const double xi = __ldg(x + i);
@@ -442,124 +443,118 @@ __global__ void __launch_bounds__(256) k_spmv_tiled(int ntiles, const int* __res
                 acc2_fma(a[2], sum, sum);
             }
         }
-        __syncthreads();
     }
     if (FIN == FIN_PAP) reduce_finish<3, FIN_PAP>(a, red, st, ticket, blockIdx.x, gridDim.x);
 }
 
-// Warp tile of a substitution level: `nrows` (<= 32) consecutive rows from
-// `row0`, made of whole units (blocks); bit l of `mask` is set where lane l
-// starts a unit; `nsteps` is the longest unit.  Eight warp tiles form one CTA
-// tile (rows contiguous across them; empty ones pad the end of a level).
-struct WarpTile {
-    int row0;
-    int nrows;
-    unsigned int mask;
-    int nsteps;
-};
-
-// Forward (L y = r, FWD) or backward (L^T z = y) substitution over the CTA
-// tiles [ct0, ct1) of one level of a contiguous schedule.  Lane l owns row
-// i = row0 + l of its warp tile; its unit spans lanes [us, ue).
-//
-// Forward: the entries of row i with column below the unit's first row
-// (earlier levels, final) are applied first, fully in parallel -- they come
-// first in the reference's column order; the unit's own entries follow, one
-// step per row of the unit: at step s the lane with position s in its unit
-// applies its in-unit entries (their y values are in the shared tile) and
-// divides.  Backward: in-unit entries come first in column order, so at its
-// step (units run in descending row order) a lane applies its in-unit
-// entries from the shared tile, then the later-level entries, whose values
-// (and matrix entries) were fetched into registers before the steps began.
-// The operation order per row equals the reference's sequential sweep.
-template <class T, bool FWD, int KX, int FIN>
-__global__ void __launch_bounds__(256) k_sweep_tiled(int ct0, int ct1, const WarpTile* __restrict__ wt,
-                                                     const int* __restrict__ Sp, const int* __restrict__ Si,
-                                                     const T* __restrict__ Sx, const T* __restrict__ dg,
-                                                     int cap, const double* __restrict__ in, double* out,
-                                                     const double* __restrict__ rdot, int slot0, int nslots,
-                                                     SolverState* st, RedBuf red, unsigned int* ticket)
+// r = b - A x with the FP64 matrix in Q order (FIN_INIT: b.b and r.r;
+// FIN_TRUE: residual replacement when requested, r.r).
+template <int FIN>
+__global__ void __launch_bounds__(256) k_residual_q(int n, SellMat A, const double* __restrict__ x,
+                                                    const double* __restrict__ b, double* __restrict__ r,
+                                                    SolverState* st, RedBuf red, unsigned int* ticket)
 {
     if (st_done(st)) return;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* s_y = reinterpret_cast<double*>(smem_raw);                       // 256 rows
-    T* s_val = reinterpret_cast<T*>(smem_raw + 256 * sizeof(double));
-    int* s_col = reinterpret_cast<int*>(smem_raw + 256 * sizeof(double) + (size_t)cap * sizeof(T));
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (FIN == FIN_TRUE && *(volatile int*)&st->rr_flag == 0) return;
+    const double* __restrict__ val = (const double*)A.val;
+    acc2 a[2] = {{0.0, 0.0}, {0.0, 0.0}};
+    const int lane = threadIdx.x & 31;
+    const int nslices = (n + 31) >> 5;
+    for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nslices; s += (gridDim.x * blockDim.x) >> 5) {
+        const int i = (s << 5) + lane;
+        if (i < n) {
+            const int L = A.len[i];
+            const int p0 = A.ptr[s] + lane;
+            double sum = 0.0;
+            for (int j = 0; j < L; ++j) {
+                const int pa = p0 + 32 * j;
+                sum = sum + __ldcs(val + pa) * __ldg(x + __ldcs(A.col + pa));
+            }
+            const double bi = b[i];
+            const double ri = bi - sum;
+            r[i] = ri;
+            if (FIN == FIN_INIT) {
+                acc2_fma(a[0], bi, bi);
+                acc2_fma(a[1], ri, ri);
+            }
+            if (FIN == FIN_TRUE) acc2_fma(a[0], ri, ri);
+        }
+    }
+    if (FIN == FIN_INIT) reduce_finish<2, FIN_INIT>(a, red, st, ticket, blockIdx.x, gridDim.x);
+    if (FIN == FIN_TRUE) {
+        acc2 t[1] = {a[0]};
+        reduce_finish<1, FIN_TRUE>(t, red, st, ticket, blockIdx.x, gridDim.x);
+    }
+}
+
+// One level of a substitution sweep in Q order.  Group g (a warp) holds up
+// to 32 units; lane u's unit has glen[32 g + u] rows (lanes sorted by
+// length, longest first, so the active lanes of step r are a prefix and the
+// rows of step r are Q rows gbase[g] + off_r + [0, cnt_r)).  Slice
+// sl0[g] + r of M holds the entries of step r's rows.  Forward steps run
+// r = 0, 1, ...; backward steps run the units' rows in reverse.  Row q:
+//     out_q = (in_q - sum_k M_qk out_{c_k}) / d_q
+// with the sum a chain of fused multiply-adds in the reference's entry order
+// (ic0.cpp:201-214, 229-244, 280-295, 319-334).  Earlier-level values come
+// from global memory; in-unit values were written by the same lane at an
+// earlier step (the value of the row just before is kept in a register).
+template <class T, bool FWD, int FIN>
+__global__ void __launch_bounds__(256) k_sweep_q(int g0, int g1, const int* __restrict__ gbase,
+                                                 const int* __restrict__ glen, const int* __restrict__ sl0,
+                                                 SellMat M, const T* __restrict__ dg,
+                                                 const double* __restrict__ in, double* out,
+                                                 const double* __restrict__ rdot, int slot0, int nslots,
+                                                 SolverState* st, RedBuf red, unsigned int* ticket)
+{
+    if (st_done(st)) return;
+    const T* __restrict__ val = (const T*)M.val;
+    const int* __restrict__ col = M.col;
+    const int lane = threadIdx.x & 31;
     acc2 rz[1] = {{0.0, 0.0}};
-    for (int ct = ct0 + blockIdx.x; ct < ct1; ct += gridDim.x) {
-        // padding warp tiles start at the end row with nrows = 0
-        const int R0 = wt[(size_t)ct * 8].row0;
-        const WarpTile w7 = wt[(size_t)ct * 8 + 7];
-        const int R1 = w7.row0 + w7.nrows;
-        const int e0 = Sp[R0], e1 = Sp[R1];
-        const int ea = e0 & ~3;
-        stage_segment<T>(Si, Sx, ea, e1 - ea, s_col, s_val);
-        const WarpTile w = wt[(size_t)ct * 8 + warp];
-        const bool valid = lane < w.nrows;
-        const int i = w.row0 + lane;
-        // unit of this lane: lanes [us, ue)
-        const unsigned int below = w.mask & (0xffffffffu >> (31 - lane));
-        const int us = 31 - __clz(below);
-        const unsigned int above = w.mask & ~(0xffffffffu >> (31 - lane));
-        const int ue = above ? (__ffs(above) - 1) : w.nrows;
-        const int pos = FWD ? (lane - us) : (ue - 1 - lane);
-        const int urow0 = w.row0 + us, urow1 = w.row0 + ue;
-        double acc = 0.0, dv = 1.0;
-        int k = 0, ke = 0;
-        if (valid) {
-            acc = in[i];
-            dv = (double)dg[i];
-            k = Sp[i] - ea;
-            ke = Sp[i + 1] - ea;
-        }
-        __syncthreads();
-        double xv[KX > 0 ? KX : 1];
-        T lv[KX > 0 ? KX : 1];
-        int kin = k, nx = 0;
-        if (valid) {
-            if (FWD) {
-                // earlier-level entries: parallel part of the chain
-                while (k < ke && s_col[k] < urow0) {
-                    acc = fma(-(double)s_val[k], out[s_col[k]], acc);
-                    ++k;
+    for (int g = g0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5); g < g1;
+         g += (gridDim.x * blockDim.x) >> 5) {
+        const int len = glen[(size_t)g * 32 + lane];
+        const int base = gbase[g];
+        const int s0 = sl0[g];
+        const int maxlen = __reduce_max_sync(0xffffffffu, (unsigned)len);
+        int prev_q = -1;
+        double prev_v = 0.0;
+        for (int t = 0; t < maxlen; ++t) {
+            const int r = FWD ? t : (maxlen - 1 - t);
+            const int off = (int)__reduce_add_sync(0xffffffffu, (unsigned)min(len, r));
+            if (r < len) {
+                const int q = base + off + lane;
+                const int p0 = M.ptr[s0 + r] + lane;
+                const int L = M.len[q];
+                double acc = in[q];
+                for (int j = 0; j < L; ++j) {
+                    const int pa = p0 + 32 * j;
+                    const int c = col[pa];
+                    const double xv = (c == prev_q) ? prev_v : out[c];
+                    acc = fma(-(double)val[pa], xv, acc);
                 }
-            } else {
-                while (kin < ke && s_col[kin] < urow1) ++kin;
-#pragma unroll
-                for (int q = 0; q < KX; ++q) {
-                    if (kin + q < ke) {
-                        lv[q] = s_val[kin + q];
-                        xv[q] = out[s_col[kin + q]];
-                        ++nx;
-                    }
-                }
+                const double v = acc / (double)dg[q];
+                out[q] = v;
+                prev_q = q;
+                prev_v = v;
+                if (FIN != FIN_NONE) acc2_fma(rz[0], rdot[q], v);
             }
         }
-        double v = 0.0;
-        for (int s = 0; s < w.nsteps; ++s) {
-            if (valid && pos == s) {
-                if (FWD) {
-                    for (; k < ke; ++k) acc = fma(-(double)s_val[k], s_y[s_col[k] - R0], acc);
-                } else {
-                    for (int q = k; q < kin; ++q) acc = fma(-(double)s_val[q], s_y[s_col[q] - R0], acc);
-#pragma unroll
-                    for (int q = 0; q < KX; ++q)
-                        if (q < nx) acc = fma(-(double)lv[q], xv[q], acc);
-                    for (int q = kin + nx; q < ke; ++q) acc = fma(-(double)s_val[q], out[s_col[q]], acc);
-                }
-                v = acc / dv;
-                s_y[i - R0] = v;
-            }
-            __syncwarp();
-        }
-        if (valid) {
-            out[i] = v;
-            if (FIN != FIN_NONE) acc2_fma(rz[0], rdot[i], v);
-        }
-        __syncthreads();
     }
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(rz, red, st, ticket, slot0 + blockIdx.x, nslots);
+}
+
+// out[q] = in[perm[q]] (gather into Q order) / out[perm[q]] = in[q] (scatter)
+__global__ void __launch_bounds__(256) k_gather_vec(int n, const int* __restrict__ perm,
+                                                    const double* __restrict__ in, double* __restrict__ out)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) out[q] = in[perm[q]];
+}
+
+__global__ void __launch_bounds__(256) k_scatter_vec(int n, const int* __restrict__ perm,
+                                                     const double* __restrict__ in, double* __restrict__ out)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) out[perm[q]] = in[q];
 }
 
 // ---------------------------------------------------------------------------
@@ -633,6 +628,17 @@ __global__ void __launch_bounds__(256) k_gather(long long m, const int* __restri
 {
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < m; k += (long long)gridDim.x * blockDim.x)
         out[k] = (T)src[idx[k]];
+}
+
+// out[k] = (T) src[idx[k]], 0 where idx[k] < 0 (SELL padding)
+template <class T>
+__global__ void __launch_bounds__(256) k_gather_pad(long long m, const int* __restrict__ idx,
+                                                    const double* __restrict__ src, T* __restrict__ out)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < m; k += (long long)gridDim.x * blockDim.x) {
+        const int i = idx[k];
+        out[k] = i >= 0 ? (T)src[i] : (T)0;
+    }
 }
 
 __global__ void __launch_bounds__(256) k_to_f32(long long m, const double* __restrict__ src, float* __restrict__ out)

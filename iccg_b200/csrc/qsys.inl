@@ -1,0 +1,201 @@
+// qsys.inl -- the lane-interleaved (Q-ordered) device system (included by
+// ctx.cu inside namespace iccg).
+//
+// Q order from the forward plan: level by level; the level's units sorted by
+// length, longest first (stable); groups of 32 consecutive units; inside a
+// group the rows (step r, unit u) in r-major order.  Lane u of a warp owns
+// unit u, so the active lanes of every step are a prefix and the rows of a
+// step are consecutive Q rows.  The backward sweep runs the same groups with
+// levels and steps reversed, which is a valid order because every backward
+// dependency is a forward dependency reversed.
+
+static void sell_build(iccg_ctx* c, const std::vector<std::pair<int, int>>& slices, const std::vector<int>& rp,
+                       const std::vector<int>& ci, const std::vector<int>* src_map, SellDev& M)
+{
+    const QSys& Q = c->Q;
+    const int n = (int)Q.q2r.size();
+    std::vector<int> ptr(slices.size() + 1), len((size_t)n, 0);
+    long long slot = 0;
+    for (size_t s = 0; s < slices.size(); ++s) {
+        if (slot > 2147483647LL) throw Error(ICCG_ERR_ARG, "matrix too large for int32 SELL slots");
+        ptr[s] = (int)slot;
+        int w = 0;
+        for (int l = 0; l < slices[s].second; ++l) {
+            const int r = Q.q2r[(size_t)(slices[s].first + l)];
+            w = std::max(w, rp[(size_t)r + 1] - rp[(size_t)r]);
+        }
+        slot += 32LL * w;
+    }
+    if (slot > 2147483647LL) throw Error(ICCG_ERR_ARG, "matrix too large for int32 SELL slots");
+    ptr[slices.size()] = (int)slot;
+    std::vector<int> col((size_t)slot, 0);
+    M.src.assign((size_t)slot, -1);
+    for (size_t s = 0; s < slices.size(); ++s)
+        for (int l = 0; l < slices[s].second; ++l) {
+            const int q = slices[s].first + l;
+            const int r = Q.q2r[(size_t)q];
+            const int b = rp[(size_t)r], L = rp[(size_t)r + 1] - b;
+            len[(size_t)q] = L;
+            for (int j = 0; j < L; ++j) {
+                const size_t pos = (size_t)ptr[s] + 32 * (size_t)j + (size_t)l;
+                col[pos] = Q.r2q[(size_t)ci[(size_t)b + j]];
+                M.src[pos] = src_map ? (*src_map)[(size_t)b + j] : b + j;
+            }
+        }
+    M.ptr.upload(ptr.data(), ptr.size(), &c->dev_bytes, c->stream);
+    M.col.upload(col.data(), col.size(), &c->dev_bytes, c->stream);
+    M.len.upload(len.data(), len.size(), &c->dev_bytes, c->stream);
+    M.slots = slot;
+    M.has32 = false;
+    M.v32.free();
+    CK(cudaStreamSynchronize(c->stream));
+}
+
+// M.v64[slot] = src[M.src[slot]] (0 on padding)
+static void sell_values(iccg_ctx* c, SellDev& M, const double* src)
+{
+    Buf<int> idx;
+    idx.upload(M.src.data(), M.src.size(), &c->dev_bytes, c->stream);
+    M.v64.alloc((size_t)M.slots, &c->dev_bytes);
+    if (M.slots)
+        launch(c, 3, k_gather_pad<double>, grid_for(c, M.slots), kThreads, (long long)M.slots,
+               (const int*)idx.get(), src, M.v64.get());
+    CK(cudaStreamSynchronize(c->stream));
+    M.has32 = false;
+}
+
+static void sell_f32(iccg_ctx* c, SellDev& M)
+{
+    if (M.has32) return;
+    M.v32.alloc((size_t)M.slots, &c->dev_bytes);
+    if (M.slots)
+        launch(c, 3, k_to_f32, grid_for(c, M.slots), kThreads, (long long)M.slots, (const double*)M.v64.get(),
+               M.v32.get());
+    CK(cudaStreamSynchronize(c->stream));
+    M.has32 = true;
+}
+
+static void build_q_order(iccg_ctx* c)
+{
+    QSys& Q = c->Q;
+    const Plan& P = c->fwd;
+    Q.q2r.clear();
+    Q.q2r.reserve((size_t)c->n);
+    Q.level_g.assign(1, 0);
+    Q.h_gbase.clear();
+    Q.h_glen.clear();
+    Q.h_sl0.clear();
+    Q.steps.clear();
+    struct U { int t0, m; };
+    std::vector<U> units;
+    for (int l = 0; l < P.nlevels; ++l) {
+        units.clear();
+        for (int u = P.level_ptr[(size_t)l]; u < P.level_ptr[(size_t)l + 1]; ++u) {
+            const int t0 = P.unit_is_row ? u : P.h_unit_ptr[(size_t)u];
+            const int t1 = P.unit_is_row ? u + 1 : P.h_unit_ptr[(size_t)u + 1];
+            if (t1 > t0) units.push_back({t0, t1 - t0});
+        }
+        std::stable_sort(units.begin(), units.end(), [](const U& a, const U& b) { return a.m > b.m; });
+        for (size_t g0 = 0; g0 < units.size(); g0 += 32) {
+            const size_t g1 = std::min(units.size(), g0 + 32);
+            Q.h_gbase.push_back((int)Q.q2r.size());
+            Q.h_sl0.push_back((int)Q.steps.size());
+            for (size_t u = g0; u < g0 + 32; ++u) Q.h_glen.push_back(u < g1 ? units[u].m : 0);
+            const int maxlen = units[g0].m;
+            for (int r = 0; r < maxlen; ++r) {
+                int cnt = 0;
+                while (g0 + (size_t)cnt < g1 && units[g0 + (size_t)cnt].m > r) ++cnt;
+                Q.steps.emplace_back((int)Q.q2r.size(), cnt);
+                for (int u = 0; u < cnt; ++u) Q.q2r.push_back(P.h_rows[(size_t)(units[g0 + (size_t)u].t0 + r)]);
+            }
+        }
+        Q.level_g.push_back((int)Q.h_gbase.size());
+    }
+    if ((int)Q.q2r.size() != c->n) throw Error(ICCG_ERR_SCHEDULE, "schedule does not cover every row once");
+    Q.h_gbase.push_back((int)Q.q2r.size());
+    Q.r2q.assign((size_t)c->n, -1);
+    for (int q = 0; q < c->n; ++q) Q.r2q[(size_t)Q.q2r[(size_t)q]] = q;
+    Q.nlevels = P.nlevels;
+    Q.ngroups = (int)Q.h_sl0.size();
+    Q.fgrid.assign((size_t)Q.nlevels, 1);
+    Q.bslot0.assign((size_t)Q.nlevels, 0);
+    const int cap = c->nsm * 8;
+    for (int l = 0; l < Q.nlevels; ++l) {
+        const int groups = Q.level_g[(size_t)l + 1] - Q.level_g[(size_t)l];
+        Q.fgrid[(size_t)l] = std::max(1, std::min(cap, (groups + 7) / 8));  // 8 warps per CTA
+    }
+    int s = 0;
+    for (int l = Q.nlevels - 1; l >= 0; --l) {
+        Q.bslot0[(size_t)l] = s;
+        s += Q.fgrid[(size_t)l];
+    }
+    Q.bnslots = s;
+    ensure_partials(c, (size_t)std::max(s, 1));
+    Q.dq2r.upload(Q.q2r.data(), Q.q2r.size(), &c->dev_bytes, c->stream);
+    Q.gbase.upload(Q.h_gbase.data(), Q.h_gbase.size(), &c->dev_bytes, c->stream);
+    Q.glen.upload(Q.h_glen.data(), Q.h_glen.size(), &c->dev_bytes, c->stream);
+    Q.sl0.upload(Q.h_sl0.data(), Q.h_sl0.size(), &c->dev_bytes, c->stream);
+    // A_run in Q order, regular 32-row slices
+    std::vector<std::pair<int, int>> sl;
+    for (int q = 0; q < c->n; q += 32) sl.emplace_back(q, std::min(32, c->n - q));
+    sell_build(c, sl, c->h_rowptr, c->h_colind, nullptr, Q.A);
+    sell_values(c, Q.A, c->val64.get());
+}
+
+static void build_q_factor(iccg_ctx* c)
+{
+    QSys& Q = c->Q;
+    Factor& F = c->F;
+    sell_build(c, Q.steps, F.Sp, F.Si, &F.s_src, Q.S);
+    sell_values(c, Q.S, F.dLx.get());
+    sell_build(c, Q.steps, F.Tp, F.Ti, &F.t_src, Q.T);
+    sell_values(c, Q.T, F.dLx.get());
+    std::vector<int> dsrc((size_t)c->n);
+    for (int q = 0; q < c->n; ++q) dsrc[(size_t)q] = F.dpos[(size_t)Q.q2r[(size_t)q]];
+    Buf<int> idx;
+    idx.upload(dsrc.data(), dsrc.size(), &c->dev_bytes, c->stream);
+    Q.d64.alloc((size_t)c->n, &c->dev_bytes);
+    launch(c, 3, k_gather<double>, grid_for(c, c->n), kThreads, (long long)c->n, (const int*)idx.get(),
+           (const double*)F.dLx.get(), Q.d64.get());
+    CK(cudaStreamSynchronize(c->stream));
+    Q.d32_ok = false;
+}
+
+static void ensure_q(iccg_ctx* c)
+{
+    QSys& Q = c->Q;
+    if (!Q.ok || Q.version != c->sched_version) {
+        Q.reset();
+        build_q_order(c);
+        Q.version = c->sched_version;
+        Q.ok = true;
+    }
+    if (Q.factor_version != c->factor_version) {
+        // a new preconditioner since the last build
+        if (c->pc_kind == ICCG_PRECOND_IC0 && c->F.built) build_q_factor(c);
+        if (c->pc_kind == ICCG_PRECOND_JACOBI) {
+            Q.inv_diag.alloc((size_t)c->n, &c->dev_bytes);
+            launch(c, 3, k_gather<double>, grid_for(c, c->n), kThreads, (long long)c->n, (const int*)Q.dq2r.get(),
+                   (const double*)c->inv_diag.get(), Q.inv_diag.get());
+            CK(cudaStreamSynchronize(c->stream));
+        }
+        Q.factor_version = c->factor_version;
+    }
+}
+
+static void ensure_q32(iccg_ctx* c)
+{
+    QSys& Q = c->Q;
+    sell_f32(c, Q.A);
+    if (c->pc_kind == ICCG_PRECOND_IC0 && c->F.built) {
+        sell_f32(c, Q.S);
+        sell_f32(c, Q.T);
+        if (!Q.d32_ok) {
+            Q.d32.alloc((size_t)c->n, &c->dev_bytes);
+            launch(c, 3, k_to_f32, grid_for(c, c->n), kThreads, (long long)c->n, (const double*)Q.d64.get(),
+                   Q.d32.get());
+            CK(cudaStreamSynchronize(c->stream));
+            Q.d32_ok = true;
+        }
+    }
+}

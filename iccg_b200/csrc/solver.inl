@@ -1,0 +1,398 @@
+// solver.inl -- kernel dispatch on the active path and the CG drivers
+// (included by ctx.cu inside namespace iccg).
+//
+// Two paths compute the same bits: the lane-interleaved path (c->use_q,
+// default; vectors in Q order, SELL-32 matrices) and the simple path (A_run
+// order, one thread per row / per unit on CRS arrays).  The drivers below
+// take vectors already in the active path's order.
+
+// --- simple-path substitutions -------------------------------------------
+template <class T, int FIN>
+static void apply_ic0_simple(iccg_ctx* c, const double* r, double* y, double* z, SolverState* st)
+{
+    Factor& F = c->F;
+    const bool f32 = std::is_same<T, float>::value;
+    RedBuf red{c->partials.get(), c->scalars.get()};
+    SweepArgs a{};
+    a.unit_ptr = c->fwd.unit_is_row ? nullptr : c->fwd.unit_ptr.get();
+    a.rows = c->fwd.rows.get();
+    a.Sp = F.dSp.get();
+    a.Si = F.dSi.get();
+    a.Sx = f32 ? (const void*)F.S32.get() : (const void*)F.S64.get();
+    a.d = f32 ? (const void*)F.d32.get() : (const void*)F.d64.get();
+    a.in = r;
+    a.out = y;
+    for (int l = 0; l < c->fwd.nlevels; ++l) {
+        const int u0 = c->fwd.level_ptr[(size_t)l], u1 = c->fwd.level_ptr[(size_t)l + 1];
+        launch(c, 1, k_sweep<T, FIN_NONE>, c->fwd.grid[(size_t)l], kThreads, a, u0, u1, 0, 0, st, red,
+               c->ticket.get());
+    }
+    SweepArgs b = a;
+    b.unit_ptr = c->bwd.unit_is_row ? nullptr : c->bwd.unit_ptr.get();
+    b.rows = c->bwd.rows.get();
+    b.Sp = F.dTp.get();
+    b.Si = F.dTi.get();
+    b.Sx = f32 ? (const void*)F.T32.get() : (const void*)F.T64.get();
+    b.in = y;
+    b.out = z;
+    b.rdot = r;
+    for (int l = 0; l < c->bwd.nlevels; ++l) {
+        const int u0 = c->bwd.level_ptr[(size_t)l], u1 = c->bwd.level_ptr[(size_t)l + 1];
+        launch(c, 2, k_sweep<T, FIN>, c->bwd.grid[(size_t)l], kThreads, b, u0, u1, c->bwd.slot0[(size_t)l],
+               c->bwd.nslots, st, red, c->ticket.get());
+    }
+}
+
+// --- lane-interleaved substitutions -----------------------------------------
+template <class T, int FIN>
+static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, SolverState* st)
+{
+    QSys& Q = c->Q;
+    const bool f32 = std::is_same<T, float>::value;
+    RedBuf red{c->partials.get(), c->scalars.get()};
+    const T* d = f32 ? (const T*)(const void*)Q.d32.get() : (const T*)(const void*)Q.d64.get();
+    const SellMat S = Q.S.view(f32), U = Q.T.view(f32);
+    for (int l = 0; l < Q.nlevels; ++l)
+        launch(c, 1, k_sweep_q<T, true, FIN_NONE>, Q.fgrid[(size_t)l], kThreads, Q.level_g[(size_t)l],
+               Q.level_g[(size_t)l + 1], (const int*)Q.gbase.get(), (const int*)Q.glen.get(),
+               (const int*)Q.sl0.get(), S, d, r, y, (const double*)nullptr, 0, 0, st, red, c->ticket.get());
+    for (int l = Q.nlevels - 1; l >= 0; --l)
+        launch(c, 2, k_sweep_q<T, false, FIN>, Q.fgrid[(size_t)l], kThreads, Q.level_g[(size_t)l],
+               Q.level_g[(size_t)l + 1], (const int*)Q.gbase.get(), (const int*)Q.glen.get(),
+               (const int*)Q.sl0.get(), U, d, (const double*)y, z, r, Q.bslot0[(size_t)l], Q.bnslots, st, red,
+               c->ticket.get());
+}
+
+// z = M^{-1} r (IC0::apply, ic0.cpp:366-393; Identity / Jacobi apply)
+template <int FIN>
+static void apply_path(iccg_ctx* c, int storage, const double* r, double* z, SolverState* st)
+{
+    RedBuf red{c->partials.get(), c->scalars.get()};
+    const bool f32 = storage == ICCG_STORE_FP32;
+    if (c->pc_kind == ICCG_PRECOND_IC0) {
+        if (c->use_q) {
+            if (f32) apply_ic0_q<float, FIN>(c, r, c->vy.get(), z, st);
+            else apply_ic0_q<double, FIN>(c, r, c->vy.get(), z, st);
+        } else {
+            if (f32) apply_ic0_simple<float, FIN>(c, r, c->vy.get(), z, st);
+            else apply_ic0_simple<double, FIN>(c, r, c->vy.get(), z, st);
+        }
+        return;
+    }
+    const double* inv = nullptr;
+    if (c->pc_kind == ICCG_PRECOND_JACOBI) inv = c->use_q ? c->Q.inv_diag.get() : c->inv_diag.get();
+    launch(c, 3, k_diag_apply<FIN>, grid_for(c, c->n), kThreads, c->n, inv, r, z, st, red, c->ticket.get());
+}
+
+// y = A x (spmv, cg_crs.cpp:54-79); FIN_PAP adds p.Ap, p.p, Ap.Ap
+template <int FIN>
+static void spmv_path(iccg_ctx* c, int storage, const double* x, double* y, SolverState* st)
+{
+    RedBuf red{c->partials.get(), c->scalars.get()};
+    const bool f32 = storage == ICCG_STORE_FP32;
+    const int g = grid_for(c, c->n);
+    if (c->use_q) {
+        const SellMat A = c->Q.A.view(f32);
+        if (f32) launch(c, 0, k_spmv_q<float, FIN>, g, kThreads, c->n, A, x, y, st, red, c->ticket.get());
+        else launch(c, 0, k_spmv_q<double, FIN>, g, kThreads, c->n, A, x, y, st, red, c->ticket.get());
+        return;
+    }
+    const int* rp = c->rowptr.get();
+    const int* ci = c->colind.get();
+    if (f32)
+        launch(c, 0, k_spmv<float, FIN>, g, kThreads, c->n, rp, ci, (const float*)c->val32.get(), x, y, st, red,
+               c->ticket.get());
+    else
+        launch(c, 0, k_spmv<double, FIN>, g, kThreads, c->n, rp, ci, (const double*)c->val64.get(), x, y, st, red,
+               c->ticket.get());
+}
+
+// r = b - A x with the FP64 matrix
+template <int FIN>
+static void residual_path(iccg_ctx* c, const double* x, const double* b, double* r, SolverState* st)
+{
+    RedBuf red{c->partials.get(), c->scalars.get()};
+    const int g = grid_for(c, c->n);
+    if (c->use_q)
+        launch(c, 4, k_residual_q<FIN>, g, kThreads, c->n, c->Q.A.view(false), x, b, r, st, red, c->ticket.get());
+    else
+        launch(c, 4, k_residual<FIN>, g, kThreads, c->n, (const int*)c->rowptr.get(), (const int*)c->colind.get(),
+               (const double*)c->val64.get(), x, b, r, st, red, c->ticket.get());
+}
+
+// makes the arrays of the active path ready (outside graph capture)
+static void prepare_path(iccg_ctx* c, int storage)
+{
+    if (c->use_q) {
+        ensure_q(c);
+        if (storage == ICCG_STORE_FP32) ensure_q32(c);
+    } else if (storage == ICCG_STORE_FP32) {
+        ensure_val32(c);
+        if (c->pc_kind == ICCG_PRECOND_IC0) ensure_factor32(c);
+    }
+}
+
+static double dot_dev(iccg_ctx* c, int n, const double* a, const double* b)
+{
+    ensure_partials(c, (size_t)grid_for(c, n));
+    RedBuf red{c->partials.get(), c->scalars.get()};
+    launch(c, 3, k_dot, grid_for(c, n), kThreads, n, a, b, red, c->ticket.get());
+    CK(cudaMemcpyAsync(c->h_scalars, c->scalars.get(), sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return c->h_scalars[0];
+}
+
+// ---------------------------------------------------------------------------
+// plain FP64 CG (cg_crs.cpp:89-162): one kernel per reference operation, the
+// scalar logic on the host after reading each reduction back.
+// ---------------------------------------------------------------------------
+static void solve_plain(iccg_ctx* c, const double* b, double* x, int max_iter, double tol, iccg_result* res)
+{
+    const int n = c->n;
+    double* r = c->vr.get();
+    double* p = c->vp.get();
+    double* z = c->vz.get();
+    double* Ap = c->vAp.get();
+    double* Ax = c->vtmp.get();
+    const int g = grid_for(c, n);
+    RedBuf red{c->partials.get(), c->scalars.get()};
+    spmv_path<FIN_NONE>(c, ICCG_STORE_FP64, x, Ax, nullptr);
+    launch(c, 3, k_sub, g, kThreads, n, b, (const double*)Ax, r);
+    double normb = std::sqrt(dot_dev(c, n, b, b));
+    if (normb == 0.0) normb = 1.0;
+    apply_path<FIN_NONE>(c, ICCG_STORE_FP64, r, z, nullptr);
+    launch(c, 3, k_copy, g, kThreads, n, (const double*)z, p, (SolverState*)nullptr);
+    double rz_old = dot_dev(c, n, r, z);
+    res->iters = 0;
+    res->converged = 0;
+    res->status = kMaxIter;
+    res->rel_resid = std::sqrt(dot_dev(c, n, r, r)) / normb;
+    if (res->rel_resid < tol) {
+        res->converged = 1;
+        res->status = kConverged;
+        return;
+    }
+    for (int k = 0; k < max_iter; ++k) {
+        spmv_path<FIN_NONE>(c, ICCG_STORE_FP64, p, Ap, nullptr);
+        const double pAp = dot_dev(c, n, p, Ap);
+        const double eps = 2.220446049250313080847e-16;
+        const double thr = eps * std::sqrt(dot_dev(c, n, p, p)) * std::sqrt(dot_dev(c, n, Ap, Ap));
+        if (pAp <= thr) {
+            res->iters = k;
+            res->status = kBreakdown;
+            return;
+        }
+        const double alpha = rz_old / pAp;
+        launch(c, 3, k_update<FIN_NONE>, g, kThreads, n, alpha, (const double*)p, (const double*)Ap, x, r,
+               (SolverState*)nullptr, red, c->ticket.get());
+        const double rel = std::sqrt(dot_dev(c, n, r, r)) / normb;
+        res->iters = k + 1;
+        res->rel_resid = rel;
+        if (rel < tol) {
+            res->converged = 1;
+            res->status = kConverged;
+            return;
+        }
+        apply_path<FIN_NONE>(c, ICCG_STORE_FP64, r, z, nullptr);
+        const double rz_new = dot_dev(c, n, r, z);
+        const double beta = rz_new / rz_old;
+        launch(c, 3, k_xpay, g, kThreads, n, beta, (const double*)z, p, (SolverState*)nullptr);
+        rz_old = rz_new;
+    }
+    res->status = kMaxIter;
+}
+
+// ---------------------------------------------------------------------------
+// fused CG: device-side scalars, iterations replayed as a CUDA graph
+// ---------------------------------------------------------------------------
+static void fused_iteration(iccg_ctx* c, int storage, bool rr, const double* b, double* x)
+{
+    const int n = c->n;
+    const int g = grid_for(c, n);
+    SolverState* st = c->state.get();
+    RedBuf red{c->partials.get(), c->scalars.get()};
+    spmv_path<FIN_PAP>(c, storage, (const double*)c->vp.get(), c->vAp.get(), st);
+    launch(c, 3, k_update<FIN_UPD>, g, kThreads, n, 0.0, (const double*)c->vp.get(), (const double*)c->vAp.get(), x,
+           c->vr.get(), st, red, c->ticket.get());
+    if (rr) residual_path<FIN_TRUE>(c, (const double*)x, b, c->vr.get(), st);
+    apply_path<FIN_RZ>(c, storage, c->vr.get(), c->vz.get(), st);
+    launch(c, 3, k_xpay, g, kThreads, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st);
+}
+
+static void solve_fused(iccg_ctx* c, const double* b, double* x, int max_iter, double tol, const iccg_solve_opts& o,
+                        iccg_result* res)
+{
+    const int n = c->n;
+    const int storage = o.storage;
+    const bool rr = storage == ICCG_STORE_FP32 && o.rr_interval > 0;
+    SolverState s0{};
+    s0.tol = tol;
+    s0.status = kRunning;
+    s0.max_iter = max_iter;
+    s0.rr_interval = rr ? o.rr_interval : 0;
+    *c->h_state = s0;
+    CK(cudaMemcpyAsync(c->state.get(), c->h_state, sizeof(SolverState), cudaMemcpyHostToDevice, c->stream));
+    unsigned int zero = 0;
+    CK(cudaMemcpyAsync(c->ticket.get(), &zero, sizeof(zero), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaEventRecord(c->ev0, c->stream));
+    const int g = grid_for(c, n);
+    SolverState* st = c->state.get();
+    // r0 = b - A x0, ||b||, z0 = M^{-1} r0, rz, p = z  (cg_crs.cpp:102-123)
+    residual_path<FIN_INIT>(c, (const double*)x, b, c->vr.get(), st);
+    apply_path<FIN_RZ0>(c, storage, c->vr.get(), c->vz.get(), st);
+    launch(c, 3, k_copy, g, kThreads, n, (const double*)c->vz.get(), c->vp.get(), st);
+
+    const int m = std::max(1, o.graph_iters);
+    const bool use_graph = !c->profile;
+    auto one_batch = [&]() {
+        for (int it = 0; it < m; ++it) fused_iteration(c, storage, rr, b, x);
+    };
+    if (use_graph) {
+        const long long key = ((long long)c->sched_version << 24) ^ ((long long)c->factor_version << 36) ^
+                              ((long long)storage << 20) ^ ((long long)rr << 19) ^ ((long long)c->use_q << 18) ^
+                              ((long long)m << 4) ^ (long long)c->pc_kind ^ ((long long)(uintptr_t)x << 32) ^
+                              ((long long)(uintptr_t)b << 40);
+        if (!c->gexec || c->gkey != key) {
+            if (c->gexec) {
+                cudaGraphExecDestroy(c->gexec);
+                c->gexec = nullptr;
+            }
+            cudaGraph_t graph = nullptr;
+            const long long before = c->launches;
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                one_batch();
+            } catch (...) {
+                cudaStreamEndCapture(c->stream, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                throw;
+            }
+            CK(cudaStreamEndCapture(c->stream, &graph));
+            CK(cudaGraphInstantiate(&c->gexec, graph, 0));
+            cudaGraphDestroy(graph);
+            c->gkernels = (int)(c->launches - before);
+            c->launches = before;
+            c->gkey = key;
+        }
+    }
+    // launch batches; poll the status of batch i-1 while batch i runs
+    for (int batch = 0;; ++batch) {
+        if (use_graph) {
+            CK(cudaGraphLaunch(c->gexec, c->stream));
+            c->launches += c->gkernels;
+        } else {
+            one_batch();
+        }
+        CK(cudaMemcpyAsync(&c->h_status[batch & 1], &st->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaEventRecord(c->evs[batch & 1], c->stream));
+        if (batch > 0) {
+            CK(cudaEventSynchronize(c->evs[(batch - 1) & 1]));
+            if (c->h_status[(batch - 1) & 1] != kRunning) break;
+        }
+        if ((long long)(batch + 1) * m > (long long)max_iter + m) {
+            CK(cudaEventSynchronize(c->evs[batch & 1]));
+            break;
+        }
+    }
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CK(cudaMemcpyAsync(c->h_state, st, sizeof(SolverState), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const SolverState& sf = *c->h_state;
+    res->iters = sf.iters;
+    res->status = sf.status == kRunning ? kMaxIter : sf.status;
+    res->converged = sf.status == kConverged ? 1 : 0;
+    res->rel_resid = sf.rel_resid;
+    res->n_replacements = sf.n_rr;
+}
+
+static double true_resid(iccg_ctx* c, const double* b, const double* x)
+{
+    residual_path<FIN_NONE>(c, x, b, c->vtmp.get(), nullptr);
+    const double nr = dot_dev(c, c->n, c->vtmp.get(), c->vtmp.get());
+    const double nb = dot_dev(c, c->n, b, b);
+    return std::sqrt(nr) / std::sqrt(nb);
+}
+
+// conjugate_gradient with b, x in A_run order on the device
+static void solve_dev(iccg_ctx* c, const double* b, double* x, int max_iter, double tol, const iccg_solve_opts* opts,
+                      iccg_result* res)
+{
+    require_precond(c);
+    iccg_solve_opts o{ICCG_MODE_FUSED, ICCG_STORE_FP64, 50, 8};
+    if (opts) o = *opts;
+    if (o.graph_iters <= 0) o.graph_iters = 8;
+    if (o.mode == ICCG_MODE_PLAIN && o.storage != ICCG_STORE_FP64)
+        throw Error(ICCG_ERR_ARG, "the plain path computes in FP64 storage only");
+    std::memset(res, 0, sizeof(*res));
+    prepare_path(c, o.storage);
+    const double* bp = b;
+    double* xp = x;
+    const int g = grid_for(c, c->n);
+    if (c->use_q) {
+        launch(c, 3, k_gather_vec, g, kThreads, c->n, (const int*)c->Q.dq2r.get(), b, c->qb.get());
+        launch(c, 3, k_gather_vec, g, kThreads, c->n, (const int*)c->Q.dq2r.get(), (const double*)x, c->qx.get());
+        bp = c->qb.get();
+        xp = c->qx.get();
+    }
+    if (o.mode == ICCG_MODE_PLAIN) {
+        CK(cudaEventRecord(c->ev0, c->stream));
+        solve_plain(c, bp, xp, max_iter, tol, res);
+        CK(cudaEventRecord(c->ev1, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    } else {
+        solve_fused(c, bp, xp, max_iter, tol, o, res);
+    }
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    res->solve_ms = ms;
+    collect_profile(c);
+    // A converged FP32-storage solve ends on a residual replacement, whose
+    // convergence test is already ||b - A x|| / ||b|| with the FP64 matrix.
+    if (o.mode == ICCG_MODE_FUSED && o.storage == ICCG_STORE_FP32 && o.rr_interval > 0 && res->converged)
+        res->true_rel_resid = res->rel_resid;
+    else
+        res->true_rel_resid = true_resid(c, bp, xp);
+    if (c->use_q) launch(c, 3, k_scatter_vec, g, kThreads, c->n, (const int*)c->Q.dq2r.get(), (const double*)xp, x);
+    CK(cudaStreamSynchronize(c->stream));
+}
+
+// z = M^{-1} r and y = A x with vectors in A_run order on the device
+static void apply_dev(iccg_ctx* c, int storage, const double* r, double* z)
+{
+    require_precond(c);
+    prepare_path(c, storage);
+    const int g = grid_for(c, c->n);
+    if (c->use_q) {
+        launch(c, 3, k_gather_vec, g, kThreads, c->n, (const int*)c->Q.dq2r.get(), r, c->qb.get());
+        apply_path<FIN_NONE>(c, storage, c->qb.get(), c->qx.get(), nullptr);
+        launch(c, 3, k_scatter_vec, g, kThreads, c->n, (const int*)c->Q.dq2r.get(), (const double*)c->qx.get(), z);
+    } else {
+        apply_path<FIN_NONE>(c, storage, r, z, nullptr);
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    collect_profile(c);
+}
+
+static void spmv_dev(iccg_ctx* c, int storage, const double* x, double* y)
+{
+    require_matrix(c);
+    prepare_path(c, storage);
+    const int g = grid_for(c, c->n);
+    if (c->use_q) {
+        launch(c, 3, k_gather_vec, g, kThreads, c->n, (const int*)c->Q.dq2r.get(), x, c->qb.get());
+        spmv_path<FIN_NONE>(c, storage, c->qb.get(), c->qx.get(), nullptr);
+        launch(c, 3, k_scatter_vec, g, kThreads, c->n, (const int*)c->Q.dq2r.get(), (const double*)c->qx.get(), y);
+    } else {
+        spmv_path<FIN_NONE>(c, storage, x, y, nullptr);
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    collect_profile(c);
+}
+
+static void ensure_vectors(iccg_ctx* c)
+{
+    const size_t n = (size_t)c->n;
+    for (Buf<double>* v : {&c->vb, &c->vx, &c->qb, &c->qx, &c->vr, &c->vp, &c->vz, &c->vy, &c->vAp, &c->vtmp})
+        v->alloc(n, &c->dev_bytes);
+    ensure_partials(c, (size_t)grid_for(c, c->n));
+}

@@ -332,3 +332,29 @@ def test_gpu_tiled_kernels_equal_simple_kernels(which):
     for a, b in zip(out[True], out[False]):
         assert np.array_equal(a, b)
     ctx.close()
+
+
+DROPIN = ob.HERE / "_ref" / "dropin_check"
+
+
+@pytest.mark.skipif(not DROPIN.exists(), reason="drop-in check program not built (needs the reference checkout)")
+def test_gpu_dropin_reference_template(tmp_path):
+    """The reference's own conjugate_gradient<Precond> (compiled from its
+    sources) with iccg::GpuIC0 in place of IC0, files read by the reference's
+    readers: same iterations and x as with the reference's IC0."""
+    import json
+    import subprocess
+    A = pb.laplace3d_aniso(20)
+    blk, nb = ib.block_partition(A, 16, "bfs")
+    bcol, nc = ib.color_blocks(A, blk, nb)
+    ib.write_matrix_market(str(tmp_path / "a.mtx"), A, symmetric=True)
+    ib.write_assignment_1based(str(tmp_path / "a.blk"), blk, nb)
+    ib.write_assignment_1based(str(tmp_path / "a.bcol"), bcol, nc)
+    out = subprocess.run([str(DROPIN), str(tmp_path / "a.mtx"), str(tmp_path / "a.blk"), str(tmp_path / "a.bcol"),
+                          "1e-8"], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    d = json.loads(out.stdout.strip().splitlines()[-1])
+    assert abs(d["adapter_iters"] - d["ref_iters"]) <= 1
+    assert d["adapter_x_rel_err"] <= X_TOL
+    assert d["gpu_converged"] == 1 and abs(d["gpu_iters"] - d["ref_iters"]) <= 1
+    assert d["gpu_x_rel_err"] <= X_TOL
