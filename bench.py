@@ -405,11 +405,43 @@ def main():
     ap.add_argument("--impl", default="iccg_b200", choices=["iccg_b200", "reference"])
     ap.add_argument("--cpu-samples", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel-only", choices=["spmv", "apply"], default=None,
+                    help="set up the workload, then launch only this operation --reps times "
+                         "(FP32 storage) and print its mean device time; for profilers")
+    ap.add_argument("--reps", type=int, default=3)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.kernel_only:
+        run_kernel_only(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)
+
+
+def run_kernel_only(args):
+    """One operation of the hot path on the benchmark system, repeated."""
+    import torch
+    import iccg_b200 as ib
+    P, _ = build_problem()
+    n = P.A_run.n
+    ctx = ib.Context(0)
+    ctx.upload(P.A_run)
+    ctx.set_schedule(P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    dev = torch.device("cuda", 0)
+    a = torch.from_numpy(ib.gen_uniform(n, 5)).to(dev)
+    b = torch.zeros(n, dtype=torch.float64, device=dev)
+    L = ib.lib()
+    fn = L.iccg_spmv_dev if args.kernel_only == "spmv" else L.iccg_precond_apply_dev
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(args.reps):
+        t0 = time.perf_counter()
+        rc = fn(ctx.h, ib.C.c_void_p(a.data_ptr()), ib.C.c_void_p(b.data_ptr()), ib.STORE_FP32)
+        ms.append((time.perf_counter() - t0) * 1e3)
+        assert rc == 0, L.iccg_ctx_last_error(ctx.h)
+    print(json.dumps({"kernel_only": args.kernel_only, "reps": args.reps, "host_ms": ms}))
+    ctx.close()
 
 
 if __name__ == "__main__":

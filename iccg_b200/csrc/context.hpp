@@ -91,6 +91,12 @@ struct QSys {
     Buf<int> gbase, glen, sl0;
     std::vector<int> h_gbase, h_glen, h_sl0;
     std::vector<std::pair<int, int>> steps;  // step slices: (first Q row, rows)
+    std::vector<int> unit_of, step_of;       // per A_run row: unit id, row index in the unit
+    int maxu = 0;                            // longest unit
+    bool two_phase = false;                  // S/T carry in-unit entries as -(step + 1)
+    int gpc = 1;                             // groups per CTA of the two-phase kernel
+    std::vector<int> g2grid, b2slot0;        // its grids and backward reduction slots
+    int b2nslots = 0;
     // matrices
     SellDev A, S, T;
     Buf<double> d64, inv_diag;
@@ -115,6 +121,14 @@ struct QSys {
         h_glen.clear();
         h_sl0.clear();
         steps.clear();
+        unit_of.clear();
+        step_of.clear();
+        maxu = 0;
+        two_phase = false;
+        gpc = 1;
+        g2grid.clear();
+        b2slot0.clear();
+        b2nslots = 0;
         A.reset();
         S.reset();
         T.reset();

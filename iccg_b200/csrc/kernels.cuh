@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(256) k_sweep_q(int g0, int g1, const int* __re
             if (r < len) {
                 const int q = base + off + lane;
                 const int p0 = M.ptr[s0 + r] + lane;
-                const int L = M.len[q];
+                const int L = M.len[q] & 0xffff;
                 double acc = in[q];
                 for (int j = 0; j < L; ++j) {
                     const int pa = p0 + 32 * j;
@@ -540,6 +540,106 @@ __global__ void __launch_bounds__(256) k_sweep_q(int g0, int g1, const int* __re
                 if (FIN != FIN_NONE) acc2_fma(rz[0], rdot[q], v);
             }
         }
+    }
+    if (FIN != FIN_NONE) reduce_finish<1, FIN>(rz, red, st, ticket, slot0 + blockIdx.x, nslots);
+}
+
+// Two-phase substitution over one level (groups [g0, g1)), used when every
+// unit has at most 64 rows.  Row lengths are stored as L | nint << 16 and the
+// nint in-unit entries of a row carry col = -(step + 1) (the unit's own row
+// at that step); they are the last entries of a forward row and the first of
+// a backward row, as in the reference's column order.
+//
+// A CTA (8 warps) takes gpc groups at a time.  Phase A, spread over all
+// warps (one warp per (group, step) slice, 32 rows in parallel), computes
+// each row's chain over its entries from earlier levels -- those values are
+// final and not written by this launch -- and parks the partial value in
+// shared memory.  Phase B, one warp per group, walks the steps: in-unit
+// entries read the unit's earlier results from shared memory, then the row
+// divides by its pivot.
+//
+// Forward rows: earlier-level entries come first in the reference's order,
+// so the split keeps its bits.  Backward rows put the in-unit entries first;
+// EXACT keeps that order (phase A only loads in_q, phase B runs in-unit then
+// earlier-level entries), otherwise the earlier-level entries are applied
+// first (the FP32-storage path, which has no reference rounding to match).
+template <class T, bool FWD, int FIN, bool EXACT>
+__global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int maxu,
+                                                  const int* __restrict__ gbase, const int* __restrict__ glen,
+                                                  const int* __restrict__ sl0, SellMat M,
+                                                  const T* __restrict__ dg, const double* __restrict__ in,
+                                                  double* out, const double* __restrict__ rdot, int slot0,
+                                                  int nslots, SolverState* st, RedBuf red, unsigned int* ticket)
+{
+    if (st_done(st)) return;
+    extern __shared__ double s_acc[];  // [gpc][maxu][32]
+    const T* __restrict__ val = (const T*)M.val;
+    const int* __restrict__ col = M.col;
+    const int* __restrict__ mlen = M.len;
+    const int* __restrict__ mptr = M.ptr;
+    const double* __restrict__ prev = out;  // earlier-level values: read-only in this launch
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool ext_first = FWD || !EXACT;
+    acc2 rz[1] = {{0.0, 0.0}};
+    for (int gb = g0 + blockIdx.x * gpc; gb < g1; gb += gridDim.x * gpc) {
+        const int ng = min(gpc, g1 - gb);
+        // phase A
+        for (int t = warp; t < ng * maxu; t += 8) {
+            const int gl = t / maxu, r = t - gl * maxu;
+            const int g = gb + gl;
+            const int len = glen[(size_t)g * 32 + lane];
+            const int off = (int)__reduce_add_sync(0xffffffffu, (unsigned)min(len, r));
+            if (r < len) {
+                const int q = gbase[g] + off + lane;
+                double a = in[q];
+                if (ext_first) {
+                    const int lw = mlen[q];
+                    const int L = lw & 0xffff, ni = lw >> 16;
+                    const int p0 = mptr[sl0[g] + r] + lane;
+                    const int j0 = FWD ? 0 : ni, j1 = FWD ? L - ni : L;
+                    for (int j = j0; j < j1; ++j) {
+                        const int pa = p0 + 32 * j;
+                        a = fma(-(double)val[pa], __ldg(prev + col[pa]), a);
+                    }
+                }
+                s_acc[((size_t)gl * maxu + r) * 32 + lane] = a;
+            }
+        }
+        __syncthreads();
+        // phase B
+        if (warp < ng) {
+            const int gl = warp, g = gb + gl;
+            const int len = glen[(size_t)g * 32 + lane];
+            const int maxlen = (int)__reduce_max_sync(0xffffffffu, (unsigned)len);
+            const int base = gbase[g], s0 = sl0[g];
+            double* sa = s_acc + (size_t)gl * maxu * 32 + lane;
+            for (int t = 0; t < maxlen; ++t) {
+                const int r = FWD ? t : maxlen - 1 - t;
+                const int off = (int)__reduce_add_sync(0xffffffffu, (unsigned)min(len, r));
+                if (r < len) {
+                    const int q = base + off + lane;
+                    const int lw = mlen[q];
+                    const int L = lw & 0xffff, ni = lw >> 16;
+                    const int p0 = mptr[s0 + r] + lane;
+                    double a = sa[r * 32];
+                    const int j0 = FWD ? L - ni : 0, j1 = FWD ? L : ni;
+                    for (int j = j0; j < j1; ++j) {
+                        const int pa = p0 + 32 * j;
+                        a = fma(-(double)val[pa], sa[(-col[pa] - 1) * 32], a);
+                    }
+                    if (!ext_first)
+                        for (int j = ni; j < L; ++j) {
+                            const int pa = p0 + 32 * j;
+                            a = fma(-(double)val[pa], __ldg(prev + col[pa]), a);
+                        }
+                    const double v = a / (double)dg[q];
+                    sa[r * 32] = v;
+                    out[q] = v;
+                    if (FIN != FIN_NONE) acc2_fma(rz[0], rdot[q], v);
+                }
+            }
+        }
+        __syncthreads();
     }
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(rz, red, st, ticket, slot0 + blockIdx.x, nslots);
 }

@@ -20,6 +20,30 @@ static void ensure_partials(iccg_ctx* c, size_t slots)
 // launch wrapper: counts launches and, when profiling, brackets each launch
 // with CUDA events on the context's stream (class cls)
 template <class K, class... Args>
+static void launch_smem(iccg_ctx* c, int cls, K kernel, int grid, int block, size_t smem, Args... args)
+{
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (c->profile) {
+        if (c->ev_used == c->ev_pool.size()) {
+            cudaEvent_t a, b;
+            CK(cudaEventCreate(&a));
+            CK(cudaEventCreate(&b));
+            c->ev_pool.emplace_back(a, b);
+            c->ev_cls.push_back(0);
+        }
+        e0 = c->ev_pool[c->ev_used].first;
+        e1 = c->ev_pool[c->ev_used].second;
+        c->ev_cls[c->ev_used] = cls;
+        ++c->ev_used;
+        CK(cudaEventRecord(e0, c->stream));
+    }
+    kernel<<<grid, block, smem, c->stream>>>(args...);
+    CK(cudaGetLastError());
+    if (c->profile) CK(cudaEventRecord(e1, c->stream));
+    c->launches++;
+}
+
+template <class K, class... Args>
 static void launch(iccg_ctx* c, int cls, K kernel, int grid, int block, Args... args)
 {
     cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -9,10 +9,29 @@
 // levels and steps reversed, which is a valid order because every backward
 // dependency is a forward dependency reversed.
 
-static void sell_build(iccg_ctx* c, const std::vector<std::pair<int, int>>& slices, const std::vector<int>& rp,
-                       const std::vector<int>& ci, const std::vector<int>* src_map, SellDev& M)
+// encode: 0 plain columns; 1 forward rows, 2 backward rows -- in-unit entries
+// become -(step + 1) and each row's length word carries their count in its
+// high half; returns false (and leaves plain columns) when a row's in-unit
+// entries are not its last (forward) / first (backward) entries.
+static bool sell_build(iccg_ctx* c, const std::vector<std::pair<int, int>>& slices, const std::vector<int>& rp,
+                       const std::vector<int>& ci, const std::vector<int>* src_map, SellDev& M, int encode = 0)
 {
     const QSys& Q = c->Q;
+    if (encode) {
+        for (size_t s = 0; s < slices.size(); ++s)
+            for (int l = 0; l < slices[s].second; ++l) {
+                const int r = Q.q2r[(size_t)(slices[s].first + l)];
+                const int b = rp[(size_t)r], L = rp[(size_t)r + 1] - b;
+                bool seen_in = false, seen_out = false;
+                for (int j = 0; j < L; ++j) {
+                    const bool inside = Q.unit_of[(size_t)ci[(size_t)b + j]] == Q.unit_of[(size_t)r];
+                    if (encode == 1 && seen_in && !inside) return false;   // forward: in-unit entries last
+                    if (encode == 2 && seen_out && inside) return false;   // backward: in-unit entries first
+                    seen_in |= inside;
+                    seen_out |= !inside;
+                }
+            }
+    }
     const int n = (int)Q.q2r.size();
     std::vector<int> ptr(slices.size() + 1), len((size_t)n, 0);
     long long slot = 0;
@@ -35,12 +54,20 @@ static void sell_build(iccg_ctx* c, const std::vector<std::pair<int, int>>& slic
             const int q = slices[s].first + l;
             const int r = Q.q2r[(size_t)q];
             const int b = rp[(size_t)r], L = rp[(size_t)r + 1] - b;
-            len[(size_t)q] = L;
+            if (L > 0xffff) throw Error(ICCG_ERR_ARG, "row longer than 65535 entries");
+            int nin = 0;
             for (int j = 0; j < L; ++j) {
                 const size_t pos = (size_t)ptr[s] + 32 * (size_t)j + (size_t)l;
-                col[pos] = Q.r2q[(size_t)ci[(size_t)b + j]];
+                const int cj = ci[(size_t)b + j];
+                if (encode && Q.unit_of[(size_t)cj] == Q.unit_of[(size_t)r]) {
+                    col[pos] = -(Q.step_of[(size_t)cj] + 1);
+                    ++nin;
+                } else {
+                    col[pos] = Q.r2q[(size_t)cj];
+                }
                 M.src[pos] = src_map ? (*src_map)[(size_t)b + j] : b + j;
             }
+            len[(size_t)q] = L | (nin << 16);
         }
     M.ptr.upload(ptr.data(), ptr.size(), &c->dev_bytes, c->stream);
     M.col.upload(col.data(), col.size(), &c->dev_bytes, c->stream);
@@ -49,6 +76,7 @@ static void sell_build(iccg_ctx* c, const std::vector<std::pair<int, int>>& slic
     M.has32 = false;
     M.v32.free();
     CK(cudaStreamSynchronize(c->stream));
+    return true;
 }
 
 // M.v64[slot] = src[M.src[slot]] (0 on padding)
@@ -88,6 +116,10 @@ static void build_q_order(iccg_ctx* c)
     Q.steps.clear();
     struct U { int t0, m; };
     std::vector<U> units;
+    Q.unit_of.assign((size_t)c->n, -1);
+    Q.step_of.assign((size_t)c->n, 0);
+    Q.maxu = 0;
+    int unit_id = 0;
     for (int l = 0; l < P.nlevels; ++l) {
         units.clear();
         for (int u = P.level_ptr[(size_t)l]; u < P.level_ptr[(size_t)l + 1]; ++u) {
@@ -102,13 +134,22 @@ static void build_q_order(iccg_ctx* c)
             Q.h_sl0.push_back((int)Q.steps.size());
             for (size_t u = g0; u < g0 + 32; ++u) Q.h_glen.push_back(u < g1 ? units[u].m : 0);
             const int maxlen = units[g0].m;
+            Q.maxu = std::max(Q.maxu, maxlen);
             for (int r = 0; r < maxlen; ++r) {
                 int cnt = 0;
                 while (g0 + (size_t)cnt < g1 && units[g0 + (size_t)cnt].m > r) ++cnt;
                 Q.steps.emplace_back((int)Q.q2r.size(), cnt);
-                for (int u = 0; u < cnt; ++u) Q.q2r.push_back(P.h_rows[(size_t)(units[g0 + (size_t)u].t0 + r)]);
+                for (int u = 0; u < cnt; ++u) {
+                    const int row = P.h_rows[(size_t)(units[g0 + (size_t)u].t0 + r)];
+                    Q.q2r.push_back(row);
+                    if (row >= 0 && row < c->n) {
+                        Q.unit_of[(size_t)row] = unit_id + (int)(g0 + (size_t)u);
+                        Q.step_of[(size_t)row] = r;
+                    }
+                }
             }
         }
+        unit_id += (int)units.size();
         Q.level_g.push_back((int)Q.h_gbase.size());
     }
     if ((int)Q.q2r.size() != c->n) throw Error(ICCG_ERR_SCHEDULE, "schedule does not cover every row once");
@@ -146,10 +187,34 @@ static void build_q_factor(iccg_ctx* c)
 {
     QSys& Q = c->Q;
     Factor& F = c->F;
-    sell_build(c, Q.steps, F.Sp, F.Si, &F.s_src, Q.S);
+    // two-phase sweeps need units of at most 64 rows and the reference's
+    // column order to put in-unit entries last (forward) / first (backward)
+    Q.two_phase = Q.maxu <= 64 && sell_build(c, Q.steps, F.Sp, F.Si, &F.s_src, Q.S, 1) &&
+                  sell_build(c, Q.steps, F.Tp, F.Ti, &F.t_src, Q.T, 2);
+    if (!Q.two_phase) {
+        sell_build(c, Q.steps, F.Sp, F.Si, &F.s_src, Q.S, 0);
+        sell_build(c, Q.steps, F.Tp, F.Ti, &F.t_src, Q.T, 0);
+    }
     sell_values(c, Q.S, F.dLx.get());
-    sell_build(c, Q.steps, F.Tp, F.Ti, &F.t_src, Q.T);
     sell_values(c, Q.T, F.dLx.get());
+    if (Q.two_phase) {
+        // gpc groups per CTA, gpc * maxu <= 64 rows of partial sums per lane slot
+        Q.gpc = std::max(1, std::min(8, 64 / std::max(1, Q.maxu)));
+        Q.g2grid.assign((size_t)Q.nlevels, 1);
+        Q.b2slot0.assign((size_t)Q.nlevels, 0);
+        const int cap = c->nsm * 8;
+        for (int l = 0; l < Q.nlevels; ++l) {
+            const int groups = Q.level_g[(size_t)l + 1] - Q.level_g[(size_t)l];
+            Q.g2grid[(size_t)l] = std::max(1, std::min(cap, (groups + Q.gpc - 1) / Q.gpc));
+        }
+        int s = 0;
+        for (int l = Q.nlevels - 1; l >= 0; --l) {
+            Q.b2slot0[(size_t)l] = s;
+            s += Q.g2grid[(size_t)l];
+        }
+        Q.b2nslots = s;
+        ensure_partials(c, (size_t)std::max(s, 1));
+    }
     std::vector<int> dsrc((size_t)c->n);
     for (int q = 0; q < c->n; ++q) dsrc[(size_t)q] = F.dpos[(size_t)Q.q2r[(size_t)q]];
     Buf<int> idx;
