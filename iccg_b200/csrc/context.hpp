@@ -60,6 +60,7 @@ struct SellDev {
     Buf<float> v32;
     bool has32 = false;
     long long slots = 0;
+    int max_nin = 0;       // most in-unit entries of a row (encoded matrices)
     std::vector<int> src;  // host: CRS value index of each slot (-1: padding)
     SellMat view(bool fp32) const
     {
@@ -72,6 +73,7 @@ struct SellDev {
         v32.free();
         has32 = false;
         slots = 0;
+        max_nin = 0;
         src.clear();
     }
 };
@@ -95,6 +97,7 @@ struct QSys {
     int maxu = 0;                            // longest unit
     bool two_phase = false;                  // S/T carry in-unit entries as -(step + 1)
     int gpc = 1;                             // groups per CTA of the two-phase kernel
+    int ni = 1;                              // in-unit entries staged per row (1, 2 or 4)
     std::vector<int> g2grid, b2slot0;        // its grids and backward reduction slots
     int b2nslots = 0;
     // matrices

@@ -550,20 +550,23 @@ __global__ void __launch_bounds__(256) k_sweep_q(int g0, int g1, const int* __re
 // at that step); they are the last entries of a forward row and the first of
 // a backward row, as in the reference's column order.
 //
-// A CTA (8 warps) takes gpc groups at a time.  Phase A, spread over all
-// warps (one warp per (group, step) slice, 32 rows in parallel), computes
-// each row's chain over its entries from earlier levels -- those values are
-// final and not written by this launch -- and parks the partial value in
-// shared memory.  Phase B, one warp per group, walks the steps: in-unit
-// entries read the unit's earlier results from shared memory, then the row
-// divides by its pivot.
-//
+// A CTA (8 warps) takes gpc groups at a time (R = gpc * maxu * 32 rows).
+//  Phase A, all warps, one warp per (group, step) slice: each row's chain
+//    over its entries from earlier levels (values final, not written by
+//    this launch) is computed and parked in shared memory together with
+//    what the serial part needs: the pivot and the first NI in-unit entries.
+//  Phase B, one warp per group, walks the steps of its 32 units reading
+//    shared memory only: in-unit entries use the unit's earlier results,
+//    then the row divides by its pivot.  Rows with more than NI in-unit
+//    entries (and the exact backward order, below) read the rest of the row
+//    from global memory.
+//  Post-pass, all warps: results are stored and r.z is accumulated.
 // Forward rows: earlier-level entries come first in the reference's order,
 // so the split keeps its bits.  Backward rows put the in-unit entries first;
-// EXACT keeps that order (phase A only loads in_q, phase B runs in-unit then
-// earlier-level entries), otherwise the earlier-level entries are applied
-// first (the FP32-storage path, which has no reference rounding to match).
-template <class T, bool FWD, int FIN, bool EXACT>
+// EXACT keeps that order (phase B applies the earlier-level entries after the
+// in-unit ones); otherwise the earlier-level entries are applied first, in
+// phase A (the FP32-storage path, which has no reference rounding to keep).
+template <class T, bool FWD, int FIN, bool EXACT, int NI>
 __global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int maxu,
                                                   const int* __restrict__ gbase, const int* __restrict__ glen,
                                                   const int* __restrict__ sl0, SellMat M,
@@ -572,14 +575,21 @@ __global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int m
                                                   int nslots, SolverState* st, RedBuf red, unsigned int* ticket)
 {
     if (st_done(st)) return;
-    extern __shared__ double s_acc[];  // [gpc][maxu][32]
+    extern __shared__ double smem_d[];
+    const int R = gpc * maxu * 32;
+    double* s_acc = smem_d;                                       // [R] partial sums, then results
+    double* s_piv = smem_d + R;                                   // [R] pivots
+    double* s_iv = smem_d + 2 * R;                                // [NI][R] in-unit matrix values
+    int* s_ii = reinterpret_cast<int*>(smem_d + (2 + NI) * R);    // [NI][R] their steps, -1 if none
+    int* s_p0 = s_ii + NI * R;                                    // [R] first slot, -1: no global rest
+    int* s_lw = s_p0 + R;                                         // [R] length word
     const T* __restrict__ val = (const T*)M.val;
     const int* __restrict__ col = M.col;
     const int* __restrict__ mlen = M.len;
     const int* __restrict__ mptr = M.ptr;
     const double* __restrict__ prev = out;  // earlier-level values: read-only in this launch
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const bool ext_first = FWD || !EXACT;
+    constexpr bool ext_first = FWD || !EXACT;
     acc2 rz[1] = {{0.0, 0.0}};
     for (int gb = g0 + blockIdx.x * gpc; gb < g1; gb += gridDim.x * gpc) {
         const int ng = min(gpc, g1 - gb);
@@ -591,18 +601,33 @@ __global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int m
             const int off = (int)__reduce_add_sync(0xffffffffu, (unsigned)min(len, r));
             if (r < len) {
                 const int q = gbase[g] + off + lane;
+                const int lw = mlen[q];
+                const int L = lw & 0xffff, ni = lw >> 16;
+                const int p0 = mptr[sl0[g] + r] + lane;
+                const int rr = (gl * maxu + r) * 32 + lane;
                 double a = in[q];
                 if (ext_first) {
-                    const int lw = mlen[q];
-                    const int L = lw & 0xffff, ni = lw >> 16;
-                    const int p0 = mptr[sl0[g] + r] + lane;
                     const int j0 = FWD ? 0 : ni, j1 = FWD ? L - ni : L;
                     for (int j = j0; j < j1; ++j) {
                         const int pa = p0 + 32 * j;
                         a = fma(-(double)val[pa], __ldg(prev + col[pa]), a);
                     }
                 }
-                s_acc[((size_t)gl * maxu + r) * 32 + lane] = a;
+                s_acc[rr] = a;
+                s_piv[rr] = (double)dg[q];
+                const int jin = FWD ? L - ni : 0;
+#pragma unroll
+                for (int k = 0; k < NI; ++k) {
+                    int idx = -1;
+                    if (k < ni) {
+                        const int pa = p0 + 32 * (jin + k);
+                        s_iv[k * R + rr] = (double)val[pa];
+                        idx = -col[pa] - 1;
+                    }
+                    s_ii[k * R + rr] = idx;
+                }
+                s_p0[rr] = (ni > NI || !ext_first) ? p0 : -1;
+                s_lw[rr] = lw;
             }
         }
         __syncthreads();
@@ -611,32 +636,48 @@ __global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int m
             const int gl = warp, g = gb + gl;
             const int len = glen[(size_t)g * 32 + lane];
             const int maxlen = (int)__reduce_max_sync(0xffffffffu, (unsigned)len);
-            const int base = gbase[g], s0 = sl0[g];
-            double* sa = s_acc + (size_t)gl * maxu * 32 + lane;
+            const int base = gl * maxu * 32 + lane;
             for (int t = 0; t < maxlen; ++t) {
                 const int r = FWD ? t : maxlen - 1 - t;
-                const int off = (int)__reduce_add_sync(0xffffffffu, (unsigned)min(len, r));
                 if (r < len) {
-                    const int q = base + off + lane;
-                    const int lw = mlen[q];
-                    const int L = lw & 0xffff, ni = lw >> 16;
-                    const int p0 = mptr[s0 + r] + lane;
-                    double a = sa[r * 32];
-                    const int j0 = FWD ? L - ni : 0, j1 = FWD ? L : ni;
-                    for (int j = j0; j < j1; ++j) {
-                        const int pa = p0 + 32 * j;
-                        a = fma(-(double)val[pa], sa[(-col[pa] - 1) * 32], a);
+                    const int rr = base + r * 32;
+                    double a = s_acc[rr];
+#pragma unroll
+                    for (int k = 0; k < NI; ++k) {
+                        const int idx = s_ii[k * R + rr];
+                        if (idx >= 0) a = fma(-s_iv[k * R + rr], s_acc[base + idx * 32], a);
                     }
-                    if (!ext_first)
-                        for (int j = ni; j < L; ++j) {
-                            const int pa = p0 + 32 * j;
-                            a = fma(-(double)val[pa], __ldg(prev + col[pa]), a);
+                    const int p0 = s_p0[rr];
+                    if (p0 >= 0) {
+                        const int lw = s_lw[rr];
+                        const int L = lw & 0xffff, ni = lw >> 16;
+                        const int jin = FWD ? L - ni : 0;
+                        for (int k = NI; k < ni; ++k) {
+                            const int pa = p0 + 32 * (jin + k);
+                            a = fma(-(double)val[pa], s_acc[base + (-col[pa] - 1) * 32], a);
                         }
-                    const double v = a / (double)dg[q];
-                    sa[r * 32] = v;
-                    out[q] = v;
-                    if (FIN != FIN_NONE) acc2_fma(rz[0], rdot[q], v);
+                        if (!ext_first)
+                            for (int j = ni; j < L; ++j) {
+                                const int pa = p0 + 32 * j;
+                                a = fma(-(double)val[pa], __ldg(prev + col[pa]), a);
+                            }
+                    }
+                    s_acc[rr] = a / s_piv[rr];
                 }
+            }
+        }
+        __syncthreads();
+        // post-pass
+        for (int t = warp; t < ng * maxu; t += 8) {
+            const int gl = t / maxu, r = t - gl * maxu;
+            const int g = gb + gl;
+            const int len = glen[(size_t)g * 32 + lane];
+            const int off = (int)__reduce_add_sync(0xffffffffu, (unsigned)min(len, r));
+            if (r < len) {
+                const int q = gbase[g] + off + lane;
+                const double v = s_acc[(gl * maxu + r) * 32 + lane];
+                out[q] = v;
+                if (FIN != FIN_NONE) acc2_fma(rz[0], rdot[q], v);
             }
         }
         __syncthreads();

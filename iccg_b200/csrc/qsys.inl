@@ -49,6 +49,7 @@ static bool sell_build(iccg_ctx* c, const std::vector<std::pair<int, int>>& slic
     ptr[slices.size()] = (int)slot;
     std::vector<int> col((size_t)slot, 0);
     M.src.assign((size_t)slot, -1);
+    M.max_nin = 0;
     for (size_t s = 0; s < slices.size(); ++s)
         for (int l = 0; l < slices[s].second; ++l) {
             const int q = slices[s].first + l;
@@ -68,6 +69,7 @@ static bool sell_build(iccg_ctx* c, const std::vector<std::pair<int, int>>& slic
                 M.src[pos] = src_map ? (*src_map)[(size_t)b + j] : b + j;
             }
             len[(size_t)q] = L | (nin << 16);
+            M.max_nin = std::max(M.max_nin, nin);
         }
     M.ptr.upload(ptr.data(), ptr.size(), &c->dev_bytes, c->stream);
     M.col.upload(col.data(), col.size(), &c->dev_bytes, c->stream);
@@ -187,19 +189,32 @@ static void build_q_factor(iccg_ctx* c)
 {
     QSys& Q = c->Q;
     Factor& F = c->F;
-    // two-phase sweeps need units of at most 64 rows and the reference's
-    // column order to put in-unit entries last (forward) / first (backward)
-    Q.two_phase = Q.maxu <= 64 && sell_build(c, Q.steps, F.Sp, F.Si, &F.s_src, Q.S, 1) &&
-                  sell_build(c, Q.steps, F.Tp, F.Ti, &F.t_src, Q.T, 2);
-    if (!Q.two_phase) {
-        sell_build(c, Q.steps, F.Sp, F.Si, &F.s_src, Q.S, 0);
-        sell_build(c, Q.steps, F.Tp, F.Ti, &F.t_src, Q.T, 0);
+    // two-phase sweeps need units of at most 64 rows, in-unit entries last
+    // (forward) / first (backward) in every row -- the reference's column
+    // order gives that for schedules from BuildABMCSchedule -- and a
+    // shared-memory tile that fits 48 KB
+    auto build = [&](bool enc) {
+        bool ok = sell_build(c, Q.steps, F.Sp, F.Si, &F.s_src, Q.S, enc ? 1 : 0) &&
+                  sell_build(c, Q.steps, F.Tp, F.Ti, &F.t_src, Q.T, enc ? 2 : 0);
+        return ok;
+    };
+    Q.two_phase = Q.maxu <= 64 && build(true);
+    if (Q.two_phase) {
+        // NI in-unit entries staged per row; gpc groups per CTA so that the
+        // tile (R = gpc * maxu * 32 rows of 24 + 12 NI bytes) stays within
+        // 48 KB and holds at most 1024 rows
+        const int mx = std::max(Q.S.max_nin, Q.T.max_nin);
+        Q.ni = mx <= 1 ? 1 : mx <= 2 ? 2 : 4;
+        const size_t row_bytes = 24 + 12 * (size_t)Q.ni;
+        const size_t per_group = (size_t)std::max(1, Q.maxu) * 32 * row_bytes;
+        Q.gpc = (int)std::max<size_t>(
+            1, std::min<size_t>({8, 48 * 1024 / per_group, 32 / (size_t)std::max(1, Q.maxu)}));
+        if (per_group * Q.gpc > 48 * 1024) Q.two_phase = false;
     }
+    if (!Q.two_phase) build(false);
     sell_values(c, Q.S, F.dLx.get());
     sell_values(c, Q.T, F.dLx.get());
     if (Q.two_phase) {
-        // gpc groups per CTA, gpc * maxu <= 64 rows of partial sums per lane slot
-        Q.gpc = std::max(1, std::min(8, 64 / std::max(1, Q.maxu)));
         Q.g2grid.assign((size_t)Q.nlevels, 1);
         Q.b2slot0.assign((size_t)Q.nlevels, 0);
         const int cap = c->nsm * 8;

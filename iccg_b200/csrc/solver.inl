@@ -44,6 +44,27 @@ static void apply_ic0_simple(iccg_ctx* c, const double* r, double* y, double* z,
 }
 
 // --- lane-interleaved substitutions -----------------------------------------
+template <class T, int FIN, int NI>
+static void apply_ic0_q2(iccg_ctx* c, const double* r, double* y, double* z, SolverState* st, const SellMat& S,
+                         const SellMat& U, const T* d)
+{
+    QSys& Q = c->Q;
+    RedBuf red{c->partials.get(), c->scalars.get()};
+    const size_t smem = (size_t)Q.gpc * Q.maxu * 32 * (24 + 12 * NI);
+    for (int l = 0; l < Q.nlevels; ++l)
+        launch_smem(c, 1, k_sweep_q2<T, true, FIN_NONE, true, NI>, Q.g2grid[(size_t)l], kThreads, smem,
+                    Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.maxu, (const int*)Q.gbase.get(),
+                    (const int*)Q.glen.get(), (const int*)Q.sl0.get(), S, d, r, y, (const double*)nullptr, 0, 0, st,
+                    red, c->ticket.get());
+    // FP64 storage keeps the reference's backward order exactly
+    constexpr bool exact = !std::is_same<T, float>::value;
+    for (int l = Q.nlevels - 1; l >= 0; --l)
+        launch_smem(c, 2, k_sweep_q2<T, false, FIN, exact, NI>, Q.g2grid[(size_t)l], kThreads, smem,
+                    Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.maxu, (const int*)Q.gbase.get(),
+                    (const int*)Q.glen.get(), (const int*)Q.sl0.get(), U, d, (const double*)y, z, r,
+                    Q.b2slot0[(size_t)l], Q.b2nslots, st, red, c->ticket.get());
+}
+
 template <class T, int FIN>
 static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, SolverState* st)
 {
@@ -53,18 +74,11 @@ static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, Solv
     const T* d = f32 ? (const T*)(const void*)Q.d32.get() : (const T*)(const void*)Q.d64.get();
     const SellMat S = Q.S.view(f32), U = Q.T.view(f32);
     if (Q.two_phase) {
-        const size_t smem = (size_t)Q.gpc * Q.maxu * 32 * sizeof(double);
-        // FP64 storage keeps the reference's backward order exactly
-        for (int l = 0; l < Q.nlevels; ++l)
-            launch_smem(c, 1, k_sweep_q2<T, true, FIN_NONE, true>, Q.g2grid[(size_t)l], kThreads, smem,
-                        Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.maxu, (const int*)Q.gbase.get(),
-                        (const int*)Q.glen.get(), (const int*)Q.sl0.get(), S, d, r, y, (const double*)nullptr, 0, 0,
-                        st, red, c->ticket.get());
-        for (int l = Q.nlevels - 1; l >= 0; --l)
-            launch_smem(c, 2, k_sweep_q2<T, false, FIN, !std::is_same<T, float>::value>, Q.g2grid[(size_t)l],
-                        kThreads, smem, Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.maxu,
-                        (const int*)Q.gbase.get(), (const int*)Q.glen.get(), (const int*)Q.sl0.get(), U, d,
-                        (const double*)y, z, r, Q.b2slot0[(size_t)l], Q.b2nslots, st, red, c->ticket.get());
+        switch (Q.ni) {
+            case 1: apply_ic0_q2<T, FIN, 1>(c, r, y, z, st, S, U, d); break;
+            case 2: apply_ic0_q2<T, FIN, 2>(c, r, y, z, st, S, U, d); break;
+            default: apply_ic0_q2<T, FIN, 4>(c, r, y, z, st, S, U, d); break;
+        }
         return;
     }
     for (int l = 0; l < Q.nlevels; ++l)
