@@ -405,7 +405,7 @@ def main():
     ap.add_argument("--impl", default="iccg_b200", choices=["iccg_b200", "reference"])
     ap.add_argument("--cpu-samples", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--kernel-only", choices=["spmv", "apply"], default=None,
+    ap.add_argument("--kernel-only", choices=["spmv", "apply", "solve"], default=None,
                     help="set up the workload, then launch only this operation --reps times "
                          "(FP32 storage) and print its mean device time; for profilers")
     ap.add_argument("--reps", type=int, default=3)
@@ -432,9 +432,18 @@ def run_kernel_only(args):
     a = torch.from_numpy(ib.gen_uniform(n, 5)).to(dev)
     b = torch.zeros(n, dtype=torch.float64, device=dev)
     L = ib.lib()
-    fn = L.iccg_spmv_dev if args.kernel_only == "spmv" else L.iccg_precond_apply_dev
     torch.cuda.synchronize()
     ms = []
+    if args.kernel_only == "solve":
+        for _ in range(args.reps):
+            b.zero_()
+            torch.cuda.synchronize()
+            res = ctx.solve_dev(a.data_ptr(), b.data_ptr(), 10000, TOL, storage=ib.STORE_FP32, rr_interval=RR)
+            ms.append(res.solve_ms)
+        print(json.dumps({"kernel_only": "solve", "reps": args.reps, "solve_ms": ms, "iters": res.iters}))
+        ctx.close()
+        return
+    fn = L.iccg_spmv_dev if args.kernel_only == "spmv" else L.iccg_precond_apply_dev
     for _ in range(args.reps):
         t0 = time.perf_counter()
         rc = fn(ctx.h, ib.C.c_void_p(a.data_ptr()), ib.C.c_void_p(b.data_ptr()), ib.STORE_FP32)

@@ -567,7 +567,7 @@ __global__ void __launch_bounds__(256) k_sweep_q(int g0, int g1, const int* __re
 // in-unit ones); otherwise the earlier-level entries are applied first, in
 // phase A (the FP32-storage path, which has no reference rounding to keep).
 template <class T, bool FWD, int FIN, bool EXACT, int NI>
-__global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int maxu,
+__global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int maxu, int slow,
                                                   const int* __restrict__ gbase, const int* __restrict__ glen,
                                                   const int* __restrict__ sl0, SellMat M,
                                                   const T* __restrict__ dg, const double* __restrict__ in,
@@ -575,14 +575,18 @@ __global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int m
                                                   int nslots, SolverState* st, RedBuf red, unsigned int* ticket)
 {
     if (st_done(st)) return;
+    // shared tile, R = gpc * maxu * 32 rows: partial sums / results (double),
+    // pivots and in-unit values (T), first slot and length word of each row
+    // (int, only when `slow`: rows with more than NI in-unit entries or the
+    // exact backward order), in-unit steps (int8, -1 if none)
     extern __shared__ double smem_d[];
     const int R = gpc * maxu * 32;
-    double* s_acc = smem_d;                                       // [R] partial sums, then results
-    double* s_piv = smem_d + R;                                   // [R] pivots
-    double* s_iv = smem_d + 2 * R;                                // [NI][R] in-unit matrix values
-    int* s_ii = reinterpret_cast<int*>(smem_d + (2 + NI) * R);    // [NI][R] their steps, -1 if none
-    int* s_p0 = s_ii + NI * R;                                    // [R] first slot, -1: no global rest
-    int* s_lw = s_p0 + R;                                         // [R] length word
+    double* s_acc = smem_d;
+    T* s_piv = reinterpret_cast<T*>(smem_d + R);
+    T* s_iv = s_piv + R;                                          // [NI][R]
+    int* s_p0 = reinterpret_cast<int*>(s_iv + NI * R);            // [R] if slow
+    int* s_lw = s_p0 + R;                                         // [R] if slow
+    signed char* s_ii = reinterpret_cast<signed char*>(slow ? s_lw + R : s_p0);  // [NI][R]
     const T* __restrict__ val = (const T*)M.val;
     const int* __restrict__ col = M.col;
     const int* __restrict__ mlen = M.len;
@@ -614,20 +618,22 @@ __global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int m
                     }
                 }
                 s_acc[rr] = a;
-                s_piv[rr] = (double)dg[q];
+                s_piv[rr] = dg[q];
                 const int jin = FWD ? L - ni : 0;
 #pragma unroll
                 for (int k = 0; k < NI; ++k) {
                     int idx = -1;
                     if (k < ni) {
                         const int pa = p0 + 32 * (jin + k);
-                        s_iv[k * R + rr] = (double)val[pa];
+                        s_iv[k * R + rr] = val[pa];
                         idx = -col[pa] - 1;
                     }
-                    s_ii[k * R + rr] = idx;
+                    s_ii[k * R + rr] = (signed char)idx;
                 }
-                s_p0[rr] = (ni > NI || !ext_first) ? p0 : -1;
-                s_lw[rr] = lw;
+                if (slow) {
+                    s_p0[rr] = (ni > NI || !ext_first) ? p0 : -1;
+                    s_lw[rr] = lw;
+                }
             }
         }
         __syncthreads();
@@ -645,9 +651,9 @@ __global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int m
 #pragma unroll
                     for (int k = 0; k < NI; ++k) {
                         const int idx = s_ii[k * R + rr];
-                        if (idx >= 0) a = fma(-s_iv[k * R + rr], s_acc[base + idx * 32], a);
+                        if (idx >= 0) a = fma(-(double)s_iv[k * R + rr], s_acc[base + idx * 32], a);
                     }
-                    const int p0 = s_p0[rr];
+                    const int p0 = slow ? s_p0[rr] : -1;
                     if (p0 >= 0) {
                         const int lw = s_lw[rr];
                         const int L = lw & 0xffff, ni = lw >> 16;
@@ -662,7 +668,7 @@ __global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int m
                                 a = fma(-(double)val[pa], __ldg(prev + col[pa]), a);
                             }
                     }
-                    s_acc[rr] = a / s_piv[rr];
+                    s_acc[rr] = a / (double)s_piv[rr];
                 }
             }
         }

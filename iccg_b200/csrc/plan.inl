@@ -10,6 +10,30 @@ static int grid_for(const iccg_ctx* c, long long work, int threads = kThreads)
     return (int)g;
 }
 
+// CTAs a grid-stride kernel should get: enough for the work, at most what is
+// resident at once (the kernel's own occupancy at this block / shared memory
+// size), so the work is spread over one wave instead of a full wave plus a
+// ragged tail.
+template <class K>
+static int occ_grid(iccg_ctx* c, K kernel, long long work, int threads = kThreads, size_t smem = 0)
+{
+    static thread_local std::vector<std::pair<std::pair<const void*, size_t>, int>> cache;
+    const void* key = reinterpret_cast<const void*>(kernel);
+    int per_sm = 0;
+    for (auto& e : cache)
+        if (e.first.first == key && e.first.second == smem) per_sm = e.second;
+    if (per_sm == 0) {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+        if (per_sm < 1) per_sm = 1;
+        cache.push_back({{key, smem}, per_sm});
+    }
+    long long g = (work + threads - 1) / threads;
+    const long long cap = (long long)c->nsm * per_sm;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
 static void ensure_partials(iccg_ctx* c, size_t slots)
 {
     if (slots <= c->partial_slots) return;
@@ -250,3 +274,10 @@ static void build_plans_abmc(iccg_ctx* c, int nc, int nb, const int* color_ptr_b
     finalize_plan(c, B);
 }
 
+
+// launch of a grid-stride kernel over `work` items, one wave of CTAs
+template <class K, class... Args>
+static void launch_n(iccg_ctx* c, int cls, K kernel, long long work, Args... args)
+{
+    launch(c, cls, kernel, occ_grid(c, kernel, work), kThreads, args...);
+}

@@ -185,6 +185,12 @@ static void build_q_order(iccg_ctx* c)
     sell_values(c, Q.A, c->val64.get());
 }
 
+// bytes per row of the two-phase sweep's shared tile (see k_sweep_q2)
+static size_t sweep_row_bytes(size_t tsize, int ni, bool slow)
+{
+    return 8 + tsize * (1 + (size_t)ni) + (slow ? 8 : 0) + (size_t)ni;
+}
+
 static void build_q_factor(iccg_ctx* c)
 {
     QSys& Q = c->Q;
@@ -205,7 +211,8 @@ static void build_q_factor(iccg_ctx* c)
         // 48 KB and holds at most 1024 rows
         const int mx = std::max(Q.S.max_nin, Q.T.max_nin);
         Q.ni = mx <= 1 ? 1 : mx <= 2 ? 2 : 4;
-        const size_t row_bytes = 24 + 12 * (size_t)Q.ni;
+        // largest tile row: FP64 pivots and values plus the slow-path words
+        const size_t row_bytes = sweep_row_bytes(8, Q.ni, true);
         const size_t per_group = (size_t)std::max(1, Q.maxu) * 32 * row_bytes;
         Q.gpc = (int)std::max<size_t>(
             1, std::min<size_t>({8, 48 * 1024 / per_group, 32 / (size_t)std::max(1, Q.maxu)}));
@@ -217,7 +224,19 @@ static void build_q_factor(iccg_ctx* c)
     if (Q.two_phase) {
         Q.g2grid.assign((size_t)Q.nlevels, 1);
         Q.b2slot0.assign((size_t)Q.nlevels, 0);
-        const int cap = c->nsm * 8;
+        // resident CTAs of the FP32-storage backward kernel at its tile size
+        const size_t fast = (size_t)Q.gpc * Q.maxu * 32 * sweep_row_bytes(4, Q.ni, Q.T.max_nin > Q.ni);
+        int per_sm = 1;
+        if (Q.ni == 1)
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_q2<float, false, FIN_RZ, false, 1>,
+                                                             kThreads, fast));
+        else if (Q.ni == 2)
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_q2<float, false, FIN_RZ, false, 2>,
+                                                             kThreads, fast));
+        else
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_q2<float, false, FIN_RZ, false, 4>,
+                                                             kThreads, fast));
+        const int cap = c->nsm * std::max(1, per_sm);
         for (int l = 0; l < Q.nlevels; ++l) {
             const int groups = Q.level_g[(size_t)l + 1] - Q.level_g[(size_t)l];
             Q.g2grid[(size_t)l] = std::max(1, std::min(cap, (groups + Q.gpc - 1) / Q.gpc));

@@ -50,19 +50,23 @@ static void apply_ic0_q2(iccg_ctx* c, const double* r, double* y, double* z, Sol
 {
     QSys& Q = c->Q;
     RedBuf red{c->partials.get(), c->scalars.get()};
-    const size_t smem = (size_t)Q.gpc * Q.maxu * 32 * (24 + 12 * NI);
-    for (int l = 0; l < Q.nlevels; ++l)
-        launch_smem(c, 1, k_sweep_q2<T, true, FIN_NONE, true, NI>, Q.g2grid[(size_t)l], kThreads, smem,
-                    Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.maxu, (const int*)Q.gbase.get(),
-                    (const int*)Q.glen.get(), (const int*)Q.sl0.get(), S, d, r, y, (const double*)nullptr, 0, 0, st,
-                    red, c->ticket.get());
+    const size_t rows = (size_t)Q.gpc * Q.maxu * 32;
     // FP64 storage keeps the reference's backward order exactly
     constexpr bool exact = !std::is_same<T, float>::value;
+    const int fslow = Q.S.max_nin > NI ? 1 : 0;
+    const int bslow = (exact || Q.T.max_nin > NI) ? 1 : 0;
+    const size_t fsmem = rows * sweep_row_bytes(sizeof(T), NI, fslow != 0);
+    const size_t bsmem = rows * sweep_row_bytes(sizeof(T), NI, bslow != 0);
+    for (int l = 0; l < Q.nlevels; ++l)
+        launch_smem(c, 1, k_sweep_q2<T, true, FIN_NONE, true, NI>, Q.g2grid[(size_t)l], kThreads, fsmem,
+                    Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.maxu, fslow,
+                    (const int*)Q.gbase.get(), (const int*)Q.glen.get(), (const int*)Q.sl0.get(), S, d, r, y,
+                    (const double*)nullptr, 0, 0, st, red, c->ticket.get());
     for (int l = Q.nlevels - 1; l >= 0; --l)
-        launch_smem(c, 2, k_sweep_q2<T, false, FIN, exact, NI>, Q.g2grid[(size_t)l], kThreads, smem,
-                    Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.maxu, (const int*)Q.gbase.get(),
-                    (const int*)Q.glen.get(), (const int*)Q.sl0.get(), U, d, (const double*)y, z, r,
-                    Q.b2slot0[(size_t)l], Q.b2nslots, st, red, c->ticket.get());
+        launch_smem(c, 2, k_sweep_q2<T, false, FIN, exact, NI>, Q.g2grid[(size_t)l], kThreads, bsmem,
+                    Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.maxu, bslow,
+                    (const int*)Q.gbase.get(), (const int*)Q.glen.get(), (const int*)Q.sl0.get(), U, d,
+                    (const double*)y, z, r, Q.b2slot0[(size_t)l], Q.b2nslots, st, red, c->ticket.get());
 }
 
 template <class T, int FIN>
@@ -110,7 +114,7 @@ static void apply_path(iccg_ctx* c, int storage, const double* r, double* z, Sol
     }
     const double* inv = nullptr;
     if (c->pc_kind == ICCG_PRECOND_JACOBI) inv = c->use_q ? c->Q.inv_diag.get() : c->inv_diag.get();
-    launch(c, 3, k_diag_apply<FIN>, grid_for(c, c->n), kThreads, c->n, inv, r, z, st, red, c->ticket.get());
+    launch_n(c, 3, k_diag_apply<FIN>, (long long)c->n, c->n, inv, r, z, st, red, c->ticket.get());
 }
 
 // y = A x (spmv, cg_crs.cpp:54-79); FIN_PAP adds p.Ap, p.p, Ap.Ap
@@ -122,17 +126,17 @@ static void spmv_path(iccg_ctx* c, int storage, const double* x, double* y, Solv
     const int g = grid_for(c, c->n);
     if (c->use_q) {
         const SellMat A = c->Q.A.view(f32);
-        if (f32) launch(c, 0, k_spmv_q<float, FIN>, g, kThreads, c->n, A, x, y, st, red, c->ticket.get());
-        else launch(c, 0, k_spmv_q<double, FIN>, g, kThreads, c->n, A, x, y, st, red, c->ticket.get());
+        if (f32) launch_n(c, 0, k_spmv_q<float, FIN>, (long long)c->n, c->n, A, x, y, st, red, c->ticket.get());
+        else launch_n(c, 0, k_spmv_q<double, FIN>, (long long)c->n, c->n, A, x, y, st, red, c->ticket.get());
         return;
     }
     const int* rp = c->rowptr.get();
     const int* ci = c->colind.get();
     if (f32)
-        launch(c, 0, k_spmv<float, FIN>, g, kThreads, c->n, rp, ci, (const float*)c->val32.get(), x, y, st, red,
+        launch_n(c, 0, k_spmv<float, FIN>, (long long)c->n, c->n, rp, ci, (const float*)c->val32.get(), x, y, st, red,
                c->ticket.get());
     else
-        launch(c, 0, k_spmv<double, FIN>, g, kThreads, c->n, rp, ci, (const double*)c->val64.get(), x, y, st, red,
+        launch_n(c, 0, k_spmv<double, FIN>, (long long)c->n, c->n, rp, ci, (const double*)c->val64.get(), x, y, st, red,
                c->ticket.get());
 }
 
@@ -143,9 +147,9 @@ static void residual_path(iccg_ctx* c, const double* x, const double* b, double*
     RedBuf red{c->partials.get(), c->scalars.get()};
     const int g = grid_for(c, c->n);
     if (c->use_q)
-        launch(c, 4, k_residual_q<FIN>, g, kThreads, c->n, c->Q.A.view(false), x, b, r, st, red, c->ticket.get());
+        launch_n(c, 4, k_residual_q<FIN>, (long long)c->n, c->n, c->Q.A.view(false), x, b, r, st, red, c->ticket.get());
     else
-        launch(c, 4, k_residual<FIN>, g, kThreads, c->n, (const int*)c->rowptr.get(), (const int*)c->colind.get(),
+        launch_n(c, 4, k_residual<FIN>, (long long)c->n, c->n, (const int*)c->rowptr.get(), (const int*)c->colind.get(),
                (const double*)c->val64.get(), x, b, r, st, red, c->ticket.get());
 }
 
@@ -165,7 +169,7 @@ static double dot_dev(iccg_ctx* c, int n, const double* a, const double* b)
 {
     ensure_partials(c, (size_t)grid_for(c, n));
     RedBuf red{c->partials.get(), c->scalars.get()};
-    launch(c, 3, k_dot, grid_for(c, n), kThreads, n, a, b, red, c->ticket.get());
+    launch_n(c, 3, k_dot, (long long)n, n, a, b, red, c->ticket.get());
     CK(cudaMemcpyAsync(c->h_scalars, c->scalars.get(), sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     return c->h_scalars[0];
@@ -186,11 +190,11 @@ static void solve_plain(iccg_ctx* c, const double* b, double* x, int max_iter, d
     const int g = grid_for(c, n);
     RedBuf red{c->partials.get(), c->scalars.get()};
     spmv_path<FIN_NONE>(c, ICCG_STORE_FP64, x, Ax, nullptr);
-    launch(c, 3, k_sub, g, kThreads, n, b, (const double*)Ax, r);
+    launch_n(c, 3, k_sub, (long long)c->n, n, b, (const double*)Ax, r);
     double normb = std::sqrt(dot_dev(c, n, b, b));
     if (normb == 0.0) normb = 1.0;
     apply_path<FIN_NONE>(c, ICCG_STORE_FP64, r, z, nullptr);
-    launch(c, 3, k_copy, g, kThreads, n, (const double*)z, p, (SolverState*)nullptr);
+    launch_n(c, 3, k_copy, (long long)c->n, n, (const double*)z, p, (SolverState*)nullptr);
     double rz_old = dot_dev(c, n, r, z);
     res->iters = 0;
     res->converged = 0;
@@ -212,7 +216,7 @@ static void solve_plain(iccg_ctx* c, const double* b, double* x, int max_iter, d
             return;
         }
         const double alpha = rz_old / pAp;
-        launch(c, 3, k_update<FIN_NONE>, g, kThreads, n, alpha, (const double*)p, (const double*)Ap, x, r,
+        launch_n(c, 3, k_update<FIN_NONE>, (long long)c->n, n, alpha, (const double*)p, (const double*)Ap, x, r,
                (SolverState*)nullptr, red, c->ticket.get());
         const double rel = std::sqrt(dot_dev(c, n, r, r)) / normb;
         res->iters = k + 1;
@@ -225,7 +229,7 @@ static void solve_plain(iccg_ctx* c, const double* b, double* x, int max_iter, d
         apply_path<FIN_NONE>(c, ICCG_STORE_FP64, r, z, nullptr);
         const double rz_new = dot_dev(c, n, r, z);
         const double beta = rz_new / rz_old;
-        launch(c, 3, k_xpay, g, kThreads, n, beta, (const double*)z, p, (SolverState*)nullptr);
+        launch_n(c, 3, k_xpay, (long long)c->n, n, beta, (const double*)z, p, (SolverState*)nullptr);
         rz_old = rz_new;
     }
     res->status = kMaxIter;
@@ -241,11 +245,11 @@ static void fused_iteration(iccg_ctx* c, int storage, bool rr, const double* b, 
     SolverState* st = c->state.get();
     RedBuf red{c->partials.get(), c->scalars.get()};
     spmv_path<FIN_PAP>(c, storage, (const double*)c->vp.get(), c->vAp.get(), st);
-    launch(c, 3, k_update<FIN_UPD>, g, kThreads, n, 0.0, (const double*)c->vp.get(), (const double*)c->vAp.get(), x,
+    launch_n(c, 3, k_update<FIN_UPD>, (long long)c->n, n, 0.0, (const double*)c->vp.get(), (const double*)c->vAp.get(), x,
            c->vr.get(), st, red, c->ticket.get());
     if (rr) residual_path<FIN_TRUE>(c, (const double*)x, b, c->vr.get(), st);
     apply_path<FIN_RZ>(c, storage, c->vr.get(), c->vz.get(), st);
-    launch(c, 3, k_xpay, g, kThreads, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st);
+    launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st);
 }
 
 static void solve_fused(iccg_ctx* c, const double* b, double* x, int max_iter, double tol, const iccg_solve_opts& o,
@@ -269,7 +273,7 @@ static void solve_fused(iccg_ctx* c, const double* b, double* x, int max_iter, d
     // r0 = b - A x0, ||b||, z0 = M^{-1} r0, rz, p = z  (cg_crs.cpp:102-123)
     residual_path<FIN_INIT>(c, (const double*)x, b, c->vr.get(), st);
     apply_path<FIN_RZ0>(c, storage, c->vr.get(), c->vz.get(), st);
-    launch(c, 3, k_copy, g, kThreads, n, (const double*)c->vz.get(), c->vp.get(), st);
+    launch_n(c, 3, k_copy, (long long)c->n, n, (const double*)c->vz.get(), c->vp.get(), st);
 
     const int m = std::max(1, o.graph_iters);
     const bool use_graph = !c->profile;
@@ -358,8 +362,8 @@ static void solve_dev(iccg_ctx* c, const double* b, double* x, int max_iter, dou
     double* xp = x;
     const int g = grid_for(c, c->n);
     if (c->use_q) {
-        launch(c, 3, k_gather_vec, g, kThreads, c->n, (const int*)c->Q.dq2r.get(), b, c->qb.get());
-        launch(c, 3, k_gather_vec, g, kThreads, c->n, (const int*)c->Q.dq2r.get(), (const double*)x, c->qx.get());
+        launch_n(c, 3, k_gather_vec, (long long)c->n, c->n, (const int*)c->Q.dq2r.get(), b, c->qb.get());
+        launch_n(c, 3, k_gather_vec, (long long)c->n, c->n, (const int*)c->Q.dq2r.get(), (const double*)x, c->qx.get());
         bp = c->qb.get();
         xp = c->qx.get();
     }
@@ -381,7 +385,7 @@ static void solve_dev(iccg_ctx* c, const double* b, double* x, int max_iter, dou
         res->true_rel_resid = res->rel_resid;
     else
         res->true_rel_resid = true_resid(c, bp, xp);
-    if (c->use_q) launch(c, 3, k_scatter_vec, g, kThreads, c->n, (const int*)c->Q.dq2r.get(), (const double*)xp, x);
+    if (c->use_q) launch_n(c, 3, k_scatter_vec, (long long)c->n, c->n, (const int*)c->Q.dq2r.get(), (const double*)xp, x);
     CK(cudaStreamSynchronize(c->stream));
 }
 
@@ -392,9 +396,9 @@ static void apply_dev(iccg_ctx* c, int storage, const double* r, double* z)
     prepare_path(c, storage);
     const int g = grid_for(c, c->n);
     if (c->use_q) {
-        launch(c, 3, k_gather_vec, g, kThreads, c->n, (const int*)c->Q.dq2r.get(), r, c->qb.get());
+        launch_n(c, 3, k_gather_vec, (long long)c->n, c->n, (const int*)c->Q.dq2r.get(), r, c->qb.get());
         apply_path<FIN_NONE>(c, storage, c->qb.get(), c->qx.get(), nullptr);
-        launch(c, 3, k_scatter_vec, g, kThreads, c->n, (const int*)c->Q.dq2r.get(), (const double*)c->qx.get(), z);
+        launch_n(c, 3, k_scatter_vec, (long long)c->n, c->n, (const int*)c->Q.dq2r.get(), (const double*)c->qx.get(), z);
     } else {
         apply_path<FIN_NONE>(c, storage, r, z, nullptr);
     }
@@ -408,9 +412,9 @@ static void spmv_dev(iccg_ctx* c, int storage, const double* x, double* y)
     prepare_path(c, storage);
     const int g = grid_for(c, c->n);
     if (c->use_q) {
-        launch(c, 3, k_gather_vec, g, kThreads, c->n, (const int*)c->Q.dq2r.get(), x, c->qb.get());
+        launch_n(c, 3, k_gather_vec, (long long)c->n, c->n, (const int*)c->Q.dq2r.get(), x, c->qb.get());
         spmv_path<FIN_NONE>(c, storage, c->qb.get(), c->qx.get(), nullptr);
-        launch(c, 3, k_scatter_vec, g, kThreads, c->n, (const int*)c->Q.dq2r.get(), (const double*)c->qx.get(), y);
+        launch_n(c, 3, k_scatter_vec, (long long)c->n, c->n, (const int*)c->Q.dq2r.get(), (const double*)c->qx.get(), y);
     } else {
         spmv_path<FIN_NONE>(c, storage, x, y, nullptr);
     }
