@@ -61,6 +61,7 @@ struct SellDev {
     bool has32 = false;
     long long slots = 0;
     int max_nin = 0;       // most in-unit entries of a row (encoded matrices)
+    std::vector<int> h_ptr;  // host copy of ptr
     std::vector<int> src;  // host: CRS value index of each slot (-1: padding)
     SellMat view(bool fp32) const
     {
@@ -75,6 +76,7 @@ struct SellDev {
         slots = 0;
         max_nin = 0;
         src.clear();
+        h_ptr.clear();
     }
 };
 
@@ -93,6 +95,10 @@ struct QSys {
     Buf<int> gbase, glen, sl0;
     std::vector<int> h_gbase, h_glen, h_sl0;
     std::vector<std::pair<int, int>> steps;  // step slices: (first Q row, rows)
+    std::vector<int> step_r;                 // step index of each slice within its unit group
+    Buf<SliceMeta> meta;                     // per slice (two-phase sweeps)
+    int tile = 0;                            // slices of one two-phase batch (gpc * maxu)
+    int ks = 8;                              // entries loaded speculatively per row
     std::vector<int> unit_of, step_of;       // per A_run row: unit id, row index in the unit
     int maxu = 0;                            // longest unit
     bool two_phase = false;                  // S/T carry in-unit entries as -(step + 1)
@@ -124,6 +130,10 @@ struct QSys {
         h_glen.clear();
         h_sl0.clear();
         steps.clear();
+        step_r.clear();
+        meta.free();
+        tile = 0;
+        ks = 8;
         unit_of.clear();
         step_of.clear();
         maxu = 0;

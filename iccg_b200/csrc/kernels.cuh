@@ -544,94 +544,127 @@ __global__ void __launch_bounds__(256) k_sweep_q(int g0, int g1, const int* __re
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(rz, red, st, ticket, slot0 + blockIdx.x, nslots);
 }
 
+// Step slices of the two-phase sweeps: first Q row, SELL slot pointers of
+// the forward (S) and backward (T) matrices, and a packed word
+// rows | step << 6 | widthS << 12 | widthT << 20 (widths clamped to 255).
+struct SliceMeta {
+    int q0, pS, pT, w;
+};
+
 // Two-phase substitution over one level (groups [g0, g1)), used when every
 // unit has at most 64 rows.  Row lengths are stored as L | nint << 16 and the
 // nint in-unit entries of a row carry col = -(step + 1) (the unit's own row
 // at that step); they are the last entries of a forward row and the first of
 // a backward row, as in the reference's column order.
 //
-// A CTA (8 warps) takes gpc groups at a time (R = gpc * maxu * 32 rows).
-//  Phase A, all warps, one warp per (group, step) slice: each row's chain
-//    over its entries from earlier levels (values final, not written by
-//    this launch) is computed and parked in shared memory together with
-//    what the serial part needs: the pivot and the first NI in-unit entries.
-//  Phase B, one warp per group, walks the steps of its 32 units reading
-//    shared memory only: in-unit entries use the unit's earlier results,
-//    then the row divides by its pivot.  Rows with more than NI in-unit
-//    entries (and the exact backward order, below) read the rest of the row
-//    from global memory.
-//  Post-pass, all warps: results are stored and r.z is accumulated.
+// A CTA (8 warps) takes gpc groups at a time; their step slices are
+// consecutive, slices [sl0[gb], sl0[gb + gpc]), and map one-to-one onto a
+// shared tile of tile * 32 rows.
+//  Phase A, all warps, one warp per slice: one metadata load, then the
+//    slice's entries (loaded speculatively up to KS per row, coalesced),
+//    pivots and inputs; each row's chain over its entries from earlier
+//    levels (final values, not written by this launch) is computed; the
+//    partial value, pivot, row index, first NI in-unit entries and (with a
+//    reduction) r_q go to the tile.
+//  Phase B, one warp per group: the steps of its 32 units, reading the tile
+//    only: in-unit entries use the unit's earlier results, the row divides
+//    by its pivot, the result is stored and r.z accumulated.  Rows with more
+//    than NI in-unit entries, and the exact backward order, read the rest of
+//    the row from global memory.
 // Forward rows: earlier-level entries come first in the reference's order,
 // so the split keeps its bits.  Backward rows put the in-unit entries first;
 // EXACT keeps that order (phase B applies the earlier-level entries after the
 // in-unit ones); otherwise the earlier-level entries are applied first, in
 // phase A (the FP32-storage path, which has no reference rounding to keep).
-template <class T, bool FWD, int FIN, bool EXACT, int NI>
-__global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int maxu, int slow,
-                                                  const int* __restrict__ gbase, const int* __restrict__ glen,
-                                                  const int* __restrict__ sl0, SellMat M,
+template <class T, bool FWD, int FIN, bool EXACT, int NI, int KS>
+__global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int tile, int slow,
+                                                  const int* __restrict__ sl0, const int* __restrict__ glen,
+                                                  const SliceMeta* __restrict__ meta, SellMat M,
                                                   const T* __restrict__ dg, const double* __restrict__ in,
                                                   double* out, const double* __restrict__ rdot, int slot0,
                                                   int nslots, SolverState* st, RedBuf red, unsigned int* ticket)
 {
     if (st_done(st)) return;
-    // shared tile, R = gpc * maxu * 32 rows: partial sums / results (double),
-    // pivots and in-unit values (T), first slot and length word of each row
-    // (int, only when `slow`: rows with more than NI in-unit entries or the
-    // exact backward order), in-unit steps (int8, -1 if none)
+    constexpr bool ext_first = FWD || !EXACT;
+    constexpr bool with_r = FIN != FIN_NONE;
+    // tile layout: partial sums / results and r (double), pivots and in-unit
+    // values (T), row index, slow-path slot and length word (int), in-unit
+    // steps (int8, -1 if none)
     extern __shared__ double smem_d[];
-    const int R = gpc * maxu * 32;
+    const int R = tile * 32;
     double* s_acc = smem_d;
-    T* s_piv = reinterpret_cast<T*>(smem_d + R);
-    T* s_iv = s_piv + R;                                          // [NI][R]
-    int* s_p0 = reinterpret_cast<int*>(s_iv + NI * R);            // [R] if slow
-    int* s_lw = s_p0 + R;                                         // [R] if slow
+    double* s_rd = smem_d + R;                                       // [R] if with_r
+    T* s_piv = reinterpret_cast<T*>(smem_d + (with_r ? 2 : 1) * R);
+    T* s_iv = s_piv + R;                                             // [NI][R]
+    int* s_q = reinterpret_cast<int*>(s_iv + NI * R);                // [R]
+    int* s_p0 = s_q + R;                                             // [R] if slow
+    int* s_lw = s_p0 + R;                                            // [R] if slow
     signed char* s_ii = reinterpret_cast<signed char*>(slow ? s_lw + R : s_p0);  // [NI][R]
     const T* __restrict__ val = (const T*)M.val;
     const int* __restrict__ col = M.col;
     const int* __restrict__ mlen = M.len;
-    const int* __restrict__ mptr = M.ptr;
     const double* __restrict__ prev = out;  // earlier-level values: read-only in this launch
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr bool ext_first = FWD || !EXACT;
     acc2 rz[1] = {{0.0, 0.0}};
     for (int gb = g0 + blockIdx.x * gpc; gb < g1; gb += gridDim.x * gpc) {
         const int ng = min(gpc, g1 - gb);
+        const int sb = sl0[gb], se = sl0[gb + ng];
         // phase A
-        for (int t = warp; t < ng * maxu; t += 8) {
-            const int gl = t / maxu, r = t - gl * maxu;
-            const int g = gb + gl;
-            const int len = glen[(size_t)g * 32 + lane];
-            const int off = (int)__reduce_add_sync(0xffffffffu, (unsigned)min(len, r));
-            if (r < len) {
-                const int q = gbase[g] + off + lane;
+        for (int t = warp; t < se - sb; t += 8) {
+            const SliceMeta m = meta[sb + t];
+            const int cnt = m.w & 63;
+            const int w = FWD ? (m.w >> 12) & 255 : (m.w >> 20) & 255;
+            const int pb = (FWD ? m.pS : m.pT) + lane;
+            if (lane < cnt) {
+                const int q = m.q0 + lane;
+                const int rr = t * 32 + lane;
                 const int lw = mlen[q];
-                const int L = lw & 0xffff, ni = lw >> 16;
-                const int p0 = mptr[sl0[g] + r] + lane;
-                const int rr = (gl * maxu + r) * 32 + lane;
                 double a = in[q];
+                const T piv = dg[q];
+                double rq = 0.0;
+                if (with_r) rq = rdot[q];
+                int cj[KS];
+                T vj[KS];
+#pragma unroll
+                for (int j = 0; j < KS; ++j) {
+                    cj[j] = 0;
+                    vj[j] = (T)0;
+                    if (j < w) {
+                        cj[j] = col[pb + 32 * j];
+                        vj[j] = val[pb + 32 * j];
+                    }
+                }
+                const int L = lw & 0xffff, ni = lw >> 16;
                 if (ext_first) {
                     const int j0 = FWD ? 0 : ni, j1 = FWD ? L - ni : L;
-                    for (int j = j0; j < j1; ++j) {
-                        const int pa = p0 + 32 * j;
+                    double xg[KS];
+#pragma unroll
+                    for (int j = 0; j < KS; ++j) xg[j] = (j >= j0 && j < j1) ? __ldg(prev + cj[j]) : 0.0;
+#pragma unroll
+                    for (int j = 0; j < KS; ++j)
+                        if (j >= j0 && j < j1) a = fma(-(double)vj[j], xg[j], a);
+                    for (int j = max(KS, j0); j < j1; ++j) {
+                        const int pa = pb + 32 * j;
                         a = fma(-(double)val[pa], __ldg(prev + col[pa]), a);
                     }
                 }
                 s_acc[rr] = a;
-                s_piv[rr] = dg[q];
+                if (with_r) s_rd[rr] = rq;
+                s_piv[rr] = piv;
+                s_q[rr] = q;
                 const int jin = FWD ? L - ni : 0;
 #pragma unroll
                 for (int k = 0; k < NI; ++k) {
                     int idx = -1;
                     if (k < ni) {
-                        const int pa = p0 + 32 * (jin + k);
+                        const int pa = pb + 32 * (jin + k);
                         s_iv[k * R + rr] = val[pa];
                         idx = -col[pa] - 1;
                     }
                     s_ii[k * R + rr] = (signed char)idx;
                 }
                 if (slow) {
-                    s_p0[rr] = (ni > NI || !ext_first) ? p0 : -1;
+                    s_p0[rr] = (ni > NI || !ext_first) ? pb : -1;
                     s_lw[rr] = lw;
                 }
             }
@@ -639,10 +672,10 @@ __global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int m
         __syncthreads();
         // phase B
         if (warp < ng) {
-            const int gl = warp, g = gb + gl;
+            const int g = gb + warp;
             const int len = glen[(size_t)g * 32 + lane];
             const int maxlen = (int)__reduce_max_sync(0xffffffffu, (unsigned)len);
-            const int base = gl * maxu * 32 + lane;
+            const int base = (sl0[g] - sb) * 32 + lane;
             for (int t = 0; t < maxlen; ++t) {
                 const int r = FWD ? t : maxlen - 1 - t;
                 if (r < len) {
@@ -668,22 +701,11 @@ __global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int m
                                 a = fma(-(double)val[pa], __ldg(prev + col[pa]), a);
                             }
                     }
-                    s_acc[rr] = a / (double)s_piv[rr];
+                    const double v = a / (double)s_piv[rr];
+                    s_acc[rr] = v;
+                    out[s_q[rr]] = v;
+                    if (with_r) acc2_fma(rz[0], s_rd[rr], v);
                 }
-            }
-        }
-        __syncthreads();
-        // post-pass
-        for (int t = warp; t < ng * maxu; t += 8) {
-            const int gl = t / maxu, r = t - gl * maxu;
-            const int g = gb + gl;
-            const int len = glen[(size_t)g * 32 + lane];
-            const int off = (int)__reduce_add_sync(0xffffffffu, (unsigned)min(len, r));
-            if (r < len) {
-                const int q = gbase[g] + off + lane;
-                const double v = s_acc[(gl * maxu + r) * 32 + lane];
-                out[q] = v;
-                if (FIN != FIN_NONE) acc2_fma(rz[0], rdot[q], v);
             }
         }
         __syncthreads();

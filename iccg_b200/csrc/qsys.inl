@@ -72,6 +72,7 @@ static bool sell_build(iccg_ctx* c, const std::vector<std::pair<int, int>>& slic
             M.max_nin = std::max(M.max_nin, nin);
         }
     M.ptr.upload(ptr.data(), ptr.size(), &c->dev_bytes, c->stream);
+    M.h_ptr = ptr;
     M.col.upload(col.data(), col.size(), &c->dev_bytes, c->stream);
     M.len.upload(len.data(), len.size(), &c->dev_bytes, c->stream);
     M.slots = slot;
@@ -120,6 +121,7 @@ static void build_q_order(iccg_ctx* c)
     std::vector<U> units;
     Q.unit_of.assign((size_t)c->n, -1);
     Q.step_of.assign((size_t)c->n, 0);
+    Q.step_r.clear();
     Q.maxu = 0;
     int unit_id = 0;
     for (int l = 0; l < P.nlevels; ++l) {
@@ -141,6 +143,7 @@ static void build_q_order(iccg_ctx* c)
                 int cnt = 0;
                 while (g0 + (size_t)cnt < g1 && units[g0 + (size_t)cnt].m > r) ++cnt;
                 Q.steps.emplace_back((int)Q.q2r.size(), cnt);
+                Q.step_r.push_back(r);
                 for (int u = 0; u < cnt; ++u) {
                     const int row = P.h_rows[(size_t)(units[g0 + (size_t)u].t0 + r)];
                     Q.q2r.push_back(row);
@@ -156,10 +159,11 @@ static void build_q_order(iccg_ctx* c)
     }
     if ((int)Q.q2r.size() != c->n) throw Error(ICCG_ERR_SCHEDULE, "schedule does not cover every row once");
     Q.h_gbase.push_back((int)Q.q2r.size());
+    Q.h_sl0.push_back((int)Q.steps.size());
     Q.r2q.assign((size_t)c->n, -1);
     for (int q = 0; q < c->n; ++q) Q.r2q[(size_t)Q.q2r[(size_t)q]] = q;
     Q.nlevels = P.nlevels;
-    Q.ngroups = (int)Q.h_sl0.size();
+    Q.ngroups = (int)Q.h_sl0.size() - 1;
     Q.fgrid.assign((size_t)Q.nlevels, 1);
     Q.bslot0.assign((size_t)Q.nlevels, 0);
     const int cap = c->nsm * 8;
@@ -186,9 +190,9 @@ static void build_q_order(iccg_ctx* c)
 }
 
 // bytes per row of the two-phase sweep's shared tile (see k_sweep_q2)
-static size_t sweep_row_bytes(size_t tsize, int ni, bool slow)
+static size_t sweep_row_bytes(size_t tsize, int ni, bool slow, bool with_r)
 {
-    return 8 + tsize * (1 + (size_t)ni) + (slow ? 8 : 0) + (size_t)ni;
+    return 8 + (with_r ? 8 : 0) + tsize * (1 + (size_t)ni) + 4 + (slow ? 8 : 0) + (size_t)ni;
 }
 
 static void build_q_factor(iccg_ctx* c)
@@ -210,9 +214,9 @@ static void build_q_factor(iccg_ctx* c)
         // tile (R = gpc * maxu * 32 rows of 24 + 12 NI bytes) stays within
         // 48 KB and holds at most 1024 rows
         const int mx = std::max(Q.S.max_nin, Q.T.max_nin);
-        Q.ni = mx <= 1 ? 1 : mx <= 2 ? 2 : 4;
+        Q.ni = mx <= 1 ? 1 : 2;  // rows with more in-unit entries take the slow path
         // largest tile row: FP64 pivots and values plus the slow-path words
-        const size_t row_bytes = sweep_row_bytes(8, Q.ni, true);
+        const size_t row_bytes = sweep_row_bytes(8, Q.ni, true, true);
         const size_t per_group = (size_t)std::max(1, Q.maxu) * 32 * row_bytes;
         Q.gpc = (int)std::max<size_t>(
             1, std::min<size_t>({8, 48 * 1024 / per_group, 32 / (size_t)std::max(1, Q.maxu)}));
@@ -225,16 +229,26 @@ static void build_q_factor(iccg_ctx* c)
         Q.g2grid.assign((size_t)Q.nlevels, 1);
         Q.b2slot0.assign((size_t)Q.nlevels, 0);
         // resident CTAs of the FP32-storage backward kernel at its tile size
-        const size_t fast = (size_t)Q.gpc * Q.maxu * 32 * sweep_row_bytes(4, Q.ni, Q.T.max_nin > Q.ni);
+        Q.tile = Q.gpc * Q.maxu;
+        int wmax = 0;
+        for (size_t s = 0; s < Q.steps.size(); ++s)
+            wmax = std::max({wmax, (Q.S.h_ptr[s + 1] - Q.S.h_ptr[s]) / 32, (Q.T.h_ptr[s + 1] - Q.T.h_ptr[s]) / 32});
+        Q.ks = wmax <= 8 ? 8 : 16;
+        std::vector<SliceMeta> mt(Q.steps.size());
+        for (size_t s = 0; s < Q.steps.size(); ++s) {
+            const int ws = std::min(255, (Q.S.h_ptr[s + 1] - Q.S.h_ptr[s]) / 32);
+            const int wt = std::min(255, (Q.T.h_ptr[s + 1] - Q.T.h_ptr[s]) / 32);
+            mt[s] = SliceMeta{Q.steps[s].first, Q.S.h_ptr[s], Q.T.h_ptr[s],
+                              Q.steps[s].second | (Q.step_r[s] << 6) | (ws << 12) | (wt << 20)};
+        }
+        Q.meta.upload(mt.data(), mt.size(), &c->dev_bytes, c->stream);
+        const size_t fast = (size_t)Q.tile * 32 * sweep_row_bytes(4, Q.ni, Q.T.max_nin > Q.ni, true);
         int per_sm = 1;
         if (Q.ni == 1)
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_q2<float, false, FIN_RZ, false, 1>,
-                                                             kThreads, fast));
-        else if (Q.ni == 2)
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_q2<float, false, FIN_RZ, false, 2>,
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_q2<float, false, FIN_RZ, false, 1, 8>,
                                                              kThreads, fast));
         else
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_q2<float, false, FIN_RZ, false, 4>,
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_q2<float, false, FIN_RZ, false, 2, 8>,
                                                              kThreads, fast));
         const int cap = c->nsm * std::max(1, per_sm);
         for (int l = 0; l < Q.nlevels; ++l) {

@@ -44,28 +44,29 @@ static void apply_ic0_simple(iccg_ctx* c, const double* r, double* y, double* z,
 }
 
 // --- lane-interleaved substitutions -----------------------------------------
-template <class T, int FIN, int NI>
+template <class T, int FIN, int NI, int KS>
 static void apply_ic0_q2(iccg_ctx* c, const double* r, double* y, double* z, SolverState* st, const SellMat& S,
                          const SellMat& U, const T* d)
 {
     QSys& Q = c->Q;
     RedBuf red{c->partials.get(), c->scalars.get()};
-    const size_t rows = (size_t)Q.gpc * Q.maxu * 32;
+    const size_t rows = (size_t)Q.tile * 32;
     // FP64 storage keeps the reference's backward order exactly
     constexpr bool exact = !std::is_same<T, float>::value;
     const int fslow = Q.S.max_nin > NI ? 1 : 0;
     const int bslow = (exact || Q.T.max_nin > NI) ? 1 : 0;
-    const size_t fsmem = rows * sweep_row_bytes(sizeof(T), NI, fslow != 0);
-    const size_t bsmem = rows * sweep_row_bytes(sizeof(T), NI, bslow != 0);
+    const size_t fsmem = rows * sweep_row_bytes(sizeof(T), NI, fslow != 0, false);
+    const size_t bsmem = rows * sweep_row_bytes(sizeof(T), NI, bslow != 0, FIN != FIN_NONE);
+    const int* sl0 = Q.sl0.get();
+    const int* glen = Q.glen.get();
+    const SliceMeta* meta = Q.meta.get();
     for (int l = 0; l < Q.nlevels; ++l)
-        launch_smem(c, 1, k_sweep_q2<T, true, FIN_NONE, true, NI>, Q.g2grid[(size_t)l], kThreads, fsmem,
-                    Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.maxu, fslow,
-                    (const int*)Q.gbase.get(), (const int*)Q.glen.get(), (const int*)Q.sl0.get(), S, d, r, y,
-                    (const double*)nullptr, 0, 0, st, red, c->ticket.get());
+        launch_smem(c, 1, k_sweep_q2<T, true, FIN_NONE, true, NI, KS>, Q.g2grid[(size_t)l], kThreads, fsmem,
+                    Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.tile, fslow, sl0, glen, meta, S, d, r,
+                    y, (const double*)nullptr, 0, 0, st, red, c->ticket.get());
     for (int l = Q.nlevels - 1; l >= 0; --l)
-        launch_smem(c, 2, k_sweep_q2<T, false, FIN, exact, NI>, Q.g2grid[(size_t)l], kThreads, bsmem,
-                    Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.maxu, bslow,
-                    (const int*)Q.gbase.get(), (const int*)Q.glen.get(), (const int*)Q.sl0.get(), U, d,
+        launch_smem(c, 2, k_sweep_q2<T, false, FIN, exact, NI, KS>, Q.g2grid[(size_t)l], kThreads, bsmem,
+                    Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.tile, bslow, sl0, glen, meta, U, d,
                     (const double*)y, z, r, Q.b2slot0[(size_t)l], Q.b2nslots, st, red, c->ticket.get());
 }
 
@@ -78,11 +79,10 @@ static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, Solv
     const T* d = f32 ? (const T*)(const void*)Q.d32.get() : (const T*)(const void*)Q.d64.get();
     const SellMat S = Q.S.view(f32), U = Q.T.view(f32);
     if (Q.two_phase) {
-        switch (Q.ni) {
-            case 1: apply_ic0_q2<T, FIN, 1>(c, r, y, z, st, S, U, d); break;
-            case 2: apply_ic0_q2<T, FIN, 2>(c, r, y, z, st, S, U, d); break;
-            default: apply_ic0_q2<T, FIN, 4>(c, r, y, z, st, S, U, d); break;
-        }
+        if (Q.ni == 1 && Q.ks == 8) apply_ic0_q2<T, FIN, 1, 8>(c, r, y, z, st, S, U, d);
+        else if (Q.ni == 1) apply_ic0_q2<T, FIN, 1, 16>(c, r, y, z, st, S, U, d);
+        else if (Q.ks == 8) apply_ic0_q2<T, FIN, 2, 8>(c, r, y, z, st, S, U, d);
+        else apply_ic0_q2<T, FIN, 2, 16>(c, r, y, z, st, S, U, d);
         return;
     }
     for (int l = 0; l < Q.nlevels; ++l)
