@@ -133,6 +133,7 @@ def lib() -> C.CDLL:
         "iccg_spmv": (_I, [_P, _P, _P, _I]),
         "iccg_spmv_dev": (_I, [_P, _P, _P, _I]),
         "iccg_dot_dev": (_I, [_P, _I, _P, _P, C.POINTER(_D)]),
+        "iccg_dot_dev_noalloc": (_I, [_I, _P, _P, _P, _P]),
         "iccg_solve": (_I, [_P, _P, _P, _I, _D, C.POINTER(_Opts), C.POINTER(_Result)]),
         "iccg_solve_dev": (_I, [_P, _P, _P, _I, _D, C.POINTER(_Opts), C.POINTER(_Result)]),
         "iccg_profile_enable": (_I, [_P, _I]),

@@ -241,6 +241,26 @@ int iccg_spmv_dev(iccg_ctx* ctx, const double* x, double* y, int storage);
    and rounded once to double */
 int iccg_dot_dev(iccg_ctx* ctx, int n, const double* a, const double* b, double* out);
 
+/* iccg_dot_dev without a context and without any device allocation.  No
+   counterpart in the reference: it exists for callers that cannot call
+   cudaMalloc (a host whose allocator has reserved the device memory for its
+   own pool, or a latency-bound loop in which the device-wide
+   synchronisation of cudaMalloc/cudaFree is not allowed).
+   a, b: n doubles in device memory; out: one double in device memory,
+   written asynchronously on `stream` (a cudaStream_t, NULL = default
+   stream).  The same double-double evaluation as iccg_dot_dev; each block
+   of 4096 elements is summed by one CTA, so the result depends only on the
+   inputs.  Its scratch is a fixed static device array (64 KiB) inside the
+   library, which limits n to ICCG_NOALLOC_MAX_N; larger n is rejected with
+   ICCG_ERR_ARG (message via iccg_last_error).
+   The first call on each device does a set-up (finds the scratch address
+   and clears its counter, synchronising `stream`); make it before any
+   stream capture.  Calls that overlap in time on one device (two host
+   threads, or two streams running concurrently) share the scratch and race:
+   serialise them. */
+#define ICCG_NOALLOC_MAX_N 16777216
+int iccg_dot_dev_noalloc(int n, const double* a, const double* b, double* out, void* stream);
+
 /* conjugate_gradient<Precond> (cg_crs.cpp:89-162) on A_run with the built
    preconditioner and schedule.  x holds x0 on entry and the solution on
    return.  opts may be NULL (FUSED, FP64, rr 50, graph 8). */
