@@ -50,6 +50,7 @@ PRECOND_NONE, PRECOND_JACOBI, PRECOND_IC0 = 0, 1, 2
 STORE_FP64, STORE_FP32 = 0, 1
 MODE_PLAIN, MODE_FUSED = 0, 1
 OPT_TILED = 0
+OPT_SWEEP = 1
 STATUS_NAMES = {0: "converged", 1: "breakdown", 2: "max_iter", 3: "nonfinite"}
 
 

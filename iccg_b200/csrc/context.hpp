@@ -63,6 +63,10 @@ struct SellDev {
     int max_nin = 0;       // most in-unit entries of a row (encoded matrices)
     std::vector<int> h_ptr;  // host copy of ptr
     std::vector<int> src;  // host: CRS value index of each slot (-1: padding)
+    // host, encoded matrices: per Q row, 1 when the row has at most one
+    // in-unit entry and that entry is the unit's row one step before it in
+    // the sweep's order
+    std::vector<unsigned char> prev_only;
     SellMat view(bool fp32) const
     {
         return SellMat{ptr.get(), col.get(), fp32 ? (const void*)v32.get() : (const void*)v64.get(), len.get()};
@@ -77,6 +81,7 @@ struct SellDev {
         max_nin = 0;
         src.clear();
         h_ptr.clear();
+        prev_only.clear();
     }
 };
 
@@ -106,6 +111,17 @@ struct QSys {
     int ni = 1;                              // in-unit entries staged per row (1, 2 or 4)
     std::vector<int> g2grid, b2slot0;        // its grids and backward reduction slots
     int b2nslots = 0;
+    // staged sweeps (k_sweep_st): batches of groups, per-level buffer
+    // capacities, and grids / backward reduction slots per value type
+    // ([0] FP64, [1] FP32)
+    bool staged = false;
+    Buf<BatchDesc> bdesc;
+    std::vector<int> lb;                                  // first batch of each level (nlevels + 1)
+    std::vector<int> st_rows, st_slotsS, st_slotsT, st_slices;
+    std::vector<int> st_fgrid[2], st_bgrid[2], st_bslot0[2];
+    int st_bnslots[2] = {0, 0};
+    Buf<float> r32;                                       // FP32 reciprocal pivots
+    bool r32_ok = false;
     // matrices
     SellDev A, S, T;
     Buf<double> d64, inv_diag;
@@ -142,6 +158,18 @@ struct QSys {
         g2grid.clear();
         b2slot0.clear();
         b2nslots = 0;
+        staged = false;
+        bdesc.free();
+        lb.clear();
+        for (auto* v : {&st_rows, &st_slotsS, &st_slotsT, &st_slices}) v->clear();
+        for (int k = 0; k < 2; ++k) {
+            st_fgrid[k].clear();
+            st_bgrid[k].clear();
+            st_bslot0[k].clear();
+            st_bnslots[k] = 0;
+        }
+        r32.free();
+        r32_ok = false;
         A.reset();
         S.reset();
         T.reset();
@@ -175,6 +203,8 @@ struct iccg_ctx {
     iccg::Plan fwd, bwd;
     // lane-interleaved system (default) or the simple one-thread-per-row path
     bool use_q = true;
+    int sweep_kernel = 0;   // ICCG_OPT_SWEEP: 0 staged where it fits, 1 two-phase per-slice kernel
+    int smem_optin = 0;     // largest dynamic shared memory per CTA
     iccg::QSys Q;
     // preconditioner
     int pc_kind = -1;

@@ -71,6 +71,7 @@ int iccg_ctx_create(int device, iccg_ctx** out)
         CK(cudaGetDeviceCount(&ndev));
         if (device < 0 || device >= ndev) throw Error(ICCG_ERR_ARG, "no such CUDA device");
         CK(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
+        CK(cudaDeviceGetAttribute(&c->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
         CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
         CK(cudaEventCreate(&c->ev0));
         CK(cudaEventCreate(&c->ev1));
@@ -126,8 +127,14 @@ long long iccg_ctx_device_bytes(const iccg_ctx* c) { return c ? c->dev_bytes : 0
 int iccg_ctx_set_option(iccg_ctx* c, int option, long long value)
 {
     return guard(c, [&] {
-        if (option != ICCG_OPT_TILED) throw Error(ICCG_ERR_ARG, "unknown option");
-        c->use_q = value != 0;
+        if (option == ICCG_OPT_TILED) {
+            c->use_q = value != 0;
+        } else if (option == ICCG_OPT_SWEEP) {
+            if (value != 0 && value != 1) throw Error(ICCG_ERR_ARG, "ICCG_OPT_SWEEP takes 0 or 1");
+            c->sweep_kernel = (int)value;
+        } else {
+            throw Error(ICCG_ERR_ARG, "unknown option");
+        }
         drop_graph(c);
     });
 }

@@ -713,6 +713,382 @@ __global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int t
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(rz, red, st, ticket, slot0 + blockIdx.x, nslots);
 }
 
+// ---------------------------------------------------------------------------
+// Staged substitution over one level (the default when a batch fits shared
+// memory).
+//
+// A batch is up to 16 consecutive groups of one level.  Its Q rows [qb, qe),
+// its step slices [sb, se) and the SELL slots of those slices are contiguous,
+// so everything the batch reads except the earlier-level values is a handful
+// of contiguous ranges: slice metadata, inputs, r (with a reduction), pivots,
+// row words, column indices and values.  A CTA takes batches b0 + blockIdx.x,
+// + gridDim.x, ... and copies batch i + 1 into the other half of a double
+// buffer with cp.async (16-byte chunks, nothing held in registers) while it
+// works on batch i:
+//  G, all warps, one slice per warp and UG slices at a time: the
+//    earlier-level values of each row's entries are gathered (the only
+//    scattered reads) and folded into the row's partial sum in the tile, or,
+//    for the exact backward order, parked beside the entries; the row's
+//    in-unit entries (count, first two steps and values) are packed for C;
+//  C, one warp per group and one lane per unit: the in-unit chains, from
+//    the tile only; each result goes to out and stays in the tile for the
+//    unit's later steps; r.z is accumulated.
+// The order of the floating-point operations of every row is the one of
+// k_sweep_q2 (and of the reference for EXACT).  Without EXACT (FP32
+// storage) dg holds reciprocal pivots and the division is a product.
+// ---------------------------------------------------------------------------
+struct BatchDesc {
+    int sb, se;    // step slices [sb, se)
+    int qb, qe;    // Q rows [qb, qe)
+    int ps0, ps1;  // SELL slots of the slices in S (forward matrix)
+    int pt0, pt1;  // SELL slots of the slices in T (backward matrix)
+    int gb, ng;    // groups [gb, gb + ng), ng <= 16
+    int flags;     // bit 0 / 1: forward / backward chains are regular (below)
+    int pad1;
+};
+
+// Byte offsets of one stage buffer.  Row arrays get room for the 16-byte
+// alignment of their first and last chunk; slot ranges start on a slice
+// boundary (a multiple of 32 slots), so only their end is rounded.
+struct StageLayout {
+    int meta, in, rd, piv, len, col, val, pv, iw, iv, bytes;
+};
+
+__host__ __device__ inline int stage_al16(int x) { return (x + 15) & ~15; }
+
+__host__ __device__ inline StageLayout stage_layout(int rows, int slots, int slices, int tsize, bool with_r,
+                                                    bool with_pv)
+{
+    StageLayout L;
+    int o = 0;
+    L.meta = o;
+    o += stage_al16(slices * 16);
+    L.in = o;
+    o += stage_al16((rows + 4) * 8);
+    L.rd = o;
+    if (with_r) o += stage_al16((rows + 4) * 8);
+    L.piv = o;
+    o += stage_al16((rows + 8) * tsize);
+    L.len = o;
+    o += stage_al16((rows + 8) * 4);
+    L.col = o;
+    o += stage_al16((slots + 4) * 4);
+    L.val = o;
+    o += stage_al16((slots + 4) * tsize);
+    L.pv = o;
+    if (with_pv) o += stage_al16(slots * 8);
+    L.iw = o;  // per row: in-unit count and the steps of the first two in-unit entries
+    o += stage_al16(rows * 4);
+    L.iv = o;  // per row: the values of those two entries
+    o += stage_al16(2 * rows * tsize);
+    L.bytes = o;
+    return L;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Copies elements [first, first + count) of src (esize bytes each) into dst
+// in 16-byte chunks, starting at the chunk that holds `first`; returns the
+// element offset of `first` in dst.
+__device__ __forceinline__ int stage_range(unsigned char* dst, const void* src, int esize, int first, int count)
+{
+    const int per = 16 / esize;
+    const int a0 = first & ~(per - 1);
+    const int a1 = (first + count + per - 1) & ~(per - 1);
+    const int chunks = (a1 - a0) / per;
+    const unsigned char* s = (const unsigned char*)src + (size_t)a0 * esize;
+    for (int k = threadIdx.x; k < chunks; k += blockDim.x) cp_async16(dst + 16 * k, s + 16 * k);
+    return first - a0;
+}
+
+template <class T, bool FWD, bool WITH_R>
+__device__ __forceinline__ void stage_batch(unsigned char* base, const StageLayout& Ly, const BatchDesc& d,
+                                            const SliceMeta* meta, const SellMat& M, const T* dg,
+                                            const double* in, const double* rdot)
+{
+    const int rows = d.qe - d.qb;
+    const int p0 = FWD ? d.ps0 : d.pt0, p1 = FWD ? d.ps1 : d.pt1;
+    stage_range(base + Ly.meta, meta, 16, d.sb, d.se - d.sb);
+    stage_range(base + Ly.in, in, 8, d.qb, rows);
+    if (WITH_R) stage_range(base + Ly.rd, rdot, 8, d.qb, rows);
+    stage_range(base + Ly.piv, dg, (int)sizeof(T), d.qb, rows);
+    stage_range(base + Ly.len, M.len, 4, d.qb, rows);
+    stage_range(base + Ly.col, M.col, 4, p0, p1 - p0);
+    stage_range(base + Ly.val, M.val, (int)sizeof(T), p0, p1 - p0);
+    cp_async_commit();
+}
+
+template <class T, bool FWD, int FIN, bool EXACT>
+__global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDesc* __restrict__ bd, int rows_cap,
+                                                  int slots_cap, int slices_cap, const int* __restrict__ sl0,
+                                                  const int* __restrict__ glen, const SliceMeta* __restrict__ meta,
+                                                  SellMat M, const T* __restrict__ dg, const double* __restrict__ in,
+                                                  double* out, const double* __restrict__ rdot, int slot0,
+                                                  int nslots, SolverState* st, RedBuf red, unsigned int* ticket)
+{
+    if (st_done(st)) return;
+    constexpr bool with_r = FIN != FIN_NONE;
+    constexpr bool ext_first = FWD || !EXACT;
+    constexpr bool with_pv = !ext_first;
+    constexpr int UG = 2;  // slices per warp in flight in G
+    constexpr int KG = 4;  // earlier-level entries per row gathered at once
+    extern __shared__ __align__(16) unsigned char smem_st[];
+    const StageLayout Ly = stage_layout(rows_cap, slots_cap, slices_cap, (int)sizeof(T), with_r, with_pv);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double* prev = out;  // earlier-level values: read-only in this launch
+    acc2 rz[1] = {{0.0, 0.0}};
+
+    int b = b0 + blockIdx.x;
+    if (b < b1) {
+        BatchDesc cur = bd[b];
+        stage_batch<T, FWD, with_r>(smem_st, Ly, cur, meta, M, dg, in, rdot);
+        bool has_next = b + (int)gridDim.x < b1;
+        BatchDesc nxt = cur;
+        if (has_next) nxt = bd[b + gridDim.x];
+        for (int i = 0;; ++i) {
+            unsigned char* base = smem_st + (i & 1) * Ly.bytes;
+            if (has_next) stage_batch<T, FWD, with_r>(smem_st + ((i + 1) & 1) * Ly.bytes, Ly, nxt, meta, M, dg, in, rdot);
+            const bool has_nn = has_next && b + 2 * (int)gridDim.x < b1;
+            BatchDesc nn = nxt;
+            if (has_nn) nn = bd[b + 2 * gridDim.x];
+            // group words for C (latency overlaps the wait)
+            int gl[2] = {0, 0}, gs[2] = {0, 0};
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int gi = warp + 8 * k;
+                if (gi < cur.ng) {
+                    gl[k] = glen[(size_t)(cur.gb + gi) * 32 + lane];
+                    gs[k] = sl0[cur.gb + gi];
+                }
+            }
+            if (has_next) cp_async_wait<1>();
+            else cp_async_wait<0>();
+            __syncthreads();
+
+            const SliceMeta* s_meta = reinterpret_cast<const SliceMeta*>(base + Ly.meta);
+            double* s_in = reinterpret_cast<double*>(base + Ly.in) + (cur.qb & 1);
+            const double* s_rd = reinterpret_cast<const double*>(base + Ly.rd) + (cur.qb & 1);
+            const T* s_piv = reinterpret_cast<const T*>(base + Ly.piv) + (cur.qb & (16 / (int)sizeof(T) - 1));
+            const int* s_len = reinterpret_cast<const int*>(base + Ly.len) + (cur.qb & 3);
+            const int* s_col = reinterpret_cast<const int*>(base + Ly.col);
+            const T* s_val = reinterpret_cast<const T*>(base + Ly.val);
+            double* s_pv = reinterpret_cast<double*>(base + Ly.pv);
+            int* s_iw = reinterpret_cast<int*>(base + Ly.iw);
+            T* s_iv = reinterpret_cast<T*>(base + Ly.iv);
+            const int p0 = FWD ? cur.ps0 : cur.pt0;
+            const int ns = cur.se - cur.sb;
+
+            // G: earlier-level entries
+            for (int t0 = warp; t0 < ns; t0 += 8 * UG) {
+                int rr[UG], e[UG], j0[UG], j1[UG];
+                bool act[UG];
+#pragma unroll
+                for (int u = 0; u < UG; ++u) {
+                    const int t = t0 + 8 * u;
+                    act[u] = false;
+                    rr[u] = e[u] = j0[u] = j1[u] = 0;
+                    if (t < ns) {
+                        const SliceMeta m = s_meta[t];
+                        if (lane < (m.w & 63)) {
+                            act[u] = true;
+                            rr[u] = m.q0 - cur.qb + lane;
+                            const int lw = s_len[rr[u]];
+                            const int L = lw & 0xffff, ni = lw >> 16;
+                            e[u] = (FWD ? m.pS : m.pT) - p0 + lane;
+                            j0[u] = FWD ? 0 : ni;
+                            j1[u] = FWD ? L - ni : L;
+                        }
+                    }
+                }
+                double x[UG][KG];
+#pragma unroll
+                for (int u = 0; u < UG; ++u)
+#pragma unroll
+                    for (int j = 0; j < KG; ++j)
+                        x[u][j] = (act[u] && j0[u] + j < j1[u]) ? __ldg(prev + s_col[e[u] + 32 * (j0[u] + j)]) : 0.0;
+                // in-unit entries of the row, for the chain: count and first two (step, value)
+#pragma unroll
+                for (int u = 0; u < UG; ++u) {
+                    if (!act[u]) continue;
+                    const int ni = FWD ? s_len[rr[u]] >> 16 : j0[u];
+                    const int jin = FWD ? j1[u] : 0;
+                    int w = ni << 16;
+                    T v0 = (T)0, v1 = (T)0;
+                    if (ni > 0) {
+                        w |= -s_col[e[u] + 32 * jin] - 1;
+                        v0 = s_val[e[u] + 32 * jin];
+                    }
+                    if (ni > 1) {
+                        w |= (-s_col[e[u] + 32 * (jin + 1)] - 1) << 8;
+                        v1 = s_val[e[u] + 32 * (jin + 1)];
+                    }
+                    s_iw[rr[u]] = w;
+                    s_iv[rr[u]] = v0;
+                    s_iv[rows_cap + rr[u]] = v1;
+                }
+#pragma unroll
+                for (int u = 0; u < UG; ++u) {
+                    if (!act[u]) continue;
+                    if (ext_first) {
+                        double a = s_in[rr[u]];
+#pragma unroll
+                        for (int j = 0; j < KG; ++j)
+                            if (j0[u] + j < j1[u]) a = fma(-(double)s_val[e[u] + 32 * (j0[u] + j)], x[u][j], a);
+                        for (int jj = j0[u] + KG; jj < j1[u]; ++jj) {
+                            const int ej = e[u] + 32 * jj;
+                            a = fma(-(double)s_val[ej], __ldg(prev + s_col[ej]), a);
+                        }
+                        s_in[rr[u]] = a;
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < KG; ++j)
+                            if (j0[u] + j < j1[u]) s_pv[e[u] + 32 * (j0[u] + j)] = x[u][j];
+                        for (int jj = j0[u] + KG; jj < j1[u]; ++jj) {
+                            const int ej = e[u] + 32 * jj;
+                            s_pv[ej] = __ldg(prev + s_col[ej]);
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+
+            // C, regular batches: every group has 32 units of one length and
+            // every in-unit entry is the row one step earlier in the sweep, so
+            // step r of a group is tile row base + 32 r and the chain is one
+            // fused multiply-add (selected by the row's in-unit count) and one
+            // division / product per step, with no branches.  (The exact
+            // backward order applies earlier-level entries inside the chain
+            // and takes the general path.)
+            if (ext_first && (cur.flags & (FWD ? 1 : 2))) {
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    const int gi = warp + 8 * k;
+                    if (gi >= cur.ng) break;
+                    const int len = gl[k];
+                    const int base = s_meta[gs[k] - cur.sb].q0 - cur.qb + lane;
+                    double last = 0.0;
+#pragma unroll 8
+                    for (int t = 0; t < len; ++t) {
+                        const int rr = base + 32 * (FWD ? t : len - 1 - t);
+                        double a = s_in[rr];
+                        const double x = fma(-(double)s_iv[rr], last, a);
+                        a = (s_iw[rr] >> 16) ? x : a;
+                        const double v = EXACT ? a / (double)s_piv[rr] : a * (double)s_piv[rr];
+                        s_in[rr] = v;
+                        out[cur.qb + rr] = v;
+                        if (with_r) acc2_fma(rz[0], s_rd[rr], v);
+                        last = v;
+                    }
+                }
+            } else {
+            // C, general batches: in-unit chains of any shape.  The steps'
+            // first Q rows sit in two registers per lane (steps lane and
+            // lane + 32, shuffled out).
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int gi = warp + 8 * k;
+                if (gi >= cur.ng) break;
+                const int len = gl[k];
+                const int sbase = gs[k] - cur.sb;
+                const int maxlen = (int)__reduce_max_sync(0xffffffffu, (unsigned)len);
+                const int qlo = lane < maxlen ? s_meta[sbase + lane].q0 - cur.qb : 0;
+                const int qhi = lane + 32 < maxlen ? s_meta[sbase + lane + 32].q0 - cur.qb : 0;
+                // row of step r for this lane; the shuffle needs the whole
+                // warp, so only warp-uniform code (fetch) may call it
+                auto row_of = [&](int r) {
+                    const int q = __shfl_sync(0xffffffffu, r < 32 ? qlo : qhi, r & 31);
+                    return q + lane;
+                };
+                // the same from the staged metadata, for per-lane code
+                auto row_at = [&](int r) { return s_meta[sbase + r].q0 - cur.qb + lane; };
+                double last = 0.0;
+                int lastr = -1;
+                struct Step {
+                    int rr, w;
+                    double a, rd, p, v0, v1;
+                };
+                auto fetch = [&](int t, Step& S) {
+                    const int r = FWD ? t : maxlen - 1 - t;
+                    S.rr = t < maxlen ? row_of(r) : 0;
+                    if (t < maxlen && r < len) {
+                        S.a = s_in[S.rr];
+                        S.p = (double)s_piv[S.rr];
+                        S.w = s_iw[S.rr];
+                        S.v0 = (double)s_iv[S.rr];
+                        S.v1 = (double)s_iv[rows_cap + S.rr];
+                        if (with_r) S.rd = s_rd[S.rr];
+                    }
+                };
+                // value of the unit's row at step idx: the register for the
+                // step just done, else the tile (a volatile load, so that it
+                // is only issued on the lanes and steps that need it and
+                // never sits in front of the chain)
+                auto unit_value = [&](int idx) {
+                    double x = last;
+                    if (idx != lastr) x = *reinterpret_cast<volatile const double*>(s_in + row_at(idx));
+                    return x;
+                };
+                auto step = [&](int t, const Step& S) {
+                    const int r = FWD ? t : maxlen - 1 - t;
+                    if (r >= len) return;
+                    double a = S.a;
+                    const int ni = S.w >> 16;
+                    if (ni > 0) a = fma(-S.v0, unit_value(S.w & 0xff), a);
+                    if (ni > 1) a = fma(-S.v1, unit_value((S.w >> 8) & 0xff), a);
+                    if (ni > 2 || !ext_first) {
+                        // more in-unit entries, and the exact backward order's
+                        // earlier-level entries: from the staged row
+                        const SliceMeta m = s_meta[sbase + r];
+                        const int L = s_len[S.rr] & 0xffff;
+                        const int e0 = (FWD ? m.pS : m.pT) - p0 + lane;
+                        const int jin = FWD ? L - ni : 0;
+                        for (int k2 = 2; k2 < ni; ++k2) {
+                            const int ek = e0 + 32 * (jin + k2);
+                            a = fma(-(double)s_val[ek], unit_value(-s_col[ek] - 1), a);
+                        }
+                        if (!ext_first)
+                            for (int j = ni; j < L; ++j) {
+                                const int ej = e0 + 32 * j;
+                                a = fma(-(double)s_val[ej], s_pv[ej], a);
+                            }
+                    }
+                    const double v = EXACT ? a / S.p : a * S.p;
+                    s_in[S.rr] = v;
+                    out[cur.qb + S.rr] = v;
+                    if (with_r) acc2_fma(rz[0], S.rd, v);
+                    last = v;
+                    lastr = r;
+                };
+                for (int t = 0; t < maxlen; ++t) {
+                    Step A{};
+                    fetch(t, A);
+                    step(t, A);
+                }
+            }
+            }
+            __syncthreads();
+            if (!has_next) break;
+            b += gridDim.x;
+            cur = nxt;
+            nxt = nn;
+            has_next = has_nn;
+        }
+    }
+    if (FIN != FIN_NONE) reduce_finish<1, FIN>(rz, red, st, ticket, slot0 + blockIdx.x, nslots);
+}
+
 // out[q] = in[perm[q]] (gather into Q order) / out[perm[q]] = in[q] (scatter)
 __global__ void __launch_bounds__(256) k_gather_vec(int n, const int* __restrict__ perm,
                                                     const double* __restrict__ in, double* __restrict__ out)
@@ -814,6 +1190,13 @@ __global__ void __launch_bounds__(256) k_to_f32(long long m, const double* __res
 {
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < m; k += (long long)gridDim.x * blockDim.x)
         out[k] = (float)src[k];
+}
+
+// out[k] = (float)(1 / src[k]): reciprocal pivots of the FP32-storage sweeps
+__global__ void __launch_bounds__(256) k_recip_f32(long long m, const double* __restrict__ src, float* __restrict__ out)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < m; k += (long long)gridDim.x * blockDim.x)
+        out[k] = (float)(1.0 / src[k]);
 }
 
 }  // namespace iccg

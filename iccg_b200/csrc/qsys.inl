@@ -50,6 +50,7 @@ static bool sell_build(iccg_ctx* c, const std::vector<std::pair<int, int>>& slic
     std::vector<int> col((size_t)slot, 0);
     M.src.assign((size_t)slot, -1);
     M.max_nin = 0;
+    M.prev_only.assign(encode ? (size_t)n : 0, 0);
     for (size_t s = 0; s < slices.size(); ++s)
         for (int l = 0; l < slices[s].second; ++l) {
             const int q = slices[s].first + l;
@@ -57,12 +58,14 @@ static bool sell_build(iccg_ctx* c, const std::vector<std::pair<int, int>>& slic
             const int b = rp[(size_t)r], L = rp[(size_t)r + 1] - b;
             if (L > 0xffff) throw Error(ICCG_ERR_ARG, "row longer than 65535 entries");
             int nin = 0;
+            bool prev = true;
             for (int j = 0; j < L; ++j) {
                 const size_t pos = (size_t)ptr[s] + 32 * (size_t)j + (size_t)l;
                 const int cj = ci[(size_t)b + j];
                 if (encode && Q.unit_of[(size_t)cj] == Q.unit_of[(size_t)r]) {
                     col[pos] = -(Q.step_of[(size_t)cj] + 1);
                     ++nin;
+                    prev = prev && Q.step_of[(size_t)cj] == Q.step_of[(size_t)r] + (encode == 1 ? -1 : 1);
                 } else {
                     col[pos] = Q.r2q[(size_t)cj];
                 }
@@ -70,6 +73,7 @@ static bool sell_build(iccg_ctx* c, const std::vector<std::pair<int, int>>& slic
             }
             len[(size_t)q] = L | (nin << 16);
             M.max_nin = std::max(M.max_nin, nin);
+            if (encode) M.prev_only[(size_t)q] = (unsigned char)(prev && nin <= 1);
         }
     M.ptr.upload(ptr.data(), ptr.size(), &c->dev_bytes, c->stream);
     M.h_ptr = ptr;
@@ -195,6 +199,120 @@ static size_t sweep_row_bytes(size_t tsize, int ni, bool slow, bool with_r)
     return 8 + (with_r ? 8 : 0) + tsize * (1 + (size_t)ni) + 4 + (slow ? 8 : 0) + (size_t)ni;
 }
 
+// Raises a kernel's dynamic shared-memory limit to the device's opt-in
+// maximum less its static shared memory (once per kernel and device).
+template <class K>
+static void allow_smem(iccg_ctx* c, K kernel)
+{
+    static std::vector<std::pair<const void*, int>> done;
+    const void* key = reinterpret_cast<const void*>(kernel);
+    for (auto& e : done)
+        if (e.first == key && e.second == c->device) return;
+    cudaFuncAttributes fa{};
+    CK(cudaFuncGetAttributes(&fa, kernel));
+    const int dyn = c->smem_optin - (int)fa.sharedSizeBytes;
+    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+    done.push_back({key, c->device});
+}
+
+// Grids of the staged sweeps for value type T at each level: one CTA per
+// batch up to what is resident at once at that level's buffer size.
+template <class T>
+static bool plan_staged_type(iccg_ctx* c, int k)
+{
+    QSys& Q = c->Q;
+    constexpr bool exact = !std::is_same<T, float>::value;
+    auto kf = k_sweep_st<T, true, FIN_NONE, exact>;
+    auto kb = k_sweep_st<T, false, FIN_RZ, exact>;
+    allow_smem(c, kf);
+    allow_smem(c, kb);
+    const int L = Q.nlevels;
+    Q.st_fgrid[k].assign((size_t)L, 1);
+    Q.st_bgrid[k].assign((size_t)L, 1);
+    Q.st_bslot0[k].assign((size_t)L, 0);
+    for (int l = 0; l < L; ++l) {
+        const int nb = Q.lb[(size_t)l + 1] - Q.lb[(size_t)l];
+        const size_t fs = 2 * (size_t)stage_layout(Q.st_rows[(size_t)l], Q.st_slotsS[(size_t)l],
+                                                   Q.st_slices[(size_t)l], (int)sizeof(T), false, false).bytes;
+        const size_t bs = 2 * (size_t)stage_layout(Q.st_rows[(size_t)l], Q.st_slotsT[(size_t)l],
+                                                   Q.st_slices[(size_t)l], (int)sizeof(T), true, exact).bytes;
+        // the kernel's static shared memory (reduction scratch) comes on top
+        const size_t lim = (size_t)std::max(0, c->smem_optin - 2048);
+        if (fs > lim || bs > lim) return false;
+        int pf = 0, pb = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf, kf, kThreads, fs));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pb, kb, kThreads, bs));
+        if (pf < 1 || pb < 1) return false;
+        Q.st_fgrid[k][(size_t)l] = std::max(1, std::min(nb, pf * c->nsm));
+        Q.st_bgrid[k][(size_t)l] = std::max(1, std::min(nb, pb * c->nsm));
+    }
+    int s = 0;
+    for (int l = L - 1; l >= 0; --l) {
+        Q.st_bslot0[k][(size_t)l] = s;
+        s += Q.st_bgrid[k][(size_t)l];
+    }
+    Q.st_bnslots[k] = s;
+    ensure_partials(c, (size_t)std::max(s, 1));
+    return true;
+}
+
+// Batches of the staged sweeps: up to 16 groups of one level, about 512 rows.
+static void plan_staged(iccg_ctx* c)
+{
+    QSys& Q = c->Q;
+    Q.staged = false;
+    const int gpc = std::max(1, std::min(16, 512 / (32 * std::max(1, Q.maxu))));
+    std::vector<BatchDesc> bds;
+    Q.lb.assign((size_t)Q.nlevels + 1, 0);
+    Q.st_rows.assign((size_t)Q.nlevels, 0);
+    Q.st_slotsS.assign((size_t)Q.nlevels, 0);
+    Q.st_slotsT.assign((size_t)Q.nlevels, 0);
+    Q.st_slices.assign((size_t)Q.nlevels, 0);
+    for (int l = 0; l < Q.nlevels; ++l) {
+        const int g1 = Q.level_g[(size_t)l + 1];
+        for (int g = Q.level_g[(size_t)l]; g < g1; g += gpc) {
+            BatchDesc d{};
+            d.gb = g;
+            d.ng = std::min(gpc, g1 - g);
+            d.sb = Q.h_sl0[(size_t)g];
+            d.se = Q.h_sl0[(size_t)(g + d.ng)];
+            if (d.se <= d.sb) return;
+            d.qb = Q.steps[(size_t)d.sb].first;
+            d.qe = Q.steps[(size_t)d.se - 1].first + Q.steps[(size_t)d.se - 1].second;
+            for (int s = d.sb + 1; s < d.se; ++s)
+                if (Q.steps[(size_t)s].first != Q.steps[(size_t)s - 1].first + Q.steps[(size_t)s - 1].second) return;
+            // regular batch: every group full (32 units of one length) and
+            // every row's in-unit entry, if any, the step just before
+            bool full = true;
+            for (int gi = 0; gi < d.ng && full; ++gi) {
+                const int g0 = d.gb + gi;
+                for (int u = 0; u < 32; ++u)
+                    full = full && Q.h_glen[(size_t)g0 * 32 + (size_t)u] == Q.h_glen[(size_t)g0 * 32];
+            }
+            bool pS = full, pT = full;
+            for (int q = d.qb; q < d.qe && (pS || pT); ++q) {
+                pS = pS && Q.S.prev_only[(size_t)q];
+                pT = pT && Q.T.prev_only[(size_t)q];
+            }
+            d.flags = (pS ? 1 : 0) | (pT ? 2 : 0);
+            d.ps0 = Q.S.h_ptr[(size_t)d.sb];
+            d.ps1 = Q.S.h_ptr[(size_t)d.se];
+            d.pt0 = Q.T.h_ptr[(size_t)d.sb];
+            d.pt1 = Q.T.h_ptr[(size_t)d.se];
+            Q.st_rows[(size_t)l] = std::max(Q.st_rows[(size_t)l], d.qe - d.qb);
+            Q.st_slotsS[(size_t)l] = std::max(Q.st_slotsS[(size_t)l], d.ps1 - d.ps0);
+            Q.st_slotsT[(size_t)l] = std::max(Q.st_slotsT[(size_t)l], d.pt1 - d.pt0);
+            Q.st_slices[(size_t)l] = std::max(Q.st_slices[(size_t)l], d.se - d.sb);
+            bds.push_back(d);
+        }
+        Q.lb[(size_t)l + 1] = (int)bds.size();
+    }
+    if (!plan_staged_type<double>(c, 0) || !plan_staged_type<float>(c, 1)) return;
+    Q.bdesc.upload(bds.data(), bds.size(), &c->dev_bytes, c->stream);
+    CK(cudaStreamSynchronize(c->stream));
+    Q.staged = true;
+}
+
 static void build_q_factor(iccg_ctx* c)
 {
     QSys& Q = c->Q;
@@ -208,6 +326,8 @@ static void build_q_factor(iccg_ctx* c)
                   sell_build(c, Q.steps, F.Tp, F.Ti, &F.t_src, Q.T, enc ? 2 : 0);
         return ok;
     };
+    Q.staged = false;
+    Q.r32_ok = false;
     Q.two_phase = Q.maxu <= 64 && build(true);
     if (Q.two_phase) {
         // NI in-unit entries staged per row; gpc groups per CTA so that the
@@ -262,6 +382,7 @@ static void build_q_factor(iccg_ctx* c)
         }
         Q.b2nslots = s;
         ensure_partials(c, (size_t)std::max(s, 1));
+        plan_staged(c);
     }
     std::vector<int> dsrc((size_t)c->n);
     for (int q = 0; q < c->n; ++q) dsrc[(size_t)q] = F.dpos[(size_t)Q.q2r[(size_t)q]];
@@ -309,6 +430,13 @@ static void ensure_q32(iccg_ctx* c)
                    Q.d32.get());
             CK(cudaStreamSynchronize(c->stream));
             Q.d32_ok = true;
+        }
+        if (Q.staged && !Q.r32_ok) {
+            Q.r32.alloc((size_t)c->n, &c->dev_bytes);
+            launch(c, 3, k_recip_f32, grid_for(c, c->n), kThreads, (long long)c->n, (const double*)Q.d64.get(),
+                   Q.r32.get());
+            CK(cudaStreamSynchronize(c->stream));
+            Q.r32_ok = true;
         }
     }
 }

@@ -70,6 +70,43 @@ static void apply_ic0_q2(iccg_ctx* c, const double* r, double* y, double* z, Sol
                     (const double*)y, z, r, Q.b2slot0[(size_t)l], Q.b2nslots, st, red, c->ticket.get());
 }
 
+// Staged sweeps (k_sweep_st): FP64 storage keeps the reference's order and
+// divisions; FP32 storage multiplies by reciprocal pivots.
+template <class T, int FIN>
+static void apply_ic0_st(iccg_ctx* c, const double* r, double* y, double* z, SolverState* st)
+{
+    QSys& Q = c->Q;
+    constexpr bool f32 = std::is_same<T, float>::value;
+    constexpr bool exact = !f32;
+    constexpr int k = f32 ? 1 : 0;
+    RedBuf red{c->partials.get(), c->scalars.get()};
+    const T* dg = f32 ? (const T*)(const void*)Q.r32.get() : (const T*)(const void*)Q.d64.get();
+    const SellMat S = Q.S.view(f32), U = Q.T.view(f32);
+    const BatchDesc* bd = Q.bdesc.get();
+    const int* sl0 = Q.sl0.get();
+    const int* glen = Q.glen.get();
+    const SliceMeta* meta = Q.meta.get();
+    allow_smem(c, k_sweep_st<T, true, FIN_NONE, exact>);
+    allow_smem(c, k_sweep_st<T, false, FIN, exact>);
+    for (int l = 0; l < Q.nlevels; ++l) {
+        const size_t l_ = (size_t)l;
+        const size_t smem =
+            2 * (size_t)stage_layout(Q.st_rows[l_], Q.st_slotsS[l_], Q.st_slices[l_], (int)sizeof(T), false, false).bytes;
+        launch_smem(c, 1, k_sweep_st<T, true, FIN_NONE, exact>, Q.st_fgrid[k][l_], kThreads, smem, Q.lb[l_],
+                    Q.lb[l_ + 1], bd, Q.st_rows[l_], Q.st_slotsS[l_], Q.st_slices[l_], sl0, glen, meta, S, dg, r, y,
+                    (const double*)nullptr, 0, 0, st, red, c->ticket.get());
+    }
+    for (int l = Q.nlevels - 1; l >= 0; --l) {
+        const size_t l_ = (size_t)l;
+        const size_t smem = 2 * (size_t)stage_layout(Q.st_rows[l_], Q.st_slotsT[l_], Q.st_slices[l_], (int)sizeof(T),
+                                                     FIN != FIN_NONE, exact)
+                                    .bytes;
+        launch_smem(c, 2, k_sweep_st<T, false, FIN, exact>, Q.st_bgrid[k][l_], kThreads, smem, Q.lb[l_],
+                    Q.lb[l_ + 1], bd, Q.st_rows[l_], Q.st_slotsT[l_], Q.st_slices[l_], sl0, glen, meta, U, dg,
+                    (const double*)y, z, r, Q.st_bslot0[k][l_], Q.st_bnslots[k], st, red, c->ticket.get());
+    }
+}
+
 template <class T, int FIN>
 static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, SolverState* st)
 {
@@ -78,6 +115,10 @@ static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, Solv
     RedBuf red{c->partials.get(), c->scalars.get()};
     const T* d = f32 ? (const T*)(const void*)Q.d32.get() : (const T*)(const void*)Q.d64.get();
     const SellMat S = Q.S.view(f32), U = Q.T.view(f32);
+    if (Q.staged && c->sweep_kernel == 0 && (!f32 || Q.r32_ok)) {
+        apply_ic0_st<T, FIN>(c, r, y, z, st);
+        return;
+    }
     if (Q.two_phase) {
         if (Q.ni == 1 && Q.ks == 8) apply_ic0_q2<T, FIN, 1, 8>(c, r, y, z, st, S, U, d);
         else if (Q.ni == 1) apply_ic0_q2<T, FIN, 1, 16>(c, r, y, z, st, S, U, d);

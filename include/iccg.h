@@ -186,11 +186,16 @@ void* iccg_ctx_stream(iccg_ctx* ctx);
 long long iccg_ctx_launch_count(const iccg_ctx* ctx);
 /* bytes of device memory held by this context */
 long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
-/* context options: ICCG_OPT_TILED (default 1) selects the shared-memory
-   tiled SpMV and substitution kernels where the matrix and schedule allow
-   them; 0 forces the one-thread-per-row / per-block kernels.  Both give the
-   same bits. */
+/* context options.
+   ICCG_OPT_TILED (default 1): 1 runs the lane-interleaved kernels (an
+   internal row order with 32 independent units per warp, SELL-32 storage);
+   0 forces the CSR kernels (one thread per row / per unit).
+   ICCG_OPT_SWEEP (default 0), lane-interleaved substitutions: 0 uses the
+   staged kernel (double-buffered shared-memory batches) where a batch fits
+   shared memory, 1 forces the per-slice two-phase kernel.
+   Every choice gives the same bits with FP64 storage. */
 #define ICCG_OPT_TILED 0
+#define ICCG_OPT_SWEEP 1
 int iccg_ctx_set_option(iccg_ctx* ctx, int option, long long value);
 
 /* Uploads A_run (the matrix conjugate_gradient runs on, cg_crs.cpp:442-447):

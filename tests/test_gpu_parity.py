@@ -307,11 +307,12 @@ def test_gpu_full_size_abmc_128():
 
 @pytest.mark.parametrize("which", ["mc2d", "abmc_lin", "abmc_bfs", "d27_abmc8", "d27_mc", "knn_abmc"])
 def test_gpu_tiled_kernels_equal_simple_kernels(which):
-    """The lane-interleaved kernels (Q order, SELL-32, two-phase sweeps) give
+    """The lane-interleaved kernels (Q order, SELL-32, staged sweeps) give
     the same bits as the one-thread-per-row (per-block) kernels in FP64 --
-    apply, SpMV and whole fused solves.  In FP32 storage the backward sweep
-    applies earlier-level entries before in-block ones (there is no reference
-    rounding to keep there): results agree to rounding level."""
+    apply, SpMV and whole fused solves.  In FP32 storage the lane-interleaved
+    backward sweep applies earlier-level entries before in-block ones and
+    multiplies by FP32 reciprocal pivots (there is no reference rounding to
+    keep there): applies agree to FP32 rounding, solves to the tolerance."""
     P = {"mc2d": lambda: pb.config_small_mc(100, seed=1),
          "abmc_lin": lambda: pb.config_abmc_aniso(40, 16, "linear"),
          "abmc_bfs": lambda: pb.config_abmc_aniso(40, 16, "bfs"),
@@ -335,11 +336,49 @@ def test_gpu_tiled_kernels_equal_simple_kernels(which):
         assert np.array_equal(a[k], b[k])
     assert a[3].iters == b[3].iters
     a, b = out[True][ib.STORE_FP32], out[False][ib.STORE_FP32]
-    assert rel_err(a[0], b[0]) < 1e-12
+    assert rel_err(a[0], b[0]) < 1e-5
     assert np.array_equal(a[1], b[1])
     assert a[3].converged and b[3].converged and abs(a[3].iters - b[3].iters) <= 1
     assert a[3].true_rel_resid <= 1e-8 and b[3].true_rel_resid <= 1e-8
     assert rel_err(a[2], b[2]) < 1e-6
+    ctx.close()
+
+
+@pytest.mark.parametrize("which", ["mc2d", "abmc_lin", "abmc_bfs", "d27_abmc8", "d27_abmc32", "d27_mc", "knn_abmc"])
+def test_gpu_staged_sweeps_equal_per_slice_sweeps(which):
+    """The staged substitution kernel (double-buffered shared-memory batches)
+    against the per-slice two-phase kernel (ICCG_OPT_SWEEP = 1): the same
+    bits in FP64 (apply and fused solve, r.z included through the solve);
+    in FP32 storage the staged kernel multiplies by reciprocal pivots, so
+    applies agree to FP32 rounding and solves to the tolerance."""
+    P = {"mc2d": lambda: pb.config_small_mc(100, seed=1),
+         "abmc_lin": lambda: pb.config_abmc_aniso(40, 16, "linear"),
+         "abmc_bfs": lambda: pb.config_abmc_aniso(40, 16, "bfs"),
+         "d27_abmc8": lambda: pb.config_diffusion27(24, "abmc", 8),
+         "d27_abmc32": lambda: pb.config_diffusion27(24, "abmc", 32),
+         "d27_mc": lambda: pb.config_diffusion27(24, "piccg"),
+         "knn_abmc": lambda: pb.config_knn(8000, seed=5, block_size=16)}[which]()
+    ctx = _ctx_for(P.A_run, P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    r = ib.gen_uniform(P.A_run.n, 23)
+    out = {}
+    for opt in (0, 1):
+        ctx.set_option(ib.OPT_SWEEP, opt)
+        res = {}
+        for st in (ib.STORE_FP64, ib.STORE_FP32):
+            x = np.zeros(P.A_run.n)
+            rr = ctx.solve(P.b_run, x, 10000, 1e-8, storage=st)
+            res[st] = (ctx.apply(r, st), x, rr)
+        out[opt] = res
+    a, b = out[0][ib.STORE_FP64], out[1][ib.STORE_FP64]
+    assert np.array_equal(a[0], b[0])
+    assert np.array_equal(a[1], b[1])
+    assert a[2].iters == b[2].iters
+    a, b = out[0][ib.STORE_FP32], out[1][ib.STORE_FP32]
+    assert rel_err(a[0], b[0]) < 1e-5
+    assert a[2].converged and b[2].converged and abs(a[2].iters - b[2].iters) <= 2
+    assert a[2].true_rel_resid <= 1e-8 and b[2].true_rel_resid <= 1e-8
+    assert rel_err(a[1], b[1]) < 1e-6
     ctx.close()
 
 
