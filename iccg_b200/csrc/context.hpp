@@ -224,9 +224,15 @@ struct iccg_ctx {
     int* h_status = nullptr;               // pinned, 2 slots
     size_t partial_slots = 0;
     // graph of the fused iteration
-    cudaGraphExec_t gexec = nullptr;
+    // graphs of the fused iterations: one per pattern of residual-replacement
+    // positions within a batch, all for the same system / vectors (gkey)
+    struct GraphEntry {
+        unsigned mask;
+        cudaGraphExec_t exec;
+        int kernels;
+    };
+    std::vector<GraphEntry> graphs;
     long long gkey = -1;
-    int gkernels = 0;
     // events
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evs[2] = {nullptr, nullptr};
     // profiling

@@ -47,12 +47,6 @@ static int guard(iccg_ctx* c, F&& f)
     }
 }
 
-static void drop_graph(iccg_ctx* c)
-{
-    if (c->gexec) cudaGraphExecDestroy(c->gexec);
-    c->gexec = nullptr;
-    c->gkey = -1;
-}
 
 }  // namespace iccg
 

@@ -30,6 +30,8 @@ constexpr int kConverged = 0;
 constexpr int kBreakdown = 1;
 constexpr int kMaxIter = 2;
 constexpr int kNonFinite = 3;
+constexpr int kTrueCheck = 4;  // stopped: the recurrence residual passed the tolerance and the
+                               // host is to confirm it with an FP64 residual (mixed precision)
 
 // Device-resident CG state (one per context).
 struct SolverState {
@@ -114,7 +116,9 @@ __device__ void finish(const double* v, SolverState* st, double* out)
         if (!isfinite(rel)) { st->status = kNonFinite; return; }
         if (st->rr_interval <= 0) {
             if (rel < st->tol) st->status = kConverged;
-        } else if (rel < st->tol || (st->k + 1) % st->rr_interval == 0) {
+        } else if (rel < st->tol) {
+            st->status = kTrueCheck;
+        } else if ((st->k + 1) % st->rr_interval == 0) {
             st->rr_flag = 1;
         }
         return;
@@ -277,6 +281,15 @@ __global__ void __launch_bounds__(256) k_xpay(int n, double beta_arg, const doub
         const int k1 = st->k + 1;
         st->k = k1;
         if (k1 >= st->max_iter) st->status = kMaxIter;
+    }
+}
+
+// resumes a solve stopped at kTrueCheck with the replacement requested
+__global__ void k_resume_true_check(SolverState* st)
+{
+    if (st->status == kTrueCheck) {
+        st->status = kRunning;
+        st->rr_flag = 1;
     }
 }
 

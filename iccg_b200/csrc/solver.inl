@@ -293,6 +293,15 @@ static void fused_iteration(iccg_ctx* c, int storage, bool rr, const double* b, 
     launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st);
 }
 
+// releases every captured iteration graph of the context
+static void drop_graph(iccg_ctx* c)
+{
+    for (auto& g : c->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    c->graphs.clear();
+    c->gkey = -1;
+}
+
 static void solve_fused(iccg_ctx* c, const double* b, double* x, int max_iter, double tol, const iccg_solve_opts& o,
                         iccg_result* res)
 {
@@ -318,55 +327,99 @@ static void solve_fused(iccg_ctx* c, const double* b, double* x, int max_iter, d
 
     const int m = std::max(1, o.graph_iters);
     const bool use_graph = !c->profile;
-    auto one_batch = [&]() {
-        for (int it = 0; it < m; ++it) fused_iteration(c, storage, rr, b, x);
+    // residual replacement every rr_interval iterations happens at iterations
+    // the host can name: a batch of m iterations starting at iteration k0
+    // carries the replacement kernel only where (k + 1) % rr_interval == 0
+    const int rri = rr ? o.rr_interval : 0;
+    auto rr_mask = [&](long long k0) {
+        unsigned mk = 0;
+        if (rri > 0)
+            for (int it = 0; it < m && it < 32; ++it)
+                if ((k0 + it + 1) % rri == 0) mk |= 1u << it;
+        return mk;
     };
-    if (use_graph) {
-        const long long key = ((long long)c->sched_version << 24) ^ ((long long)c->factor_version << 36) ^
-                              ((long long)storage << 20) ^ ((long long)rr << 19) ^ ((long long)c->use_q << 18) ^
-                              ((long long)m << 4) ^ (long long)c->pc_kind ^ ((long long)(uintptr_t)x << 32) ^
-                              ((long long)(uintptr_t)b << 40);
-        if (!c->gexec || c->gkey != key) {
-            if (c->gexec) {
-                cudaGraphExecDestroy(c->gexec);
-                c->gexec = nullptr;
-            }
-            cudaGraph_t graph = nullptr;
-            const long long before = c->launches;
-            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-            try {
-                one_batch();
-            } catch (...) {
-                cudaStreamEndCapture(c->stream, &graph);
-                if (graph) cudaGraphDestroy(graph);
-                throw;
-            }
-            CK(cudaStreamEndCapture(c->stream, &graph));
-            CK(cudaGraphInstantiate(&c->gexec, graph, 0));
-            cudaGraphDestroy(graph);
-            c->gkernels = (int)(c->launches - before);
-            c->launches = before;
-            c->gkey = key;
-        }
+    auto one_batch = [&](unsigned mk) {
+        for (int it = 0; it < m; ++it) fused_iteration(c, storage, it < 32 && ((mk >> it) & 1u), b, x);
+    };
+    const long long key = ((long long)c->sched_version << 24) ^ ((long long)c->factor_version << 36) ^
+                          ((long long)storage << 20) ^ ((long long)rri << 8) ^ ((long long)c->use_q << 18) ^
+                          ((long long)m << 4) ^ (long long)c->pc_kind ^ ((long long)(uintptr_t)x << 32) ^
+                          ((long long)(uintptr_t)b << 40) ^ ((long long)c->sweep_kernel << 50);
+    if (use_graph && c->gkey != key) {
+        drop_graph(c);
+        c->gkey = key;
     }
-    // launch batches; poll the status of batch i-1 while batch i runs
-    for (int batch = 0;; ++batch) {
+    auto graph_for = [&](unsigned mk) -> iccg_ctx::GraphEntry& {
+        for (auto& g : c->graphs)
+            if (g.mask == mk) return g;
+        cudaGraph_t graph = nullptr;
+        const long long before = c->launches;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            one_batch(mk);
+        } catch (...) {
+            cudaStreamEndCapture(c->stream, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            throw;
+        }
+        CK(cudaStreamEndCapture(c->stream, &graph));
+        iccg_ctx::GraphEntry e{mk, nullptr, 0};
+        const cudaError_t ie = cudaGraphInstantiate(&e.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        CK(ie);
+        e.kernels = (int)(c->launches - before);
+        c->launches = before;
+        c->graphs.push_back(e);
+        return c->graphs.back();
+    };
+    auto run_batch = [&](long long k0) {
+        const unsigned mk = rr_mask(k0);
         if (use_graph) {
-            CK(cudaGraphLaunch(c->gexec, c->stream));
-            c->launches += c->gkernels;
+            auto& g = graph_for(mk);
+            CK(cudaGraphLaunch(g.exec, c->stream));
+            c->launches += g.kernels;
         } else {
-            one_batch();
+            one_batch(mk);
         }
-        CK(cudaMemcpyAsync(&c->h_status[batch & 1], &st->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaEventRecord(c->evs[batch & 1], c->stream));
-        if (batch > 0) {
-            CK(cudaEventSynchronize(c->evs[(batch - 1) & 1]));
-            if (c->h_status[(batch - 1) & 1] != kRunning) break;
+    };
+    // Batches are launched ahead: the status of batch i - 1 is read while
+    // batch i runs.  A batch that finds the solve stopped does nothing.
+    long long k_base = 0;  // iterations completed before the current run of batches
+    for (;;) {
+        int stopped = kRunning;
+        int batch = 0;
+        for (;; ++batch) {
+            run_batch(k_base + (long long)batch * m);
+            CK(cudaMemcpyAsync(&c->h_status[batch & 1], &st->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+            CK(cudaEventRecord(c->evs[batch & 1], c->stream));
+            if (batch > 0) {
+                CK(cudaEventSynchronize(c->evs[(batch - 1) & 1]));
+                stopped = c->h_status[(batch - 1) & 1];
+                if (stopped != kRunning) break;
+            }
+            if (k_base + (long long)(batch + 1) * m > (long long)max_iter + m) {
+                CK(cudaEventSynchronize(c->evs[batch & 1]));
+                stopped = c->h_status[batch & 1];
+                break;
+            }
         }
-        if ((long long)(batch + 1) * m > (long long)max_iter + m) {
-            CK(cudaEventSynchronize(c->evs[batch & 1]));
-            break;
+        if (stopped != kTrueCheck) {
+            CK(cudaStreamSynchronize(c->stream));
+            if (c->h_status[batch & 1] != kTrueCheck) break;
         }
+        // The recurrence residual passed the tolerance: replace it by the
+        // FP64 residual b - A x (cg_crs.cpp:518-528 semantics), test that,
+        // and, if it is not below the tolerance, finish this iteration
+        // (z = M^-1 r, beta, p) and go on.
+        CK(cudaStreamSynchronize(c->stream));
+        launch(c, 3, k_resume_true_check, 1, 1, st);
+        residual_path<FIN_TRUE>(c, (const double*)x, b, c->vr.get(), st);
+        apply_path<FIN_RZ>(c, storage, c->vr.get(), c->vz.get(), st);
+        launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st);
+        CK(cudaMemcpyAsync(c->h_state, st, sizeof(SolverState), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (c->h_state->status != kRunning) break;
+        k_base = c->h_state->k;
     }
     CK(cudaEventRecord(c->ev1, c->stream));
     CK(cudaMemcpyAsync(c->h_state, st, sizeof(SolverState), cudaMemcpyDeviceToHost, c->stream));
