@@ -259,11 +259,51 @@ __global__ void __launch_bounds__(256) k_update(int n, double alpha_arg, const d
     if (st_done(st)) return;
     const double alpha = st ? st->alpha : alpha_arg;
     acc2 a[1] = {{0.0, 0.0}};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        x[i] = fma(alpha, p[i], x[i]);
-        const double ri = fma(-alpha, Ap[i], r[i]);
-        r[i] = ri;
-        if (FIN != FIN_NONE) acc2_fma(a[0], ri, ri);
+    // pairs of elements as 16-byte accesses, two pairs in flight per thread
+    // (all four vectors 16-byte aligned; otherwise one element at a time)
+    const bool vec = (((uintptr_t)p | (uintptr_t)Ap | (uintptr_t)x | (uintptr_t)r) & 15) == 0;
+    if (!vec) {
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+            x[k] = fma(alpha, p[k], x[k]);
+            const double rk = fma(-alpha, Ap[k], r[k]);
+            r[k] = rk;
+            if (FIN != FIN_NONE) acc2_fma(a[0], rk, rk);
+        }
+        if (FIN != FIN_NONE) reduce_finish<1, FIN>(a, red, st, ticket, blockIdx.x, gridDim.x);
+        return;
+    }
+    const int n2 = n >> 1;
+    const int stride = gridDim.x * blockDim.x;
+    const double2* __restrict__ p2 = reinterpret_cast<const double2*>(p);
+    const double2* __restrict__ q2 = reinterpret_cast<const double2*>(Ap);
+    double2* __restrict__ x2 = reinterpret_cast<double2*>(x);
+    double2* __restrict__ r2 = reinterpret_cast<double2*>(r);
+    auto pair = [&](int i) {
+        const double2 pv = p2[i], qv = q2[i];
+        double2 xv = x2[i], rv = r2[i];
+        xv.x = fma(alpha, pv.x, xv.x);
+        xv.y = fma(alpha, pv.y, xv.y);
+        rv.x = fma(-alpha, qv.x, rv.x);
+        rv.y = fma(-alpha, qv.y, rv.y);
+        x2[i] = xv;
+        r2[i] = rv;
+        if (FIN != FIN_NONE) {
+            acc2_fma(a[0], rv.x, rv.x);
+            acc2_fma(a[0], rv.y, rv.y);
+        }
+    };
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + stride < n2; i += 2 * stride) {
+        pair(i);
+        pair(i + stride);
+    }
+    if (i < n2) pair(i);
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        const int k = n - 1;
+        x[k] = fma(alpha, p[k], x[k]);
+        const double rk = fma(-alpha, Ap[k], r[k]);
+        r[k] = rk;
+        if (FIN != FIN_NONE) acc2_fma(a[0], rk, rk);
     }
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(a, red, st, ticket, blockIdx.x, gridDim.x);
 }
@@ -275,8 +315,29 @@ __global__ void __launch_bounds__(256) k_xpay(int n, double beta_arg, const doub
 {
     if (st_done(st)) return;
     const double beta = st ? st->beta : beta_arg;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        p[i] = fma(beta, p[i], z[i]);
+    if ((((uintptr_t)z | (uintptr_t)p) & 15) != 0) {
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+            p[k] = fma(beta, p[k], z[k]);
+    } else {
+        const int n2 = n >> 1;
+        const int stride = gridDim.x * blockDim.x;
+        const double2* __restrict__ z2 = reinterpret_cast<const double2*>(z);
+        double2* __restrict__ p2 = reinterpret_cast<double2*>(p);
+        auto pair = [&](int i) {
+            const double2 zv = z2[i];
+            double2 pv = p2[i];
+            pv.x = fma(beta, pv.x, zv.x);
+            pv.y = fma(beta, pv.y, zv.y);
+            p2[i] = pv;
+        };
+        int i = blockIdx.x * blockDim.x + threadIdx.x;
+        for (; i + stride < n2; i += 2 * stride) {
+            pair(i);
+            pair(i + stride);
+        }
+        if (i < n2) pair(i);
+        if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) p[n - 1] = fma(beta, p[n - 1], z[n - 1]);
+    }
     if (st && blockIdx.x == 0 && threadIdx.x == 0) {
         const int k1 = st->k + 1;
         st->k = k1;
