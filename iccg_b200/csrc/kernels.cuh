@@ -817,7 +817,7 @@ struct BatchDesc {
     int ps0, ps1;  // SELL slots of the slices in S (forward matrix)
     int pt0, pt1;  // SELL slots of the slices in T (backward matrix)
     int gb, ng;    // groups [gb, gb + ng), ng <= 16
-    int flags;     // bit 0 / 1: forward / backward chains are regular (below)
+    int flags;     // bit 0 / 1: forward / backward chains are regular; bit 2: full slices (below)
     int pad1;
 };
 
@@ -964,6 +964,75 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
             const int p0 = FWD ? cur.ps0 : cur.pt0;
             const int ns = cur.se - cur.sb;
 
+            // G, full batches (every slice 32 rows, so tile row rr is lane
+            // rr % 32 of slice rr / 32): rows tid + 256 k, straight-line code
+            // with predicated loads, RG rows of a thread in flight at once.
+            if (cur.flags & 4) {
+                constexpr int RG = 2;
+                const int nrows = ns * 32;
+                for (int rb = 0; rb < nrows; rb += 256 * RG) {
+                    int rr[RG], e[RG], j0[RG], j1[RG], ni[RG];
+                    bool act[RG];
+                    double xg[RG][KG];
+#pragma unroll
+                    for (int k = 0; k < RG; ++k) {
+                        rr[k] = rb + (int)threadIdx.x + 256 * k;
+                        act[k] = rr[k] < nrows;
+                        const SliceMeta m = s_meta[act[k] ? rr[k] >> 5 : 0];
+                        const int lw = act[k] ? s_len[rr[k]] : 0;
+                        const int L = lw & 0xffff;
+                        ni[k] = lw >> 16;
+                        e[k] = (FWD ? m.pS : m.pT) - p0 + (rr[k] & 31);
+                        j0[k] = FWD ? 0 : ni[k];
+                        j1[k] = FWD ? L - ni[k] : L;
+                    }
+#pragma unroll
+                    for (int k = 0; k < RG; ++k)
+#pragma unroll
+                        for (int j = 0; j < KG; ++j) {
+                            const bool pj = j0[k] + j < j1[k];
+                            const int cj = s_col[pj ? e[k] + 32 * (j0[k] + j) : e[k]];
+                            xg[k][j] = pj ? __ldg(prev + cj) : 0.0;
+                        }
+#pragma unroll
+                    for (int k = 0; k < RG; ++k) {
+                        if (!act[k]) continue;
+                        const int jin = FWD ? j1[k] : 0;
+                        const int ea = ni[k] > 0 ? e[k] + 32 * jin : e[k];
+                        const int eb = ni[k] > 1 ? e[k] + 32 * (jin + 1) : e[k];
+                        const int ca = s_col[ea], cb = s_col[eb];
+                        const T va = s_val[ea], vb = s_val[eb];
+                        int w = ni[k] << 16;
+                        w |= ni[k] > 0 ? -ca - 1 : 0;
+                        w |= ni[k] > 1 ? (-cb - 1) << 8 : 0;
+                        s_iw[rr[k]] = w;
+                        s_iv[rr[k]] = ni[k] > 0 ? va : (T)0;
+                        s_iv[rows_cap + rr[k]] = ni[k] > 1 ? vb : (T)0;
+                        if (ext_first) {
+                            double a = s_in[rr[k]];
+#pragma unroll
+                            for (int j = 0; j < KG; ++j) {
+                                const bool pj = j0[k] + j < j1[k];
+                                const double v = (double)s_val[pj ? e[k] + 32 * (j0[k] + j) : e[k]];
+                                a = pj ? fma(-v, xg[k][j], a) : a;
+                            }
+                            for (int jj = j0[k] + KG; jj < j1[k]; ++jj) {
+                                const int ej = e[k] + 32 * jj;
+                                a = fma(-(double)s_val[ej], __ldg(prev + s_col[ej]), a);
+                            }
+                            s_in[rr[k]] = a;
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < KG; ++j)
+                                if (j0[k] + j < j1[k]) s_pv[e[k] + 32 * (j0[k] + j)] = xg[k][j];
+                            for (int jj = j0[k] + KG; jj < j1[k]; ++jj) {
+                                const int ej = e[k] + 32 * jj;
+                                s_pv[ej] = __ldg(prev + s_col[ej]);
+                            }
+                        }
+                    }
+                }
+            } else
             // G: earlier-level entries
             for (int t0 = warp; t0 < ns; t0 += 8 * UG) {
                 int rr[UG], e[UG], j0[UG], j1[UG];

@@ -294,7 +294,7 @@ static void plan_staged(iccg_ctx* c)
                 pS = pS && Q.S.prev_only[(size_t)q];
                 pT = pT && Q.T.prev_only[(size_t)q];
             }
-            d.flags = (pS ? 1 : 0) | (pT ? 2 : 0);
+            d.flags = (pS ? 1 : 0) | (pT ? 2 : 0) | (full ? 4 : 0);
             d.ps0 = Q.S.h_ptr[(size_t)d.sb];
             d.ps1 = Q.S.h_ptr[(size_t)d.se];
             d.pt0 = Q.T.h_ptr[(size_t)d.sb];
