@@ -44,9 +44,11 @@ static void apply_ic0_simple(iccg_ctx* c, const double* r, double* y, double* z,
 }
 
 // --- lane-interleaved substitutions -----------------------------------------
+// The routines below run the forward sweep (which & 1) and / or the
+// backward sweep (which & 2).
 template <class T, int FIN, int NI, int KS>
-static void apply_ic0_q2(iccg_ctx* c, const double* r, double* y, double* z, SolverState* st, const SellMat& S,
-                         const SellMat& U, const T* d)
+static void apply_ic0_q2(iccg_ctx* c, int which, const double* r, double* y, double* z, SolverState* st,
+                         const SellMat& S, const SellMat& U, const T* d)
 {
     QSys& Q = c->Q;
     RedBuf red{c->partials.get(), c->scalars.get()};
@@ -60,20 +62,22 @@ static void apply_ic0_q2(iccg_ctx* c, const double* r, double* y, double* z, Sol
     const int* sl0 = Q.sl0.get();
     const int* glen = Q.glen.get();
     const SliceMeta* meta = Q.meta.get();
-    for (int l = 0; l < Q.nlevels; ++l)
-        launch_smem(c, 1, k_sweep_q2<T, true, FIN_NONE, true, NI, KS>, Q.g2grid[(size_t)l], kThreads, fsmem,
-                    Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.tile, fslow, sl0, glen, meta, S, d, r,
-                    y, (const double*)nullptr, 0, 0, st, red, c->ticket.get());
-    for (int l = Q.nlevels - 1; l >= 0; --l)
-        launch_smem(c, 2, k_sweep_q2<T, false, FIN, exact, NI, KS>, Q.g2grid[(size_t)l], kThreads, bsmem,
-                    Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.tile, bslow, sl0, glen, meta, U, d,
-                    (const double*)y, z, r, Q.b2slot0[(size_t)l], Q.b2nslots, st, red, c->ticket.get());
+    if (which & 1)
+        for (int l = 0; l < Q.nlevels; ++l)
+            launch_smem(c, 1, k_sweep_q2<T, true, FIN_NONE, true, NI, KS>, Q.g2grid[(size_t)l], kThreads, fsmem,
+                        Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.tile, fslow, sl0, glen, meta, S, d, r,
+                        y, (const double*)nullptr, 0, 0, st, red, c->ticket.get());
+    if (which & 2)
+        for (int l = Q.nlevels - 1; l >= 0; --l)
+            launch_smem(c, 2, k_sweep_q2<T, false, FIN, exact, NI, KS>, Q.g2grid[(size_t)l], kThreads, bsmem,
+                        Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.tile, bslow, sl0, glen, meta, U, d,
+                        (const double*)y, z, r, Q.b2slot0[(size_t)l], Q.b2nslots, st, red, c->ticket.get());
 }
 
 // Staged sweeps (k_sweep_st): FP64 storage keeps the reference's order and
 // divisions; FP32 storage multiplies by reciprocal pivots.
 template <class T, int FIN>
-static void apply_ic0_st(iccg_ctx* c, const double* r, double* y, double* z, SolverState* st)
+static void apply_ic0_st(iccg_ctx* c, int which, const double* r, double* y, double* z, SolverState* st)
 {
     QSys& Q = c->Q;
     constexpr bool f32 = std::is_same<T, float>::value;
@@ -88,23 +92,25 @@ static void apply_ic0_st(iccg_ctx* c, const double* r, double* y, double* z, Sol
     const SliceMeta* meta = Q.meta.get();
     allow_smem(c, k_sweep_st<T, true, FIN_NONE, exact>);
     allow_smem(c, k_sweep_st<T, false, FIN, exact>);
-    for (int l = 0; l < Q.nlevels; ++l) {
-        const size_t l_ = (size_t)l;
-        const size_t smem =
-            2 * (size_t)stage_layout(Q.st_rows[l_], Q.st_slotsS[l_], Q.st_slices[l_], (int)sizeof(T), false, false).bytes;
-        launch_smem(c, 1, k_sweep_st<T, true, FIN_NONE, exact>, Q.st_fgrid[k][l_], kThreads, smem, Q.lb[l_],
-                    Q.lb[l_ + 1], bd, Q.st_rows[l_], Q.st_slotsS[l_], Q.st_slices[l_], sl0, glen, meta, S, dg, r, y,
-                    (const double*)nullptr, 0, 0, st, red, c->ticket.get());
-    }
-    for (int l = Q.nlevels - 1; l >= 0; --l) {
-        const size_t l_ = (size_t)l;
-        const size_t smem = 2 * (size_t)stage_layout(Q.st_rows[l_], Q.st_slotsT[l_], Q.st_slices[l_], (int)sizeof(T),
-                                                     FIN != FIN_NONE, exact)
-                                    .bytes;
-        launch_smem(c, 2, k_sweep_st<T, false, FIN, exact>, Q.st_bgrid[k][l_], kThreads, smem, Q.lb[l_],
-                    Q.lb[l_ + 1], bd, Q.st_rows[l_], Q.st_slotsT[l_], Q.st_slices[l_], sl0, glen, meta, U, dg,
-                    (const double*)y, z, r, Q.st_bslot0[k][l_], Q.st_bnslots[k], st, red, c->ticket.get());
-    }
+    if (which & 1)
+        for (int l = 0; l < Q.nlevels; ++l) {
+            const size_t l_ = (size_t)l;
+            const size_t smem =
+                2 * (size_t)stage_layout(Q.st_rows[l_], Q.st_slotsS[l_], Q.st_slices[l_], (int)sizeof(T), false, false).bytes;
+            launch_smem(c, 1, k_sweep_st<T, true, FIN_NONE, exact>, Q.st_fgrid[k][l_], kThreads, smem, Q.lb[l_],
+                        Q.lb[l_ + 1], bd, Q.st_rows[l_], Q.st_slotsS[l_], Q.st_slices[l_], sl0, glen, meta, S, dg, r, y,
+                        (const double*)nullptr, 0, 0, st, red, c->ticket.get());
+        }
+    if (which & 2)
+        for (int l = Q.nlevels - 1; l >= 0; --l) {
+            const size_t l_ = (size_t)l;
+            const size_t smem = 2 * (size_t)stage_layout(Q.st_rows[l_], Q.st_slotsT[l_], Q.st_slices[l_], (int)sizeof(T),
+                                                         FIN != FIN_NONE, exact)
+                                        .bytes;
+            launch_smem(c, 2, k_sweep_st<T, false, FIN, exact>, Q.st_bgrid[k][l_], kThreads, smem, Q.lb[l_],
+                        Q.lb[l_ + 1], bd, Q.st_rows[l_], Q.st_slotsT[l_], Q.st_slices[l_], sl0, glen, meta, U, dg,
+                        (const double*)y, z, r, Q.st_bslot0[k][l_], Q.st_bnslots[k], st, red, c->ticket.get());
+        }
 }
 
 template <class T, int FIN>
@@ -115,26 +121,33 @@ static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, Solv
     RedBuf red{c->partials.get(), c->scalars.get()};
     const T* d = f32 ? (const T*)(const void*)Q.d32.get() : (const T*)(const void*)Q.d64.get();
     const SellMat S = Q.S.view(f32), U = Q.T.view(f32);
-    if (Q.staged && c->sweep_kernel == 0 && (!f32 || Q.r32_ok)) {
-        apply_ic0_st<T, FIN>(c, r, y, z, st);
-        return;
-    }
+    // Staged sweeps where planned: both sweeps with FP32 storage; the forward
+    // sweep only with FP64, whose exact backward order parks every gathered
+    // value in the tile (twice the shared memory), where the per-slice
+    // kernel measured faster.  The rest by the per-slice / one-phase kernels.
+    int staged = 0;
+    if (Q.staged && c->sweep_kernel == 0 && (!f32 || Q.r32_ok)) staged = f32 ? 3 : 1;
+    if (staged) apply_ic0_st<T, FIN>(c, staged, r, y, z, st);
+    const int rest = 3 & ~staged;
+    if (!rest) return;
     if (Q.two_phase) {
-        if (Q.ni == 1 && Q.ks == 8) apply_ic0_q2<T, FIN, 1, 8>(c, r, y, z, st, S, U, d);
-        else if (Q.ni == 1) apply_ic0_q2<T, FIN, 1, 16>(c, r, y, z, st, S, U, d);
-        else if (Q.ks == 8) apply_ic0_q2<T, FIN, 2, 8>(c, r, y, z, st, S, U, d);
-        else apply_ic0_q2<T, FIN, 2, 16>(c, r, y, z, st, S, U, d);
+        if (Q.ni == 1 && Q.ks == 8) apply_ic0_q2<T, FIN, 1, 8>(c, rest, r, y, z, st, S, U, d);
+        else if (Q.ni == 1) apply_ic0_q2<T, FIN, 1, 16>(c, rest, r, y, z, st, S, U, d);
+        else if (Q.ks == 8) apply_ic0_q2<T, FIN, 2, 8>(c, rest, r, y, z, st, S, U, d);
+        else apply_ic0_q2<T, FIN, 2, 16>(c, rest, r, y, z, st, S, U, d);
         return;
     }
-    for (int l = 0; l < Q.nlevels; ++l)
-        launch(c, 1, k_sweep_q<T, true, FIN_NONE>, Q.fgrid[(size_t)l], kThreads, Q.level_g[(size_t)l],
-               Q.level_g[(size_t)l + 1], (const int*)Q.gbase.get(), (const int*)Q.glen.get(),
-               (const int*)Q.sl0.get(), S, d, r, y, (const double*)nullptr, 0, 0, st, red, c->ticket.get());
-    for (int l = Q.nlevels - 1; l >= 0; --l)
-        launch(c, 2, k_sweep_q<T, false, FIN>, Q.fgrid[(size_t)l], kThreads, Q.level_g[(size_t)l],
-               Q.level_g[(size_t)l + 1], (const int*)Q.gbase.get(), (const int*)Q.glen.get(),
-               (const int*)Q.sl0.get(), U, d, (const double*)y, z, r, Q.bslot0[(size_t)l], Q.bnslots, st, red,
-               c->ticket.get());
+    if (rest & 1)
+        for (int l = 0; l < Q.nlevels; ++l)
+            launch(c, 1, k_sweep_q<T, true, FIN_NONE>, Q.fgrid[(size_t)l], kThreads, Q.level_g[(size_t)l],
+                   Q.level_g[(size_t)l + 1], (const int*)Q.gbase.get(), (const int*)Q.glen.get(),
+                   (const int*)Q.sl0.get(), S, d, r, y, (const double*)nullptr, 0, 0, st, red, c->ticket.get());
+    if (rest & 2)
+        for (int l = Q.nlevels - 1; l >= 0; --l)
+            launch(c, 2, k_sweep_q<T, false, FIN>, Q.fgrid[(size_t)l], kThreads, Q.level_g[(size_t)l],
+                   Q.level_g[(size_t)l + 1], (const int*)Q.gbase.get(), (const int*)Q.glen.get(),
+                   (const int*)Q.sl0.get(), U, d, (const double*)y, z, r, Q.bslot0[(size_t)l], Q.bnslots, st, red,
+                   c->ticket.get());
 }
 
 // z = M^{-1} r (IC0::apply, ic0.cpp:366-393; Identity / Jacobi apply)
