@@ -243,8 +243,18 @@ def run_gpu(args):
                        "frac": round(gbs / peak, 4), "launches": cnt}
     kernels["vector"] = {"ms_total": round(prof["vector"][0], 4), "launches": prof["vector"][1]}
     kernels["residual_replacement"] = {"ms_total": round(prof["residual"][0], 4), "launches": prof["residual"][1]}
-    dom = kernels["spmv"]
-    traffic = _traffic_from_profiles()
+    # the dominant kernel: largest device time per solve; per-launch figures
+    # (a sweep is one launch per color)
+    per_solve = {"spmv": prof["spmv"][0], "fwd_sweep": prof["fwd_sweep"][0], "bwd_sweep": prof["bwd_sweep"][0]}
+    dom_name = max(per_solve, key=per_solve.get)
+    launches_per_unit = 1 if dom_name == "spmv" else max(1, P.nc)
+    dom = dict(kernels[dom_name])
+    dom["bytes"] = bm[dom_name] // launches_per_unit
+    traffic = _traffic_from_profiles(dom_name)
+    dom_label = {"spmv": "k_spmv_q: SpMV p -> Ap with p.Ap, p.p, Ap.Ap (FP32 values, FP64 vectors)",
+                 "fwd_sweep": "k_sweep_st: forward substitution L y = r, one launch per color (FP32 factor)",
+                 "bwd_sweep": "k_sweep_st: backward substitution L^T z = y with r.z, one launch per color "
+                              "(FP32 factor)"}[dom_name]
 
     # e2e: through the C ABI with host (pinned) buffers, H2D of b and x0 and D2H of x inside the timed region
     pin_b = torch.from_numpy(P.b_run).pin_memory()
@@ -299,9 +309,10 @@ def run_gpu(args):
                  "true_rel_resid": r64.true_rel_resid},
         "speedup_vs_plain_fp64": round(plain.solve_ms / ms_per, 3),
         "speedup_vs_fused_fp64": round(fused64.solve_ms / ms_per, 3),
-        "roofline": {"bound": "hbm", "kernel": "spmv (FP32 values, FP64 x)", "achieved": dom["GB/s"],
+        "roofline": {"bound": "hbm", "kernel": dom_label, "achieved": dom["GB/s"],
                      "peak": peak, "unit": "GB/s", "frac": dom["frac"], "peak_source": peak_kind,
-                     "traffic": traffic, "algorithmic_bytes": dom["bytes"]},
+                     "traffic": traffic, "algorithmic_bytes_per_launch": dom["bytes"],
+                     "share_of_solve": round(per_solve[dom_name] / max(rp.solve_ms, 1e-9), 3)},
         "kernels": kernels,
         "iteration_bytes": bm["iteration"],
         "iteration_GBps": round(bm["iteration"] * iters / (rp.solve_ms * 1e-3) / 1e9, 1) if rp.solve_ms else None,
@@ -320,10 +331,14 @@ def run_gpu(args):
         print(json.dumps(line), flush=True)
 
 
-def _traffic_from_profiles():
-    """DRAM bytes per SpMV launch from the committed ncu summary, if any."""
-    p = ROOT / "profiles" / "ncu_spmv_abmc128.txt"
-    if not p.exists():
+_PROFILE_OF = {"spmv": "ncu_spmv_abmc128.txt", "bwd_sweep": "ncu_sweep_st_abmc128.txt"}
+
+
+def _traffic_from_profiles(kernel: str):
+    """DRAM bytes per launch of `kernel` from its committed ncu summary, if any."""
+    name = _PROFILE_OF.get(kernel)
+    p = ROOT / "profiles" / name if name else None
+    if p is None or not p.exists():
         return None
     for ln in p.read_text().splitlines():
         if ln.startswith("traffic_bytes_per_launch:"):

@@ -1,8 +1,8 @@
 """Host-side routines of iccg_b200 against the oracle (no GPU needed).
 
 Orderings, P^T A P, expansion and schedules must equal the reference bit for
-bit (SURVEY bit-exact contract); readers must accept and reject the same
-inputs as the reference's.
+bit (the schedule arrays are the drop-in contract); readers must accept and
+reject the same inputs as the reference's.
 """
 import re
 from pathlib import Path
