@@ -245,8 +245,8 @@ def run_gpu(args):
     kernels["residual_replacement"] = {"ms_total": round(prof["residual"][0], 4), "launches": prof["residual"][1]}
     # the dominant kernel: largest device time per solve; per-launch figures
     # (a sweep is one launch per color)
-    per_solve = {"spmv": prof["spmv"][0], "fwd_sweep": prof["fwd_sweep"][0], "bwd_sweep": prof["bwd_sweep"][0]}
-    dom_name = max(per_solve, key=per_solve.get)
+    kernel_ms = {"spmv": prof["spmv"][0], "fwd_sweep": prof["fwd_sweep"][0], "bwd_sweep": prof["bwd_sweep"][0]}
+    dom_name = max(kernel_ms, key=kernel_ms.get)
     launches_per_unit = 1 if dom_name == "spmv" else max(1, P.nc)
     dom = dict(kernels[dom_name])
     dom["bytes"] = bm[dom_name] // launches_per_unit
@@ -312,7 +312,7 @@ def run_gpu(args):
         "roofline": {"bound": "hbm", "kernel": dom_label, "achieved": dom["GB/s"],
                      "peak": peak, "unit": "GB/s", "frac": dom["frac"], "peak_source": peak_kind,
                      "traffic": traffic, "algorithmic_bytes_per_launch": dom["bytes"],
-                     "share_of_solve": round(per_solve[dom_name] / max(rp.solve_ms, 1e-9), 3)},
+                     "share_of_solve": round(kernel_ms[dom_name] / max(rp.solve_ms, 1e-9), 3)},
         "kernels": kernels,
         "iteration_bytes": bm["iteration"],
         "iteration_GBps": round(bm["iteration"] * iters / (rp.solve_ms * 1e-3) / 1e9, 1) if rp.solve_ms else None,

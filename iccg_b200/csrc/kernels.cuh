@@ -486,29 +486,53 @@ __global__ void __launch_bounds__(256) k_spmv_q(int n, SellMat A, const double* 
     acc2 a[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
     const int lane = threadIdx.x & 31;
     const int nslices = (n + 31) >> 5;
-    for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nslices; s += (gridDim.x * blockDim.x) >> 5) {
+    const int stride = (gridDim.x * blockDim.x) >> 5;
+    // Software pipeline over the warp's slices: the row length, columns and
+    // values of the next slice (up to K entries per row) are loaded while
+    // the current slice's x gathers and sums run.  Rows longer than K take
+    // the rest of their entries in a tail loop.
+    constexpr int K = 8;
+    int L = 0, c[K];
+    T v[K];
+    auto load = [&](int s) {
         const int i = (s << 5) + lane;
-        if (i < n) {
-            const int L = A.len[i];
+        L = i < n ? A.len[i] : 0;
+        const int p0 = A.ptr[s] + lane;
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            c[j] = j < L ? __ldcs(col + p0 + 32 * j) : 0;
+            v[j] = j < L ? __ldcs(val + p0 + 32 * j) : (T)0;
+        }
+    };
+    int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (s < nslices) load(s);
+    for (; s < nslices; s += stride) {
+        const int Lc = L;
+        int cc[K];
+        T vc[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            cc[j] = c[j];
+            vc[j] = v[j];
+        }
+        const int sn = s + stride;
+        if (sn < nslices) load(sn);
+        double xv[K];
+#pragma unroll
+        for (int j = 0; j < K; ++j) xv[j] = j < Lc ? __ldg(x + cc[j]) : 0.0;
+        const int i = (s << 5) + lane;
+        double sum = 0.0;
+#pragma unroll
+        for (int j = 0; j < K; ++j)
+            if (j < Lc) sum = sum + (double)vc[j] * xv[j];
+        if (Lc > K) {
             const int p0 = A.ptr[s] + lane;
-            double sum = 0.0;
-            int j = 0;
-            for (; j + 4 <= L; j += 4) {
-                const int pa = p0 + 32 * j;
-                const int c0 = __ldcs(col + pa), c1 = __ldcs(col + pa + 32), c2 = __ldcs(col + pa + 64),
-                          c3 = __ldcs(col + pa + 96);
-                const double v0 = (double)__ldcs(val + pa), v1 = (double)__ldcs(val + pa + 32),
-                             v2 = (double)__ldcs(val + pa + 64), v3 = (double)__ldcs(val + pa + 96);
-                const double x0 = __ldg(x + c0), x1 = __ldg(x + c1), x2 = __ldg(x + c2), x3 = __ldg(x + c3);
-                sum = sum + v0 * x0;
-                sum = sum + v1 * x1;
-                sum = sum + v2 * x2;
-                sum = sum + v3 * x3;
-            }
-            for (; j < L; ++j) {
+            for (int j = K; j < Lc; ++j) {
                 const int pa = p0 + 32 * j;
                 sum = sum + (double)__ldcs(val + pa) * __ldg(x + __ldcs(col + pa));
             }
+        }
+        if (i < n) {
             y[i] = sum;
             if (FIN == FIN_PAP) {
                 const double xi = __ldg(x + i);
