@@ -51,6 +51,7 @@ STORE_FP64, STORE_FP32 = 0, 1
 MODE_PLAIN, MODE_FUSED = 0, 1
 OPT_TILED = 0
 OPT_SWEEP = 1
+OPT_PDL = 2
 STATUS_NAMES = {0: "converged", 1: "breakdown", 2: "max_iter", 3: "nonfinite"}
 
 

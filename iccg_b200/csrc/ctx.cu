@@ -126,6 +126,8 @@ int iccg_ctx_set_option(iccg_ctx* c, int option, long long value)
         } else if (option == ICCG_OPT_SWEEP) {
             if (value != 0 && value != 1) throw Error(ICCG_ERR_ARG, "ICCG_OPT_SWEEP takes 0 or 1");
             c->sweep_kernel = (int)value;
+        } else if (option == ICCG_OPT_PDL) {
+            c->pdl = value != 0;
         } else {
             throw Error(ICCG_ERR_ARG, "unknown option");
         }

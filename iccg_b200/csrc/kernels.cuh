@@ -64,6 +64,16 @@ struct RedBuf {
     double* out;    // FIN_STORE destination
 };
 
+// Programmatic dependent launch: wait until the preceding kernel in the
+// stream has finished and its writes are visible (a no-op for a launch
+// without the attribute), then let the next kernel start placing its CTAs.
+// Every kernel begins with this, before any global memory access.
+__device__ __forceinline__ void grid_dep_begin()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ bool st_done(const SolverState* st)
 {
     return st != nullptr && *(volatile const int*)&st->status != kRunning;
@@ -199,6 +209,7 @@ __global__ void __launch_bounds__(256) k_spmv(int n, const int* __restrict__ rp,
                                               double* __restrict__ y, SolverState* st, RedBuf red,
                                               unsigned int* ticket)
 {
+    grid_dep_begin();
     if (st_done(st)) return;
     acc2 a[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -225,6 +236,7 @@ __global__ void __launch_bounds__(256) k_residual(int n, const int* __restrict__
                                                   const double* __restrict__ b, double* __restrict__ r,
                                                   SolverState* st, RedBuf red, unsigned int* ticket)
 {
+    grid_dep_begin();
     if (st_done(st)) return;
     if (FIN == FIN_TRUE && *(volatile int*)&st->rr_flag == 0) return;
     acc2 a[2] = {{0.0, 0.0}, {0.0, 0.0}};
@@ -256,6 +268,7 @@ __global__ void __launch_bounds__(256) k_update(int n, double alpha_arg, const d
                                                 double* __restrict__ r, SolverState* st, RedBuf red,
                                                 unsigned int* ticket)
 {
+    grid_dep_begin();
     if (st_done(st)) return;
     const double alpha = st ? st->alpha : alpha_arg;
     acc2 a[1] = {{0.0, 0.0}};
@@ -313,6 +326,7 @@ __global__ void __launch_bounds__(256) k_update(int n, double alpha_arg, const d
 __global__ void __launch_bounds__(256) k_xpay(int n, double beta_arg, const double* __restrict__ z,
                                               double* __restrict__ p, SolverState* st)
 {
+    grid_dep_begin();
     if (st_done(st)) return;
     const double beta = st ? st->beta : beta_arg;
     if ((((uintptr_t)z | (uintptr_t)p) & 15) != 0) {
@@ -348,6 +362,7 @@ __global__ void __launch_bounds__(256) k_xpay(int n, double beta_arg, const doub
 // resumes a solve stopped at kTrueCheck with the replacement requested
 __global__ void k_resume_true_check(SolverState* st)
 {
+    grid_dep_begin();
     if (st->status == kTrueCheck) {
         st->status = kRunning;
         st->rr_flag = 1;
@@ -357,6 +372,7 @@ __global__ void k_resume_true_check(SolverState* st)
 __global__ void __launch_bounds__(256) k_copy(int n, const double* __restrict__ a, double* __restrict__ b,
                                               SolverState* st)
 {
+    grid_dep_begin();
     if (st_done(st)) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
 }
@@ -364,6 +380,7 @@ __global__ void __launch_bounds__(256) k_copy(int n, const double* __restrict__ 
 __global__ void __launch_bounds__(256) k_sub(int n, const double* __restrict__ b, const double* __restrict__ ax,
                                              double* __restrict__ r)
 {
+    grid_dep_begin();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) r[i] = b[i] - ax[i];
 }
 
@@ -371,6 +388,7 @@ __global__ void __launch_bounds__(256) k_sub(int n, const double* __restrict__ b
 __global__ void __launch_bounds__(256) k_dot(int n, const double* __restrict__ a, const double* __restrict__ b,
                                              RedBuf red, unsigned int* ticket)
 {
+    grid_dep_begin();
     acc2 s[1] = {{0.0, 0.0}};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         acc2_fma(s[0], a[i], b[i]);
@@ -384,6 +402,7 @@ __global__ void __launch_bounds__(256) k_diag_apply(int n, const double* __restr
                                                     const double* __restrict__ r, double* __restrict__ z,
                                                     SolverState* st, RedBuf red, unsigned int* ticket)
 {
+    grid_dep_begin();
     if (st_done(st)) return;
     acc2 a[1] = {{0.0, 0.0}};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -425,6 +444,7 @@ template <class T, int FIN>
 __global__ void __launch_bounds__(256) k_sweep(SweepArgs a, int u0, int u1, int slot0, int nslots,
                                                SolverState* st, RedBuf red, unsigned int* ticket)
 {
+    grid_dep_begin();
     if (st_done(st)) return;
     const T* __restrict__ Sx = (const T*)a.Sx;
     const T* __restrict__ d = (const T*)a.d;
@@ -480,6 +500,7 @@ __global__ void __launch_bounds__(256) k_spmv_q(int n, SellMat A, const double* 
                                                 double* __restrict__ y, SolverState* st, RedBuf red,
                                                 unsigned int* ticket)
 {
+    grid_dep_begin();
     if (st_done(st)) return;
     const T* __restrict__ val = (const T*)A.val;
     const int* __restrict__ col = A.col;
@@ -552,6 +573,7 @@ __global__ void __launch_bounds__(256) k_residual_q(int n, SellMat A, const doub
                                                     const double* __restrict__ b, double* __restrict__ r,
                                                     SolverState* st, RedBuf red, unsigned int* ticket)
 {
+    grid_dep_begin();
     if (st_done(st)) return;
     if (FIN == FIN_TRUE && *(volatile int*)&st->rr_flag == 0) return;
     const double* __restrict__ val = (const double*)A.val;
@@ -604,6 +626,7 @@ __global__ void __launch_bounds__(256) k_sweep_q(int g0, int g1, const int* __re
                                                  const double* __restrict__ rdot, int slot0, int nslots,
                                                  SolverState* st, RedBuf red, unsigned int* ticket)
 {
+    grid_dep_begin();
     if (st_done(st)) return;
     const T* __restrict__ val = (const T*)M.val;
     const int* __restrict__ col = M.col;
@@ -682,6 +705,7 @@ __global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int t
                                                   double* out, const double* __restrict__ rdot, int slot0,
                                                   int nslots, SolverState* st, RedBuf red, unsigned int* ticket)
 {
+    grid_dep_begin();
     if (st_done(st)) return;
     constexpr bool ext_first = FWD || !EXACT;
     constexpr bool with_r = FIN != FIN_NONE;
@@ -936,6 +960,7 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
                                                   double* out, const double* __restrict__ rdot, int slot0,
                                                   int nslots, SolverState* st, RedBuf red, unsigned int* ticket)
 {
+    grid_dep_begin();
     if (st_done(st)) return;
     constexpr bool with_r = FIN != FIN_NONE;
     constexpr bool ext_first = FWD || !EXACT;
@@ -1260,12 +1285,14 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
 __global__ void __launch_bounds__(256) k_gather_vec(int n, const int* __restrict__ perm,
                                                     const double* __restrict__ in, double* __restrict__ out)
 {
+    grid_dep_begin();
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) out[q] = in[perm[q]];
 }
 
 __global__ void __launch_bounds__(256) k_scatter_vec(int n, const int* __restrict__ perm,
                                                      const double* __restrict__ in, double* __restrict__ out)
 {
+    grid_dep_begin();
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) out[perm[q]] = in[q];
 }
 
@@ -1281,6 +1308,7 @@ __global__ void __launch_bounds__(128) k_ic0_level(int u0, int u1, const int* __
                                                    const int* __restrict__ dpos, double shift,
                                                    unsigned long long* err)
 {
+    grid_dep_begin();
     for (int u = u0 + blockIdx.x * blockDim.x + threadIdx.x; u < u1; u += gridDim.x * blockDim.x) {
         const int t0 = unit_ptr ? unit_ptr[u] : u;
         const int t1 = unit_ptr ? unit_ptr[u + 1] : u + 1;
@@ -1338,6 +1366,7 @@ template <class T>
 __global__ void __launch_bounds__(256) k_gather(long long m, const int* __restrict__ idx,
                                                 const double* __restrict__ src, T* __restrict__ out)
 {
+    grid_dep_begin();
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < m; k += (long long)gridDim.x * blockDim.x)
         out[k] = (T)src[idx[k]];
 }
@@ -1347,6 +1376,7 @@ template <class T>
 __global__ void __launch_bounds__(256) k_gather_pad(long long m, const int* __restrict__ idx,
                                                     const double* __restrict__ src, T* __restrict__ out)
 {
+    grid_dep_begin();
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < m; k += (long long)gridDim.x * blockDim.x) {
         const int i = idx[k];
         out[k] = i >= 0 ? (T)src[i] : (T)0;
@@ -1355,6 +1385,7 @@ __global__ void __launch_bounds__(256) k_gather_pad(long long m, const int* __re
 
 __global__ void __launch_bounds__(256) k_to_f32(long long m, const double* __restrict__ src, float* __restrict__ out)
 {
+    grid_dep_begin();
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < m; k += (long long)gridDim.x * blockDim.x)
         out[k] = (float)src[k];
 }
@@ -1362,6 +1393,7 @@ __global__ void __launch_bounds__(256) k_to_f32(long long m, const double* __res
 // out[k] = (float)(1 / src[k]): reciprocal pivots of the FP32-storage sweeps
 __global__ void __launch_bounds__(256) k_recip_f32(long long m, const double* __restrict__ src, float* __restrict__ out)
 {
+    grid_dep_begin();
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < m; k += (long long)gridDim.x * blockDim.x)
         out[k] = (float)(1.0 / src[k]);
 }

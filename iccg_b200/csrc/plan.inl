@@ -41,6 +41,31 @@ static void ensure_partials(iccg_ctx* c, size_t slots)
     c->partial_slots = slots;
 }
 
+// One launch on the context's stream.  With c->pdl the launch allows
+// programmatic dependent launch: its CTAs may be placed while the previous
+// kernel drains; every kernel waits for its predecessor before touching
+// global memory (grid_dep_begin), so the data dependencies are unchanged.
+template <class... KArgs, class... Args>
+static void launch_raw(iccg_ctx* c, void (*kernel)(KArgs...), int grid, int block, size_t smem, Args... args)
+{
+    if (c->pdl) {
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3((unsigned)grid);
+        cfg.blockDim = dim3((unsigned)block);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = c->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CK(cudaLaunchKernelEx(&cfg, kernel, args...));
+    } else {
+        kernel<<<grid, block, smem, c->stream>>>(args...);
+        CK(cudaGetLastError());
+    }
+}
+
 // launch wrapper: counts launches and, when profiling, brackets each launch
 // with CUDA events on the context's stream (class cls)
 template <class K, class... Args>
@@ -61,8 +86,7 @@ static void launch_smem(iccg_ctx* c, int cls, K kernel, int grid, int block, siz
         ++c->ev_used;
         CK(cudaEventRecord(e0, c->stream));
     }
-    kernel<<<grid, block, smem, c->stream>>>(args...);
-    CK(cudaGetLastError());
+    launch_raw(c, kernel, grid, block, smem, args...);
     if (c->profile) CK(cudaEventRecord(e1, c->stream));
     c->launches++;
 }
@@ -85,8 +109,7 @@ static void launch(iccg_ctx* c, int cls, K kernel, int grid, int block, Args... 
         ++c->ev_used;
         CK(cudaEventRecord(e0, c->stream));
     }
-    kernel<<<grid, block, 0, c->stream>>>(args...);
-    CK(cudaGetLastError());
+    launch_raw(c, kernel, grid, block, 0, args...);
     if (c->profile) CK(cudaEventRecord(e1, c->stream));
     c->launches++;
 }

@@ -193,9 +193,14 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
    ICCG_OPT_SWEEP (default 0), lane-interleaved substitutions: 0 uses the
    staged kernel (double-buffered shared-memory batches) where a batch fits
    shared memory, 1 forces the per-slice two-phase kernel.
+   ICCG_OPT_PDL (default 0): 1 launches kernels with programmatic dependent
+   launch, so a kernel's CTAs are placed while its predecessor drains (each
+   kernel still waits for its predecessor's results).  On the 128^3 system it
+   made the plain path faster and the graph-replayed fused path slower.
    Every choice gives the same bits with FP64 storage. */
 #define ICCG_OPT_TILED 0
 #define ICCG_OPT_SWEEP 1
+#define ICCG_OPT_PDL 2
 int iccg_ctx_set_option(iccg_ctx* ctx, int option, long long value);
 
 /* Uploads A_run (the matrix conjugate_gradient runs on, cg_crs.cpp:442-447):

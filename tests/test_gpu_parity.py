@@ -406,3 +406,29 @@ def test_gpu_dropin_reference_template(tmp_path):
     assert d["adapter_x_rel_err"] <= X_TOL
     assert d["gpu_converged"] == 1 and abs(d["gpu_iters"] - d["ref_iters"]) <= 1
     assert d["gpu_x_rel_err"] <= X_TOL
+
+
+@pytest.mark.parametrize("which", ["abmc_lin", "d27_mc"])
+def test_gpu_pdl_launches_give_the_same_bits(which):
+    """Programmatic dependent launch only lets a kernel's CTAs be placed
+    early; every kernel still waits for its predecessor.  FP64 and FP32
+    solves and applies must be identical with it on and off."""
+    P = {"abmc_lin": lambda: pb.config_abmc_aniso(40, 16, "linear"),
+         "d27_mc": lambda: pb.config_diffusion27(24, "piccg")}[which]()
+    ctx = _ctx_for(P.A_run, P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    r = ib.gen_uniform(P.A_run.n, 29)
+    out = {}
+    for pdl in (1, 0):
+        ctx.set_option(ib.OPT_PDL, pdl)
+        res = []
+        for st in (ib.STORE_FP64, ib.STORE_FP32):
+            x = np.zeros(P.A_run.n)
+            rr = ctx.solve(P.b_run, x, 10000, 1e-8, storage=st)
+            res.append((ctx.apply(r, st), x, rr.iters))
+        out[pdl] = res
+    for a, b in zip(out[1], out[0]):
+        assert np.array_equal(a[0], b[0])
+        assert np.array_equal(a[1], b[1])
+        assert a[2] == b[2]
+    ctx.close()
