@@ -252,9 +252,10 @@ def run_gpu(args):
     dom["bytes"] = bm[dom_name] // launches_per_unit
     traffic = _traffic_from_profiles(dom_name)
     dom_label = {"spmv": "k_spmv_q: SpMV p -> Ap with p.Ap, p.p, Ap.Ap (FP32 values, FP64 vectors)",
-                 "fwd_sweep": "k_sweep_st: forward substitution L y = r, one launch per color (FP32 factor)",
-                 "bwd_sweep": "k_sweep_st: backward substitution L^T z = y with r.z, one launch per color "
-                              "(FP32 factor)"}[dom_name]
+                 "fwd_sweep": "forward substitution L y = r, one launch per color (k_sweep_chain for the color "
+                              "with in-block entries only, k_sweep_st for the other; FP32 factor)",
+                 "bwd_sweep": "backward substitution L^T z = y with r.z, one launch per color (k_sweep_chain for "
+                              "the color with in-block entries only, k_sweep_st for the other; FP32 factor)"}[dom_name]
 
     # e2e: through the C ABI with host (pinned) buffers, H2D of b and x0 and D2H of x inside the timed region
     pin_b = torch.from_numpy(P.b_run).pin_memory()

@@ -67,6 +67,7 @@ struct SellDev {
     // in-unit entry and that entry is the unit's row one step before it in
     // the sweep's order
     std::vector<unsigned char> prev_only;
+    std::vector<unsigned char> unit_only;  // host, encoded matrices: 1 when every entry of the row is in-unit
     SellMat view(bool fp32) const
     {
         return SellMat{ptr.get(), col.get(), fp32 ? (const void*)v32.get() : (const void*)v64.get(), len.get()};
@@ -82,6 +83,7 @@ struct SellDev {
         src.clear();
         h_ptr.clear();
         prev_only.clear();
+        unit_only.clear();
     }
 };
 
@@ -118,8 +120,11 @@ struct QSys {
     Buf<BatchDesc> bdesc;
     std::vector<int> lb;                                  // first batch of each level (nlevels + 1)
     std::vector<int> st_rows, st_slotsS, st_slotsT, st_slices;
-    std::vector<int> st_fgrid[2], st_bgrid[2], st_bslot0[2];
-    int st_bnslots[2] = {0, 0};
+    // levels whose rows have in-unit entries only, one per row, the previous
+    // step, in full groups of at most 16 steps: the chain-only kernel
+    std::vector<int> chainS, chainT;
+    std::vector<int> st_fgrid[2], st_bgrid[2];
+    std::vector<int> ch_grid[2];                          // chain-only kernel grids per level
     Buf<float> r32;                                       // FP32 reciprocal pivots
     bool r32_ok = false;
     // matrices
@@ -161,12 +166,11 @@ struct QSys {
         staged = false;
         bdesc.free();
         lb.clear();
-        for (auto* v : {&st_rows, &st_slotsS, &st_slotsT, &st_slices}) v->clear();
+        for (auto* v : {&st_rows, &st_slotsS, &st_slotsT, &st_slices, &chainS, &chainT}) v->clear();
         for (int k = 0; k < 2; ++k) {
             st_fgrid[k].clear();
             st_bgrid[k].clear();
-            st_bslot0[k].clear();
-            st_bnslots[k] = 0;
+            ch_grid[k].clear();
         }
         r32.free();
         r32_ok = false;

@@ -1281,6 +1281,86 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(rz, red, st, ticket, slot0 + blockIdx.x, nslots);
 }
 
+// ---------------------------------------------------------------------------
+// Chain-only levels: every row's entries are in-unit, at most one, on the
+// unit's previous step in the sweep's order, and the groups are full (32
+// units of one length, at most 16 steps).  A row is then
+//     out_r = (in_r - v_r out_{r-1}) / d_r     (v_r absent on a unit's first row)
+// with the fused multiply-add and the division / product of the staged
+// kernel's regular chain, so the bits are the same.  One warp per group, one
+// lane per unit; the steps' rows stream in chunks of CH, the next chunk's
+// loads in flight while the current one is chained; no shared memory.
+// ---------------------------------------------------------------------------
+template <class T, bool FWD, int FIN, bool EXACT>
+__global__ void __launch_bounds__(256) k_sweep_chain(int g0, int g1, const int* __restrict__ glen,
+                                                     const int* __restrict__ sl0, const SliceMeta* __restrict__ meta,
+                                                     SellMat M, const T* __restrict__ dg,
+                                                     const double* __restrict__ in, double* __restrict__ out,
+                                                     const double* __restrict__ rdot, int slot0, int nslots,
+                                                     SolverState* st, RedBuf red, unsigned int* ticket)
+{
+    grid_dep_begin();
+    if (st_done(st)) return;
+    constexpr bool with_r = FIN != FIN_NONE;
+    constexpr int CH = 4;
+    const T* __restrict__ val = (const T*)M.val;
+    const int lane = threadIdx.x & 31;
+    acc2 rz[1] = {{0.0, 0.0}};
+    struct Chunk {
+        double a[CH], rd[CH];
+        T v[CH], p[CH];
+        int L[CH], q[CH];
+    };
+    const int wg = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nwg = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int g = g0 + wg; g < g1; g += nwg) {
+        const int len = glen[(size_t)g * 32];  // every unit of the group has this length
+        const int sb = sl0[g];
+        // lane r holds step r's first Q row, slot pointer and slice width
+        const SliceMeta mine = lane < len ? meta[sb + lane] : SliceMeta{0, 0, 0, 0};
+        const int my_q = mine.q0;
+        const int my_p = FWD ? mine.pS : mine.pT;
+        const int my_w = FWD ? (mine.w >> 12) & 255 : (mine.w >> 20) & 255;
+        auto load = [&](int t0, Chunk& C) {
+#pragma unroll
+            for (int u = 0; u < CH; ++u) {
+                const int t = t0 + u;
+                const bool ok = t < len;
+                const int rs = ok ? (FWD ? t : len - 1 - t) : 0;
+                const int q = __shfl_sync(0xffffffffu, my_q, rs) + lane;
+                const int p = __shfl_sync(0xffffffffu, my_p, rs) + lane;
+                const int w = __shfl_sync(0xffffffffu, my_w, rs);
+                C.q[u] = q;
+                C.a[u] = ok ? in[q] : 0.0;
+                C.p[u] = ok ? dg[q] : (T)1;
+                C.L[u] = ok ? M.len[q] & 0xffff : 0;
+                C.v[u] = (ok && w > 0) ? val[p] : (T)0;
+                C.rd[u] = (with_r && ok) ? rdot[q] : 0.0;
+            }
+        };
+        double last = 0.0;
+        Chunk A, B;
+        load(0, A);
+        for (int t0 = 0; t0 < len; t0 += CH) {
+            if (t0 + CH < len) load(t0 + CH, B);
+#pragma unroll
+            for (int u = 0; u < CH; ++u) {
+                if (t0 + u < len) {
+                    double a = A.a[u];
+                    const double x = fma(-(double)A.v[u], last, a);
+                    a = A.L[u] ? x : a;
+                    const double v = EXACT ? a / (double)A.p[u] : a * (double)A.p[u];
+                    out[A.q[u]] = v;
+                    if (with_r) acc2_fma(rz[0], A.rd[u], v);
+                    last = v;
+                }
+            }
+            A = B;
+        }
+    }
+    if (FIN != FIN_NONE) reduce_finish<1, FIN>(rz, red, st, ticket, slot0 + blockIdx.x, nslots);
+}
+
 // out[q] = in[perm[q]] (gather into Q order) / out[perm[q]] = in[q] (scatter)
 __global__ void __launch_bounds__(256) k_gather_vec(int n, const int* __restrict__ perm,
                                                     const double* __restrict__ in, double* __restrict__ out)

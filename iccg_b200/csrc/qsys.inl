@@ -51,6 +51,7 @@ static bool sell_build(iccg_ctx* c, const std::vector<std::pair<int, int>>& slic
     M.src.assign((size_t)slot, -1);
     M.max_nin = 0;
     M.prev_only.assign(encode ? (size_t)n : 0, 0);
+    M.unit_only.assign(encode ? (size_t)n : 0, 0);
     for (size_t s = 0; s < slices.size(); ++s)
         for (int l = 0; l < slices[s].second; ++l) {
             const int q = slices[s].first + l;
@@ -73,7 +74,10 @@ static bool sell_build(iccg_ctx* c, const std::vector<std::pair<int, int>>& slic
             }
             len[(size_t)q] = L | (nin << 16);
             M.max_nin = std::max(M.max_nin, nin);
-            if (encode) M.prev_only[(size_t)q] = (unsigned char)(prev && nin <= 1);
+            if (encode) {
+                M.prev_only[(size_t)q] = (unsigned char)(prev && nin <= 1);
+                M.unit_only[(size_t)q] = (unsigned char)(nin == L);
+            }
         }
     M.ptr.upload(ptr.data(), ptr.size(), &c->dev_bytes, c->stream);
     M.h_ptr = ptr;
@@ -229,7 +233,6 @@ static bool plan_staged_type(iccg_ctx* c, int k)
     const int L = Q.nlevels;
     Q.st_fgrid[k].assign((size_t)L, 1);
     Q.st_bgrid[k].assign((size_t)L, 1);
-    Q.st_bslot0[k].assign((size_t)L, 0);
     for (int l = 0; l < L; ++l) {
         const int nb = Q.lb[(size_t)l + 1] - Q.lb[(size_t)l];
         const size_t fs = 2 * (size_t)stage_layout(Q.st_rows[(size_t)l], Q.st_slotsS[(size_t)l],
@@ -246,13 +249,20 @@ static bool plan_staged_type(iccg_ctx* c, int k)
         Q.st_fgrid[k][(size_t)l] = std::max(1, std::min(nb, pf * c->nsm));
         Q.st_bgrid[k][(size_t)l] = std::max(1, std::min(nb, pb * c->nsm));
     }
-    int s = 0;
-    for (int l = L - 1; l >= 0; --l) {
-        Q.st_bslot0[k][(size_t)l] = s;
-        s += Q.st_bgrid[k][(size_t)l];
+    // chain-only levels: one warp per group
+    int pc = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pc, k_sweep_chain<T, false, FIN_RZ, exact>, kThreads, 0));
+    Q.ch_grid[k].assign((size_t)L, 1);
+    for (int l = 0; l < L; ++l) {
+        const int ng = Q.level_g[(size_t)l + 1] - Q.level_g[(size_t)l];
+        Q.ch_grid[k][(size_t)l] = std::max(1, std::min((ng + 7) / 8, std::max(1, pc) * c->nsm));
     }
-    Q.st_bnslots[k] = s;
-    ensure_partials(c, (size_t)std::max(s, 1));
+    // reduction slots of a backward sweep, whichever kernels its levels use
+    long long s = 0;
+    for (int l = 0; l < L; ++l)
+        s += std::max({Q.st_bgrid[k][(size_t)l], Q.ch_grid[k][(size_t)l],
+                       Q.two_phase ? Q.g2grid[(size_t)l] : 0, Q.fgrid.empty() ? 0 : Q.fgrid[(size_t)l]});
+    ensure_partials(c, (size_t)std::max<long long>(s, 1));
     return true;
 }
 
@@ -268,8 +278,12 @@ static void plan_staged(iccg_ctx* c)
     Q.st_slotsS.assign((size_t)Q.nlevels, 0);
     Q.st_slotsT.assign((size_t)Q.nlevels, 0);
     Q.st_slices.assign((size_t)Q.nlevels, 0);
+    Q.chainS.assign((size_t)Q.nlevels, 1);
+    Q.chainT.assign((size_t)Q.nlevels, 1);
     for (int l = 0; l < Q.nlevels; ++l) {
         const int g1 = Q.level_g[(size_t)l + 1];
+        for (int g = Q.level_g[(size_t)l]; g < g1; ++g)
+            if (Q.h_glen[(size_t)g * 32] > 16) Q.chainS[(size_t)l] = Q.chainT[(size_t)l] = 0;
         for (int g = Q.level_g[(size_t)l]; g < g1; g += gpc) {
             BatchDesc d{};
             d.gb = g;
@@ -295,6 +309,12 @@ static void plan_staged(iccg_ctx* c)
                 pT = pT && Q.T.prev_only[(size_t)q];
             }
             d.flags = (pS ? 1 : 0) | (pT ? 2 : 0) | (full ? 4 : 0);
+            if (!full || !pS) Q.chainS[(size_t)l] = 0;
+            if (!full || !pT) Q.chainT[(size_t)l] = 0;
+            for (int q = d.qb; q < d.qe && (Q.chainS[(size_t)l] || Q.chainT[(size_t)l]); ++q) {
+                if (!Q.S.unit_only[(size_t)q]) Q.chainS[(size_t)l] = 0;
+                if (!Q.T.unit_only[(size_t)q]) Q.chainT[(size_t)l] = 0;
+            }
             d.ps0 = Q.S.h_ptr[(size_t)d.sb];
             d.ps1 = Q.S.h_ptr[(size_t)d.se];
             d.pt0 = Q.T.h_ptr[(size_t)d.sb];

@@ -44,110 +44,113 @@ static void apply_ic0_simple(iccg_ctx* c, const double* r, double* y, double* z,
 }
 
 // --- lane-interleaved substitutions -----------------------------------------
-// The routines below run the forward sweep (which & 1) and / or the
-// backward sweep (which & 2).
-template <class T, int FIN, int NI, int KS>
-static void apply_ic0_q2(iccg_ctx* c, int which, const double* r, double* y, double* z, SolverState* st,
-                         const SellMat& S, const SellMat& U, const T* d)
+// Each level (color) of a sweep runs on one of four kernels:
+//  0 chain-only (k_sweep_chain): rows whose entries are all in-unit, one per
+//    row on the previous step, in full groups of at most 16 steps;
+//  1 staged (k_sweep_st): FP32 storage, and FP64 forward sweeps -- the exact
+//    FP64 backward order would park every gathered value in the tile (twice
+//    the shared memory), where the per-slice kernel measured faster;
+//  2 per-slice two-phase (k_sweep_q2); 3 one-phase (k_sweep_q), for units of
+//    more than 64 rows.
+// The backward sweep's r.z reduction spans all its launches: slots are laid
+// out level after level over the grids actually launched.
+struct SweepLevel {
+    int kind, grid;
+};
+
+template <class T>
+static SweepLevel sweep_level(iccg_ctx* c, int l, bool fwd)
+{
+    QSys& Q = c->Q;
+    constexpr bool f32 = std::is_same<T, float>::value;
+    constexpr int k = f32 ? 1 : 0;
+    const size_t l_ = (size_t)l;
+    const bool st_ok = Q.staged && c->sweep_kernel == 0 && (!f32 || Q.r32_ok);
+    if (st_ok && (fwd ? Q.chainS[l_] : Q.chainT[l_])) return {0, Q.ch_grid[k][l_]};
+    if (st_ok && (fwd || f32)) return {1, fwd ? Q.st_fgrid[k][l_] : Q.st_bgrid[k][l_]};
+    if (Q.two_phase) return {2, Q.g2grid[l_]};
+    return {3, Q.fgrid[l_]};
+}
+
+template <class T, int FIN, bool FWD, int NI, int KS>
+static void launch_q2_level(iccg_ctx* c, int l, int grid, const double* in, double* out, const double* rdot,
+                            int slot0, int nslots, SolverState* st, const SellMat& M, const T* d)
 {
     QSys& Q = c->Q;
     RedBuf red{c->partials.get(), c->scalars.get()};
-    const size_t rows = (size_t)Q.tile * 32;
     // FP64 storage keeps the reference's backward order exactly
-    constexpr bool exact = !std::is_same<T, float>::value;
-    const int fslow = Q.S.max_nin > NI ? 1 : 0;
-    const int bslow = (exact || Q.T.max_nin > NI) ? 1 : 0;
-    const size_t fsmem = rows * sweep_row_bytes(sizeof(T), NI, fslow != 0, false);
-    const size_t bsmem = rows * sweep_row_bytes(sizeof(T), NI, bslow != 0, FIN != FIN_NONE);
-    const int* sl0 = Q.sl0.get();
-    const int* glen = Q.glen.get();
-    const SliceMeta* meta = Q.meta.get();
-    if (which & 1)
-        for (int l = 0; l < Q.nlevels; ++l)
-            launch_smem(c, 1, k_sweep_q2<T, true, FIN_NONE, true, NI, KS>, Q.g2grid[(size_t)l], kThreads, fsmem,
-                        Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.tile, fslow, sl0, glen, meta, S, d, r,
-                        y, (const double*)nullptr, 0, 0, st, red, c->ticket.get());
-    if (which & 2)
-        for (int l = Q.nlevels - 1; l >= 0; --l)
-            launch_smem(c, 2, k_sweep_q2<T, false, FIN, exact, NI, KS>, Q.g2grid[(size_t)l], kThreads, bsmem,
-                        Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.tile, bslow, sl0, glen, meta, U, d,
-                        (const double*)y, z, r, Q.b2slot0[(size_t)l], Q.b2nslots, st, red, c->ticket.get());
+    constexpr bool exact = FWD || !std::is_same<T, float>::value;
+    const int slow = FWD ? (Q.S.max_nin > NI ? 1 : 0) : ((exact || Q.T.max_nin > NI) ? 1 : 0);
+    const size_t smem = (size_t)Q.tile * 32 * sweep_row_bytes(sizeof(T), NI, slow != 0, FIN != FIN_NONE);
+    launch_smem(c, FWD ? 1 : 2, k_sweep_q2<T, FWD, FIN, exact, NI, KS>, grid, kThreads, smem,
+                Q.level_g[(size_t)l], Q.level_g[(size_t)l + 1], Q.gpc, Q.tile, slow, (const int*)Q.sl0.get(),
+                (const int*)Q.glen.get(), (const SliceMeta*)Q.meta.get(), M, d, in, out, rdot, slot0, nslots, st, red,
+                c->ticket.get());
 }
 
-// Staged sweeps (k_sweep_st): FP64 storage keeps the reference's order and
-// divisions; FP32 storage multiplies by reciprocal pivots.
-template <class T, int FIN>
-static void apply_ic0_st(iccg_ctx* c, int which, const double* r, double* y, double* z, SolverState* st)
+template <class T, int FIN, bool FWD>
+static void launch_sweep_level(iccg_ctx* c, int l, const SweepLevel& sl, const double* in, double* out,
+                               const double* rdot, int slot0, int nslots, SolverState* st)
 {
     QSys& Q = c->Q;
     constexpr bool f32 = std::is_same<T, float>::value;
     constexpr bool exact = !f32;
-    constexpr int k = f32 ? 1 : 0;
+    const size_t l_ = (size_t)l;
     RedBuf red{c->partials.get(), c->scalars.get()};
+    const SellMat M = FWD ? Q.S.view(f32) : Q.T.view(f32);
+    // pivots: reciprocal for the FP32 staged / chain kernels, plain otherwise
     const T* dg = f32 ? (const T*)(const void*)Q.r32.get() : (const T*)(const void*)Q.d64.get();
-    const SellMat S = Q.S.view(f32), U = Q.T.view(f32);
-    const BatchDesc* bd = Q.bdesc.get();
-    const int* sl0 = Q.sl0.get();
-    const int* glen = Q.glen.get();
-    const SliceMeta* meta = Q.meta.get();
-    allow_smem(c, k_sweep_st<T, true, FIN_NONE, exact>);
-    allow_smem(c, k_sweep_st<T, false, FIN, exact>);
-    if (which & 1)
-        for (int l = 0; l < Q.nlevels; ++l) {
-            const size_t l_ = (size_t)l;
-            const size_t smem =
-                2 * (size_t)stage_layout(Q.st_rows[l_], Q.st_slotsS[l_], Q.st_slices[l_], (int)sizeof(T), false, false).bytes;
-            launch_smem(c, 1, k_sweep_st<T, true, FIN_NONE, exact>, Q.st_fgrid[k][l_], kThreads, smem, Q.lb[l_],
-                        Q.lb[l_ + 1], bd, Q.st_rows[l_], Q.st_slotsS[l_], Q.st_slices[l_], sl0, glen, meta, S, dg, r, y,
-                        (const double*)nullptr, 0, 0, st, red, c->ticket.get());
-        }
-    if (which & 2)
-        for (int l = Q.nlevels - 1; l >= 0; --l) {
-            const size_t l_ = (size_t)l;
-            const size_t smem = 2 * (size_t)stage_layout(Q.st_rows[l_], Q.st_slotsT[l_], Q.st_slices[l_], (int)sizeof(T),
-                                                         FIN != FIN_NONE, exact)
-                                        .bytes;
-            launch_smem(c, 2, k_sweep_st<T, false, FIN, exact>, Q.st_bgrid[k][l_], kThreads, smem, Q.lb[l_],
-                        Q.lb[l_ + 1], bd, Q.st_rows[l_], Q.st_slotsT[l_], Q.st_slices[l_], sl0, glen, meta, U, dg,
-                        (const double*)y, z, r, Q.st_bslot0[k][l_], Q.st_bnslots[k], st, red, c->ticket.get());
-        }
+    const T* d = f32 ? (const T*)(const void*)Q.d32.get() : (const T*)(const void*)Q.d64.get();
+    const int cls = FWD ? 1 : 2;
+    switch (sl.kind) {
+    case 0:
+        launch(c, cls, k_sweep_chain<T, FWD, FIN, exact>, sl.grid, kThreads, Q.level_g[l_], Q.level_g[l_ + 1],
+               (const int*)Q.glen.get(), (const int*)Q.sl0.get(), (const SliceMeta*)Q.meta.get(), M, dg, in, out,
+               rdot, slot0, nslots, st, red, c->ticket.get());
+        break;
+    case 1: {
+        const int slots = FWD ? Q.st_slotsS[l_] : Q.st_slotsT[l_];
+        const size_t smem = 2 * (size_t)stage_layout(Q.st_rows[l_], slots, Q.st_slices[l_], (int)sizeof(T),
+                                                     FIN != FIN_NONE, !FWD && exact)
+                                    .bytes;
+        allow_smem(c, k_sweep_st<T, FWD, FIN, exact>);
+        launch_smem(c, cls, k_sweep_st<T, FWD, FIN, exact>, sl.grid, kThreads, smem, Q.lb[l_], Q.lb[l_ + 1],
+                    (const BatchDesc*)Q.bdesc.get(), Q.st_rows[l_], slots, Q.st_slices[l_], (const int*)Q.sl0.get(),
+                    (const int*)Q.glen.get(), (const SliceMeta*)Q.meta.get(), M, dg, in, out, rdot, slot0, nslots,
+                    st, red, c->ticket.get());
+        break;
+    }
+    case 2:
+        if (Q.ni == 1 && Q.ks == 8) launch_q2_level<T, FIN, FWD, 1, 8>(c, l, sl.grid, in, out, rdot, slot0, nslots, st, M, d);
+        else if (Q.ni == 1) launch_q2_level<T, FIN, FWD, 1, 16>(c, l, sl.grid, in, out, rdot, slot0, nslots, st, M, d);
+        else if (Q.ks == 8) launch_q2_level<T, FIN, FWD, 2, 8>(c, l, sl.grid, in, out, rdot, slot0, nslots, st, M, d);
+        else launch_q2_level<T, FIN, FWD, 2, 16>(c, l, sl.grid, in, out, rdot, slot0, nslots, st, M, d);
+        break;
+    default:
+        launch(c, cls, k_sweep_q<T, FWD, FIN>, sl.grid, kThreads, Q.level_g[l_], Q.level_g[l_ + 1],
+               (const int*)Q.gbase.get(), (const int*)Q.glen.get(), (const int*)Q.sl0.get(), M, d, in, out, rdot,
+               slot0, nslots, st, red, c->ticket.get());
+        break;
+    }
 }
 
 template <class T, int FIN>
 static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, SolverState* st)
 {
     QSys& Q = c->Q;
-    const bool f32 = std::is_same<T, float>::value;
-    RedBuf red{c->partials.get(), c->scalars.get()};
-    const T* d = f32 ? (const T*)(const void*)Q.d32.get() : (const T*)(const void*)Q.d64.get();
-    const SellMat S = Q.S.view(f32), U = Q.T.view(f32);
-    // Staged sweeps where planned: both sweeps with FP32 storage; the forward
-    // sweep only with FP64, whose exact backward order parks every gathered
-    // value in the tile (twice the shared memory), where the per-slice
-    // kernel measured faster.  The rest by the per-slice / one-phase kernels.
-    int staged = 0;
-    if (Q.staged && c->sweep_kernel == 0 && (!f32 || Q.r32_ok)) staged = f32 ? 3 : 1;
-    if (staged) apply_ic0_st<T, FIN>(c, staged, r, y, z, st);
-    const int rest = 3 & ~staged;
-    if (!rest) return;
-    if (Q.two_phase) {
-        if (Q.ni == 1 && Q.ks == 8) apply_ic0_q2<T, FIN, 1, 8>(c, rest, r, y, z, st, S, U, d);
-        else if (Q.ni == 1) apply_ic0_q2<T, FIN, 1, 16>(c, rest, r, y, z, st, S, U, d);
-        else if (Q.ks == 8) apply_ic0_q2<T, FIN, 2, 8>(c, rest, r, y, z, st, S, U, d);
-        else apply_ic0_q2<T, FIN, 2, 16>(c, rest, r, y, z, st, S, U, d);
-        return;
+    for (int l = 0; l < Q.nlevels; ++l)
+        launch_sweep_level<T, FIN_NONE, true>(c, l, sweep_level<T>(c, l, true), r, y, nullptr, 0, 0, st);
+    std::vector<SweepLevel> bl((size_t)Q.nlevels);
+    int nslots = 0;
+    for (int l = Q.nlevels - 1; l >= 0; --l) {
+        bl[(size_t)l] = sweep_level<T>(c, l, false);
+        nslots += bl[(size_t)l].grid;
     }
-    if (rest & 1)
-        for (int l = 0; l < Q.nlevels; ++l)
-            launch(c, 1, k_sweep_q<T, true, FIN_NONE>, Q.fgrid[(size_t)l], kThreads, Q.level_g[(size_t)l],
-                   Q.level_g[(size_t)l + 1], (const int*)Q.gbase.get(), (const int*)Q.glen.get(),
-                   (const int*)Q.sl0.get(), S, d, r, y, (const double*)nullptr, 0, 0, st, red, c->ticket.get());
-    if (rest & 2)
-        for (int l = Q.nlevels - 1; l >= 0; --l)
-            launch(c, 2, k_sweep_q<T, false, FIN>, Q.fgrid[(size_t)l], kThreads, Q.level_g[(size_t)l],
-                   Q.level_g[(size_t)l + 1], (const int*)Q.gbase.get(), (const int*)Q.glen.get(),
-                   (const int*)Q.sl0.get(), U, d, (const double*)y, z, r, Q.bslot0[(size_t)l], Q.bnslots, st, red,
-                   c->ticket.get());
+    int slot0 = 0;
+    for (int l = Q.nlevels - 1; l >= 0; --l) {
+        launch_sweep_level<T, FIN, false>(c, l, bl[(size_t)l], y, z, r, slot0, nslots, st);
+        slot0 += bl[(size_t)l].grid;
+    }
 }
 
 // z = M^{-1} r (IC0::apply, ic0.cpp:366-393; Identity / Jacobi apply)
