@@ -180,32 +180,30 @@ def run_gpu(args):
     x64 = x_d.cpu().numpy().copy()
     for _ in range(args.warmup):
         solve(ib.STORE_FP32)
-    # timed region
+    # timed region: barrier, CUDA events on the context's stream, barrier,
+    # slowest rank's time (replicas: no collective on the data path)
+    from iccg_b200.replicas import timed_replicas, max_over_ranks
     clocks = ClockSampler(local)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks.start()
     launches0 = ctx.launches
     results = []
-    with torch.cuda.stream(stream):
-        e0.record(stream)
-    for _ in range(args.steps):
-        results.append(solve(ib.STORE_FP32))
-    with torch.cuda.stream(stream):
-        e1.record(stream)
-    torch.cuda.synchronize()
+
+    def timed():
+        clocks.start()
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+        for _ in range(args.steps):
+            results.append(solve(ib.STORE_FP32))
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    tr = timed_replicas(timed, args.steps, dist=dist, device=dev, sync=torch.cuda.synchronize)
     launches = ctx.launches - launches0
     clk = clocks.stop()
-    if dist:
-        dist.barrier()
-    total_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = tr.ms
     ms_per = total_ms / args.steps
     r32 = results[-1]
     x32 = x_d.cpu().numpy()
@@ -268,11 +266,7 @@ def run_gpu(args):
         t0 = time.perf_counter()
         ctx.solve(pin_b.numpy(), xb, 10000, TOL, storage=ib.STORE_FP32, rr_interval=RR)
         e2e.append((time.perf_counter() - t0) * 1e3)
-    e2e_ms = statistics.median(e2e)
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(statistics.median(e2e), dist=dist, device=dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -299,7 +293,7 @@ def run_gpu(args):
             "l2": "inputs larger than L2: ~0.5 GB streamed per iteration vs 126 MB L2",
             "parallelism": f"replicas x{world}",
         },
-        "solves_per_s": round(world * 1000.0 / ms_per, 3),
+        "solves_per_s": round(tr.units_per_s, 3),
         "iters": r32.iters,
         "true_rel_resid": r32.true_rel_resid,
         "residual_replacements": r32.n_replacements,
