@@ -419,13 +419,146 @@ def main():
                     help="set up the workload, then launch only this operation --reps times "
                          "(FP32 storage) and print its mean device time; for profilers")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--workload", choices=["abmc128", "batched", "serving"], default="abmc128",
+                    help="abmc128: the headline solve (default); batched: many uneven systems with 4 "
+                         "right-hand sides each, solved concurrently; serving: Poisson-arriving kNN "
+                         "Laplacian solves under a device-memory budget")
+    ap.add_argument("--systems", type=int, default=512, help="batched: number of systems")
+    ap.add_argument("--threads", type=int, default=16, help="batched / serving: concurrent solves")
+    ap.add_argument("--requests", type=int, default=200, help="serving: requests per arrival rate")
+    ap.add_argument("--max-points", type=int, default=100000, help="serving: largest kNN system")
     args = ap.parse_args()
-    if args.kernel_only:
+    if args.workload == "batched":
+        run_batched(args)
+    elif args.workload == "serving":
+        run_serving(args)
+    elif args.kernel_only:
         run_kernel_only(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)
+
+
+def run_batched(args):
+    """Many independent SPD systems of uneven size, 4 right-hand sides each.
+
+    The systems are drawn 50/50 from two families. One is a 2D 5-point
+    Poisson problem with side U{32..256}. The other is a 3D 7-point
+    Laplacian with side U{16..48}. Each gets multicolor IC(0), FP32 storage
+    of A and L, and FP64 recurrences. Every system stays resident, and
+    `--threads` of them solve at once, each on its own stream. The
+    comparison is the same solves one at a time on the plain FP64 path.
+    """
+    import torch
+    import iccg_b200 as ib
+    import iccg_b200.batch as bt
+    import iccg_b200.problems as pb
+    rng = np.random.default_rng(4)
+    t0 = time.perf_counter()
+    probs = []
+    for i in range(args.systems):
+        if rng.random() < 0.5:
+            probs.append(pb.make(pb.poisson2d(int(rng.integers(32, 257))), "piccg", seed=i))
+        else:
+            probs.append(pb.make(pb.laplace3d_aniso(int(rng.integers(16, 49)), 1.0), "piccg", seed=i))
+    rhs = [[pb.with_rhs(P, seed=1000 * i + k).b_run.copy() for k in range(4)] for i, P in enumerate(probs)]
+    host_setup_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    systems = [bt.ResidentSystem(P, storage=ib.STORE_FP32) for P in probs]
+    upload_s = time.perf_counter() - t0
+    # warm-up: one solve per system (graph capture, first-touch)
+    bt.solve_batch(systems, [[r[0]] for r in rhs], threads=args.threads)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    recs = bt.solve_batch(systems, rhs, threads=args.threads)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    ok = all(r.converged and r.true_rel_resid <= 1e-8 for r in recs)
+    # one at a time, plain FP64, on a sample of the systems
+    sample = list(range(0, len(systems), max(1, len(systems) // 32)))
+    plain_ms = []
+    for i in sample:
+        s = bt.ResidentSystem(probs[i], storage=ib.STORE_FP64)
+        s.solve(rhs[i][0], mode=ib.MODE_PLAIN)
+        x, res, wms = s.solve(rhs[i][0], mode=ib.MODE_PLAIN)
+        plain_ms.append(wms)
+        s.close()
+    for s in systems:
+        s.close()
+    plain_per_s = 1000.0 / statistics.mean(plain_ms)
+    line = {"workload": "batched", "systems": len(systems), "rhs_per_system": 4, "solves": len(recs),
+            "all_converged_1e-8": ok, "threads": args.threads,
+            "rows": {"min": min(P.A.n for P in probs), "max": max(P.A.n for P in probs),
+                     "mean": round(statistics.mean(P.A.n for P in probs))},
+            "solves_per_s": round(len(recs) / wall, 2), "wall_s": round(wall, 3),
+            "latency_ms": {"p50": round(bt.percentile([r.wall_ms for r in recs], 50), 3),
+                           "p99": round(bt.percentile([r.wall_ms for r in recs], 99), 3)},
+            "mean_iters": round(statistics.mean(r.iters for r in recs), 1),
+            "plain_fp64_one_at_a_time_solves_per_s": round(plain_per_s, 2),
+            "speedup_vs_plain_fp64_one_at_a_time": round(len(recs) / wall / plain_per_s, 2),
+            "setup_s": {"host": round(host_setup_s, 2), "upload_and_ic0": round(upload_s, 2)},
+            "storage": "fp32 A and L, fp64 vectors", "preconditioner": "IC(0), greedy multicolor",
+            "data": "synthetic", "timing": "host wall clock around the batch (many streams)"}
+    print(json.dumps(line), flush=True)
+
+
+def run_serving(args):
+    """Serving: kNN-Laplacian solve requests arriving as a Poisson process.
+
+    Each request is a symmetrised 8-nearest-neighbour graph Laplacian plus
+    1e-2 I, on N points with N log-uniform in [1e3, --max-points]. It gets a
+    seeded right-hand side and ABMC ICCG to 1e-8 with FP32 storage.
+    Requests are admitted under a 100 GB device-memory budget, and up to
+    `--threads` solves overlap. Each arrival rate reports p50 / p99 latency
+    (arrival to result, host set-up included) and solves/s. The comparison is
+    the same requests one at a time on the plain FP64 path.
+    """
+    import iccg_b200 as ib
+    import iccg_b200.batch as bt
+    import iccg_b200.problems as pb
+    rng = np.random.default_rng(5)
+    lo, hi = np.log(1e3), np.log(float(args.max_points))
+    sizes = [int(np.exp(rng.uniform(lo, hi))) for _ in range(args.requests)]
+
+    def make_requests(rate):
+        t, reqs = 0.0, []
+        arr = np.random.default_rng(int(rate * 1000) + 7)
+        for i, npts in enumerate(sizes):
+            t += arr.exponential(1.0 / rate)
+            reqs.append(bt.Request(i, t, (lambda npts=npts, i=i: pb.config_knn(npts, seed=i)),
+                                   bt.estimate_device_bytes(npts, 18 * npts)))
+        return reqs
+
+    # service time one at a time (FP32 mixed and plain FP64) on a sample
+    sample = sizes[:: max(1, len(sizes) // 16)]
+    alone_ms, plain_ms = [], []
+    for i, npts in enumerate(sample):
+        t0 = time.perf_counter()
+        P = pb.config_knn(npts, seed=10_000 + i)
+        s = bt.ResidentSystem(P, storage=ib.STORE_FP32)
+        s.solve(P.b_run)
+        alone_ms.append((time.perf_counter() - t0) * 1e3)
+        s.close()
+        s = bt.ResidentSystem(P, storage=ib.STORE_FP64)
+        _, _, wms = s.solve(P.b_run, mode=ib.MODE_PLAIN)
+        plain_ms.append(wms)
+        s.close()
+    sat = args.threads * 1000.0 / statistics.mean(alone_ms)
+    out = []
+    for f in (0.25, 0.5, 1.0):
+        loop = bt.ServingLoop(budget_bytes=100 * 10**9, workers=args.threads)
+        st = loop.run(make_requests(f * sat)).summary()
+        st["arrival_rate_per_s"] = round(f * sat, 2)
+        out.append(st)
+    line = {"workload": "serving", "requests_per_rate": len(sizes), "points": {"min": min(sizes), "max": max(sizes)},
+            "threads": args.threads, "budget_bytes": 100 * 10**9, "rates": out,
+            "one_at_a_time_ms": {"mixed_end_to_end_mean": round(statistics.mean(alone_ms), 3),
+                                 "plain_fp64_solve_mean": round(statistics.mean(plain_ms), 3)},
+            "plain_fp64_one_at_a_time_solves_per_s": round(1000.0 / statistics.mean(plain_ms), 2),
+            "storage": "fp32 A and L, fp64 vectors", "preconditioner": "IC(0), ABMC B=16",
+            "data": "synthetic", "latency": "arrival to result, host set-up (kNN graph, blocking, PtAP) included"}
+    print(json.dumps(line), flush=True)
 
 
 def run_kernel_only(args):

@@ -1,0 +1,197 @@
+"""Many independent solves on one GPU: batched systems and a serving loop.
+
+Every system gets its own context: one CUDA stream with the system's matrix,
+schedule, IC(0) factor and work vectors resident in device memory, and the
+captured graphs of its CG iterations. Host threads drive several contexts
+at once, one context per thread at a time. Their kernels run concurrently
+on the GPU, which is how small systems, too small to fill 148 SMs alone,
+share the device. A solve's arithmetic does not depend on what else runs,
+so each result is the same bits alone and in the mix.
+
+* ``solve_batch`` solves a fixed set of systems, each with several
+  right-hand sides. It returns the results plus per-solve timings.
+* ``ServingLoop`` takes requests as they arrive. It admits them while the
+  device memory held by admitted solves stays under a budget, solves them on
+  worker threads, and releases each system when its solve is done. It
+  reports p50 / p99 latency (arrival to completion) and solves/s.
+"""
+from __future__ import annotations
+
+import statistics
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+from dataclasses import dataclass, field
+from typing import Callable, List, Optional, Sequence
+
+import numpy as np
+
+from . import STORE_FP32, STORE_FP64, MODE_FUSED, PRECOND_IC0, Context
+from .problems import Problem
+
+
+@dataclass
+class SolveRecord:
+    system: int
+    rhs: int
+    iters: int
+    converged: bool
+    true_rel_resid: float
+    device_ms: float       # the solve's device time (CUDA events)
+    wall_ms: float         # host time of the call, copies included
+    x: Optional[np.ndarray] = None
+
+
+class ResidentSystem:
+    """One system on the device: A_run, schedule and IC(0) factor resident."""
+
+    def __init__(self, P: Problem, device: int = 0, storage: int = STORE_FP32):
+        self.P = P
+        self.storage = storage
+        self.ctx = Context(device)
+        self.ctx.upload(P.A_run)
+        self.ctx.set_schedule(P.sched)
+        self.ctx.build(P.precond_kind if P.precond_kind != 2 else PRECOND_IC0, 0.0)
+
+    @property
+    def device_bytes(self) -> int:
+        return self.ctx.device_bytes
+
+    def solve(self, b_run: np.ndarray, tol: float = 1e-8, max_iter: int = 10000, mode: int = MODE_FUSED,
+              rr_interval: int = 50):
+        x = np.zeros(self.P.A_run.n)
+        t0 = time.perf_counter()
+        res = self.ctx.solve(b_run, x, max_iter, tol, mode=mode, storage=self.storage, rr_interval=rr_interval)
+        return x, res, (time.perf_counter() - t0) * 1e3
+
+    def close(self):
+        self.ctx.close()
+
+
+def solve_batch(systems: Sequence[ResidentSystem], rhs: Sequence[Sequence[np.ndarray]], threads: int = 8,
+                tol: float = 1e-8, keep_x: bool = False) -> List[SolveRecord]:
+    """Solves rhs[i][j] on systems[i] for every i, j; system i's right-hand
+    sides run in order on one thread, the systems on `threads` threads."""
+
+    def work(i: int) -> List[SolveRecord]:
+        out = []
+        for j, b in enumerate(rhs[i]):
+            x, res, wall = systems[i].solve(b, tol)
+            out.append(SolveRecord(i, j, res.iters, res.converged, res.true_rel_resid, res.solve_ms, wall,
+                                   x if keep_x else None))
+        return out
+
+    with ThreadPoolExecutor(max_workers=max(1, threads)) as ex:
+        parts = list(ex.map(work, range(len(systems))))
+    return [r for p in parts for r in p]
+
+
+def percentile(v: Sequence[float], q: float) -> float:
+    if not v:
+        return 0.0
+    return float(np.percentile(np.asarray(v, dtype=np.float64), q))
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival_s: float                     # seconds after the loop starts
+    build: Callable[[], Problem]         # makes the system (host set-up) when admitted
+    est_bytes: int                       # device memory it will hold (admission)
+
+
+@dataclass
+class ServingStats:
+    latencies_ms: List[float] = field(default_factory=list)
+    iters: List[int] = field(default_factory=list)
+    failed: int = 0
+    elapsed_s: float = 0.0
+    peak_bytes: int = 0
+
+    def summary(self) -> dict:
+        n = len(self.latencies_ms)
+        return {"solves": n, "failed": self.failed, "elapsed_s": round(self.elapsed_s, 3),
+                "solves_per_s": round(n / self.elapsed_s, 3) if self.elapsed_s > 0 else 0.0,
+                "p50_ms": round(percentile(self.latencies_ms, 50), 3),
+                "p99_ms": round(percentile(self.latencies_ms, 99), 3),
+                "mean_iters": round(statistics.mean(self.iters), 1) if self.iters else 0.0,
+                "peak_device_bytes": self.peak_bytes}
+
+
+class ServingLoop:
+    """Continuous batching of independent solves.
+
+    Requests are admitted in arrival order once they have arrived, as long as
+    the admitted solves' device memory stays within `budget_bytes` and a
+    worker slot is free. An admitted request builds its system (host set-up,
+    upload, IC(0) on the device), solves it, and frees the device memory
+    when done. Up to `workers` solves overlap on the GPU.
+    """
+
+    def __init__(self, budget_bytes: int, workers: int = 8, device: int = 0, storage: int = STORE_FP32,
+                 tol: float = 1e-8):
+        self.budget = budget_bytes
+        self.workers = workers
+        self.device = device
+        self.storage = storage
+        self.tol = tol
+
+    def run(self, requests: Sequence[Request]) -> ServingStats:
+        stats = ServingStats()
+        lock = threading.Condition()
+        in_use = [0]
+        queue = sorted(requests, key=lambda r: r.arrival_s)
+        t_start = time.perf_counter()
+
+        def serve(req: Request):
+            try:
+                P = req.build()
+                sysm = ResidentSystem(P, self.device, self.storage)
+                try:
+                    with lock:
+                        stats.peak_bytes = max(stats.peak_bytes, in_use[0] - req.est_bytes + sysm.device_bytes)
+                    _, res, _ = sysm.solve(P.b_run, self.tol)
+                finally:
+                    sysm.close()
+                done = time.perf_counter() - t_start
+                with lock:
+                    if res.converged:
+                        stats.latencies_ms.append((done - req.arrival_s) * 1e3)
+                        stats.iters.append(res.iters)
+                    else:
+                        stats.failed += 1
+            except Exception:
+                with lock:
+                    stats.failed += 1
+            finally:
+                with lock:
+                    in_use[0] -= req.est_bytes
+                    lock.notify_all()
+
+        with ThreadPoolExecutor(max_workers=max(1, self.workers)) as ex:
+            active = []
+            for req in queue:
+                # wait for the arrival time
+                delay = req.arrival_s - (time.perf_counter() - t_start)
+                if delay > 0:
+                    time.sleep(delay)
+                with lock:
+                    # admission: memory budget and a free worker
+                    while in_use[0] + req.est_bytes > self.budget and in_use[0] > 0:
+                        lock.wait(timeout=1.0)
+                    while sum(1 for f in active if not f.done()) >= self.workers:
+                        lock.wait(timeout=0.05)
+                    in_use[0] += req.est_bytes
+                active.append(ex.submit(serve, req))
+            for f in active:
+                f.result()
+        stats.elapsed_s = time.perf_counter() - t_start
+        return stats
+
+
+def estimate_device_bytes(n: int, nnz: int) -> int:
+    """Device memory of one resident system (FP64 + FP32 copies of A in CSR and
+    SELL-32, the IC(0) factor in both layouts, about a dozen vectors): a
+    conservative linear model used for admission."""
+    nnz_l = (nnz + n) // 2
+    return int(nnz * 40 + nnz_l * 56 + n * 220 + (8 << 20))

@@ -208,7 +208,11 @@ static size_t sweep_row_bytes(size_t tsize, int ni, bool slow, bool with_r)
 template <class K>
 static void allow_smem(iccg_ctx* c, K kernel)
 {
+    // shared by every context of the process, which may run in several host
+    // threads at once
+    static std::mutex mu;
     static std::vector<std::pair<const void*, int>> done;
+    std::lock_guard<std::mutex> lock(mu);
     const void* key = reinterpret_cast<const void*>(kernel);
     for (auto& e : done)
         if (e.first == key && e.second == c->device) return;
