@@ -419,10 +419,12 @@ def main():
                     help="set up the workload, then launch only this operation --reps times "
                          "(FP32 storage) and print its mean device time; for profilers")
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--workload", choices=["abmc128", "batched", "serving"], default="abmc128",
+    ap.add_argument("--workload", choices=["abmc128", "batched", "serving", "diffusion27"], default="abmc128",
                     help="abmc128: the headline solve (default); batched: many uneven systems with 4 "
                          "right-hand sides each, solved concurrently; serving: Poisson-arriving kNN "
-                         "Laplacian solves under a device-memory budget")
+                         "Laplacian solves under a device-memory budget; diffusion27: multicolor vs "
+                         "ABMC B=8/16/32 on the 27-point variable-coefficient 96^3 problem")
+    ap.add_argument("--side", type=int, default=96, help="diffusion27: grid side")
     ap.add_argument("--systems", type=int, default=512, help="batched: number of systems")
     ap.add_argument("--threads", type=int, default=16, help="batched / serving: concurrent solves")
     ap.add_argument("--requests", type=int, default=200, help="serving: requests per arrival rate")
@@ -432,6 +434,8 @@ def main():
         run_batched(args)
     elif args.workload == "serving":
         run_serving(args)
+    elif args.workload == "diffusion27":
+        run_diffusion27(args)
     elif args.kernel_only:
         run_kernel_only(args)
     elif args.impl == "reference":
@@ -558,6 +562,91 @@ def run_serving(args):
             "plain_fp64_one_at_a_time_solves_per_s": round(1000.0 / statistics.mean(plain_ms), 2),
             "storage": "fp32 A and L, fp64 vectors", "preconditioner": "IC(0), ABMC B=16",
             "data": "synthetic", "latency": "arrival to result, host set-up (kNN graph, blocking, PtAP) included"}
+    print(json.dumps(line), flush=True)
+
+
+def run_diffusion27(args):
+    """Multicolor vs ABMC (B = 8, 16, 32) on a 27-point diffusion problem.
+
+    The operator is the 27-point variable-coefficient diffusion on a
+    --side^3 grid (96^3: n = 884,736, nnz = 23,393,656). Its face
+    coefficients are harmonic means of exp(sigma g), where g is a smoothed
+    Gaussian field; sigma is set for a 1e4 contrast. b = A x*, and
+    x* ~ U(-1,1) from splitmix64(0).
+    - IC(0) is factored in FP64 on the device. A non-positive pivot restarts
+      it with a larger shift, and the shift used is reported.
+    - Each variant is solved in FP64 and in mixed precision: FP32 A and L,
+      FP64 recurrences, residual replacement every 50 iterations.
+    - Reported per variant: colors, iterations and device ms per solve
+      (CUDA events, mean over --steps after --warmup), plus the iteration's
+      algorithmic bandwidth.
+    - The reference's OpenMP CG runs once, on the ABMC B=16 system.
+    """
+    import torch
+    import iccg_b200 as ib
+    import iccg_b200.problems as pb
+    side = args.side
+    variants = [("mc", "piccg", 0), ("abmc8", "abmc", 8), ("abmc16", "abmc", 16), ("abmc32", "abmc", 32)]
+    peak, peak_kind = _peaks()
+    dev = torch.device("cuda", 0)
+    out = []
+    cpu = None
+    for label, variant, B in variants:
+        t0 = time.perf_counter()
+        P = pb.config_diffusion27(side, variant, block_size=max(B, 1), seed=0)
+        host_s = time.perf_counter() - t0
+        n = P.A_run.n
+        ctx = ib.Context(0)
+        t0 = time.perf_counter()
+        ctx.upload(P.A_run)
+        ctx.set_schedule(P.sched)
+        ctx.build(ib.PRECOND_IC0, 0.0, auto_shift=True)
+        factor_s = time.perf_counter() - t0
+        b_d = torch.from_numpy(P.b_run).to(dev)
+        x_d = torch.zeros(n, dtype=torch.float64, device=dev)
+        stream = torch.cuda.ExternalStream(ctx.stream)
+        torch.cuda.synchronize()
+        row = {"variant": label, "colors": P.nc, "blocks": P.nb if variant == "abmc" else None,
+               "ic0_shift": ctx.shift, "setup_s": {"host": round(host_s, 2), "upload_and_ic0": round(factor_s, 2)}}
+        for st_name, storage in (("fp64", ib.STORE_FP64), ("mixed", ib.STORE_FP32)):
+            res = []
+            for i in range(args.warmup + args.steps):
+                with torch.cuda.stream(stream):
+                    x_d.zero_()
+                r = ctx.solve_dev(b_d.data_ptr(), x_d.data_ptr(), 10000, TOL, storage=storage, rr_interval=RR)
+                if i >= args.warmup:
+                    res.append(r)
+            ms = statistics.mean(r.solve_ms for r in res)
+            last = res[-1]
+            bm = bytes_model(P, 8 if storage == ib.STORE_FP64 else 4)
+            gbs = bm["iteration"] * last.iters / (ms * 1e-3) / 1e9
+            row[st_name] = {"ms": round(ms, 3), "iters": last.iters, "converged": last.converged,
+                            "true_rel_resid": last.true_rel_resid, "iteration_GBps": round(gbs, 1),
+                            "frac": round(gbs / peak, 4)}
+        if label == "abmc16" and not args.no_cpu_baseline:
+            from oracle import bindings as ob
+            if ob.ref() is not None:
+                cores = os.cpu_count() or 1
+                ob.ref().ref_set_threads(cores)
+                R = ob.RefProblem(4, P.A.n, P.A.rowptr, P.A.colind, P.A.val, P.block_of_old, P.nb,
+                                  P.block_color, P.nc)
+                _, it, _, cv, us = R.cg(P.b_run, np.zeros(P.A.n), 10000, TOL)
+                cpu = {"value": round(us / 1e3, 3), "unit": "ms", "cores": cores, "kind": "reference",
+                       "iters": it, "converged": bool(cv), "sample": "1 full ABMC B=16 solve, conjugate_gradient only"}
+        out.append(row)
+        del b_d, x_d
+        ctx.close()
+        torch.cuda.synchronize()
+    line = {"workload": "diffusion27", "metric": "ICCG ms to resid 1e-8 per variant", "unit": "ms",
+            "higher_is_better": False, "steps": args.steps, "warmup": args.warmup,
+            "config": {"grid": f"{side}^3", "stencil": "27-point", "n": side ** 3, "contrast": 1e4,
+                       "coefficients": "harmonic means of exp(sigma g), g a 3-cell box-smoothed Gaussian field",
+                       "tol": TOL, "rr_interval": RR, "x0": "zeros",
+                       "rhs": "b = A x*, x* ~ U(-1,1) splitmix64(0)", "blocking": "bfs"},
+            "peak_GBps": peak, "peak_source": peak_kind, "variants": out,
+            "dtype": "f64", "data": "synthetic"}
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
 
 

@@ -110,6 +110,7 @@ struct QSys {
     int maxu = 0;                            // longest unit
     bool two_phase = false;                  // S/T carry in-unit entries as -(step + 1)
     int gpc = 1;                             // groups per CTA of the two-phase kernel
+    bool q2_big = false;                     // its tile needs more than 48 KB (opt-in shared memory)
     int ni = 1;                              // in-unit entries staged per row (1, 2 or 4)
     std::vector<int> g2grid, b2slot0;        // its grids and backward reduction slots
     int b2nslots = 0;
@@ -160,6 +161,7 @@ struct QSys {
         maxu = 0;
         two_phase = false;
         gpc = 1;
+        q2_big = false;
         g2grid.clear();
         b2slot0.clear();
         b2nslots = 0;

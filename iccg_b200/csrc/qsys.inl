@@ -223,6 +223,31 @@ static void allow_smem(iccg_ctx* c, K kernel)
     done.push_back({key, c->device});
 }
 
+// Every k_sweep_q2 instantiation the sweeps launch, for tiles above the
+// default 48 KB of dynamic shared memory (set at plan time, before any
+// graph capture).
+template <class T, int NI, int KS>
+static void allow_q2_smem_t(iccg_ctx* c)
+{
+    constexpr bool f32 = std::is_same<T, float>::value;
+    allow_smem(c, k_sweep_q2<T, true, FIN_NONE, true, NI, KS>);
+    allow_smem(c, k_sweep_q2<T, false, FIN_NONE, !f32, NI, KS>);
+    allow_smem(c, k_sweep_q2<T, false, FIN_RZ, !f32, NI, KS>);
+    allow_smem(c, k_sweep_q2<T, false, FIN_RZ0, !f32, NI, KS>);
+}
+
+static void allow_q2_smem(iccg_ctx* c)
+{
+    allow_q2_smem_t<double, 1, 8>(c);
+    allow_q2_smem_t<double, 1, 16>(c);
+    allow_q2_smem_t<double, 2, 8>(c);
+    allow_q2_smem_t<double, 2, 16>(c);
+    allow_q2_smem_t<float, 1, 8>(c);
+    allow_q2_smem_t<float, 1, 16>(c);
+    allow_q2_smem_t<float, 2, 8>(c);
+    allow_q2_smem_t<float, 2, 16>(c);
+}
+
 // Grids of the staged sweeps for value type T at each level: one CTA per
 // batch up to what is resident at once at that level's buffer size.
 template <class T>
@@ -343,8 +368,9 @@ static void build_q_factor(iccg_ctx* c)
     Factor& F = c->F;
     // two-phase sweeps need units of at most 64 rows, in-unit entries last
     // (forward) / first (backward) in every row -- the reference's column
-    // order gives that for schedules from BuildABMCSchedule -- and a
-    // shared-memory tile that fits 48 KB
+    // order gives that for schedules from BuildABMCSchedule -- and the tile
+    // of one group in shared memory: up to 8 groups in 48 KB, or, for units
+    // of 32 to 64 rows, one group in the opt-in shared memory
     auto build = [&](bool enc) {
         bool ok = sell_build(c, Q.steps, F.Sp, F.Si, &F.s_src, Q.S, enc ? 1 : 0) &&
                   sell_build(c, Q.steps, F.Tp, F.Ti, &F.t_src, Q.T, enc ? 2 : 0);
@@ -364,7 +390,10 @@ static void build_q_factor(iccg_ctx* c)
         const size_t per_group = (size_t)std::max(1, Q.maxu) * 32 * row_bytes;
         Q.gpc = (int)std::max<size_t>(
             1, std::min<size_t>({8, 48 * 1024 / per_group, 32 / (size_t)std::max(1, Q.maxu)}));
-        if (per_group * Q.gpc > 48 * 1024) Q.two_phase = false;
+        Q.q2_big = per_group * Q.gpc > 48 * 1024;
+        // the kernel's static shared memory (reduction scratch) comes on top
+        if (Q.q2_big && per_group > (size_t)std::max(0, c->smem_optin - 4096)) Q.two_phase = false;
+        if (Q.two_phase && Q.q2_big) allow_q2_smem(c);
     }
     if (!Q.two_phase) build(false);
     sell_values(c, Q.S, F.dLx.get());

@@ -94,7 +94,8 @@ def _assert_x_parity(x, xo, P):
     assert best <= X_TOL, (err, best, spread)
 
 
-@pytest.mark.parametrize("which", ["c1_mc", "abmc64_bfs", "abmc64_lin", "iccg_natural", "d27_abmc", "d27_mc", "knn"])
+@pytest.mark.parametrize("which", ["c1_mc", "abmc64_bfs", "abmc64_lin", "iccg_natural", "d27_abmc", "d27_abmc32",
+                                   "d27_abmc64", "d27_mc", "knn"])
 def test_gpu_cg_parity_vs_oracle(which):
     if which == "c1_mc":
         P = pb.config_small_mc(128, seed=0)
@@ -106,6 +107,11 @@ def test_gpu_cg_parity_vs_oracle(which):
         P = pb.make(pb.laplace3d_aniso(40), "iccg", seed=1)
     elif which == "d27_abmc":
         P = pb.config_diffusion27(40, "abmc", 16)
+    elif which == "d27_abmc32":
+        # blocks of 32 rows: one group's sweep tile exceeds 48 KB of shared memory
+        P = pb.config_diffusion27(32, "abmc", 32)
+    elif which == "d27_abmc64":
+        P = pb.config_diffusion27(32, "abmc", 64)
     elif which == "d27_mc":
         P = pb.config_diffusion27(40, "piccg")
     else:
@@ -129,9 +135,11 @@ def test_gpu_cg_parity_vs_oracle(which):
     ctx.close()
 
 
-@pytest.mark.parametrize("which", ["abmc64", "d27_abmc"])
+@pytest.mark.parametrize("which", ["abmc64", "d27_abmc", "d27_abmc32"])
 def test_gpu_mixed_precision(which):
-    P = pb.config_abmc_aniso(64, 16, "bfs") if which == "abmc64" else pb.config_diffusion27(40, "abmc", 16)
+    P = {"abmc64": lambda: pb.config_abmc_aniso(64, 16, "bfs"),
+         "d27_abmc": lambda: pb.config_diffusion27(40, "abmc", 16),
+         "d27_abmc32": lambda: pb.config_diffusion27(40, "abmc", 32)}[which]()
     ctx = _ctx_for(P.A_run, P.sched)
     ctx.build(ib.PRECOND_IC0, 0.0)
     x64 = np.zeros(P.A_run.n)
@@ -305,7 +313,7 @@ def test_gpu_full_size_abmc_128():
     ctx.close()
 
 
-@pytest.mark.parametrize("which", ["mc2d", "abmc_lin", "abmc_bfs", "d27_abmc8", "d27_mc", "knn_abmc"])
+@pytest.mark.parametrize("which", ["mc2d", "abmc_lin", "abmc_bfs", "d27_abmc8", "d27_abmc32", "d27_mc", "knn_abmc"])
 def test_gpu_tiled_kernels_equal_simple_kernels(which):
     """The lane-interleaved kernels (Q order, SELL-32, staged sweeps) give
     the same bits as the one-thread-per-row (per-block) kernels in FP64 --
@@ -317,6 +325,7 @@ def test_gpu_tiled_kernels_equal_simple_kernels(which):
          "abmc_lin": lambda: pb.config_abmc_aniso(40, 16, "linear"),
          "abmc_bfs": lambda: pb.config_abmc_aniso(40, 16, "bfs"),
          "d27_abmc8": lambda: pb.config_diffusion27(24, "abmc", 8),
+         "d27_abmc32": lambda: pb.config_diffusion27(24, "abmc", 32),
          "d27_mc": lambda: pb.config_diffusion27(24, "piccg"),
          "knn_abmc": lambda: pb.config_knn(8000, seed=5, block_size=16)}[which]()
     ctx = _ctx_for(P.A_run, P.sched)
