@@ -608,6 +608,14 @@ def run_diffusion27(args):
         torch.cuda.synchronize()
         row = {"variant": label, "colors": P.nc, "blocks": P.nb if variant == "abmc" else None,
                "ic0_shift": ctx.shift, "setup_s": {"host": round(host_s, 2), "upload_and_ic0": round(factor_s, 2)}}
+        # substitution kernel per color (counts by kind) for each storage and direction
+        row["sweep_kernels"] = {}
+        for st_name, storage in (("fp64", ib.STORE_FP64), ("mixed", ib.STORE_FP32)):
+            for d in ("fwd", "bwd"):
+                kinds = {}
+                for k, _ in ctx.sweep_plan(storage, d == "fwd"):
+                    kinds[k] = kinds.get(k, 0) + 1
+                row["sweep_kernels"][f"{st_name}_{d}"] = kinds
         for st_name, storage in (("fp64", ib.STORE_FP64), ("mixed", ib.STORE_FP32)):
             res = []
             for i in range(args.warmup + args.steps):

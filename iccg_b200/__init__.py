@@ -52,6 +52,7 @@ MODE_PLAIN, MODE_FUSED = 0, 1
 OPT_TILED = 0
 OPT_SWEEP = 1
 OPT_PDL = 2
+OPT_STAGE_KB = 3
 STATUS_NAMES = {0: "converged", 1: "breakdown", 2: "max_iter", 3: "nonfinite"}
 
 
@@ -140,6 +141,7 @@ def lib() -> C.CDLL:
         "iccg_solve_dev": (_I, [_P, _P, _P, _I, _D, C.POINTER(_Opts), C.POINTER(_Result)]),
         "iccg_profile_enable": (_I, [_P, _I]),
         "iccg_profile_read": (_I, [_P, _I, C.POINTER(_D), C.POINTER(C.c_longlong)]),
+        "iccg_sweep_plan": (_I, [_P, _I, _I, _P, _P, _I, C.POINTER(_I)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -573,6 +575,17 @@ class Context:
         ms, n = C.c_double(), C.c_longlong()
         self._ck(lib().iccg_profile_read(self.h, cls, C.byref(ms), C.byref(n)))
         return ms.value, n.value
+
+    SWEEP_KINDS = ("chain", "staged", "two_phase", "one_phase", "csr")
+
+    def sweep_plan(self, storage: int = STORE_FP64, fwd: bool = True):
+        """[(kind name, CTAs)] per level of the IC(0) sweep in that direction."""
+        nl = C.c_int()
+        self._ck(lib().iccg_sweep_plan(self.h, storage, int(fwd), None, None, 0, C.byref(nl)))
+        kinds = np.zeros(max(nl.value, 1), np.int32)
+        grids = np.zeros(max(nl.value, 1), np.int32)
+        self._ck(lib().iccg_sweep_plan(self.h, storage, int(fwd), _ptr(kinds), _ptr(grids), nl.value, C.byref(nl)))
+        return [(self.SWEEP_KINDS[k], int(g)) for k, g in zip(kinds[:nl.value], grids[:nl.value])]
 
 
 def _cg_result(res: _Result) -> CGResult:

@@ -121,6 +121,7 @@ struct QSys {
     Buf<BatchDesc> bdesc;
     std::vector<int> lb;                                  // first batch of each level (nlevels + 1)
     std::vector<int> st_rows, st_slotsS, st_slotsT, st_slices;
+    std::vector<int> st_fit;                              // 1: the level's batches fit the stage budget
     // levels whose rows have in-unit entries only, one per row, the previous
     // step, in full groups of at most 16 steps: the chain-only kernel
     std::vector<int> chainS, chainT;
@@ -168,7 +169,7 @@ struct QSys {
         staged = false;
         bdesc.free();
         lb.clear();
-        for (auto* v : {&st_rows, &st_slotsS, &st_slotsT, &st_slices, &chainS, &chainT}) v->clear();
+        for (auto* v : {&st_rows, &st_slotsS, &st_slotsT, &st_slices, &st_fit, &chainS, &chainT}) v->clear();
         for (int k = 0; k < 2; ++k) {
             st_fgrid[k].clear();
             st_bgrid[k].clear();
@@ -211,6 +212,7 @@ struct iccg_ctx {
     bool use_q = true;
     int sweep_kernel = 0;   // ICCG_OPT_SWEEP: 0 staged where it fits, 1 two-phase per-slice kernel
     bool pdl = false;       // ICCG_OPT_PDL: programmatic dependent launch
+    int stage_kb = 0;       // ICCG_OPT_STAGE_KB: staged-sweep buffer budget (0: the opt-in maximum)
     int smem_optin = 0;     // largest dynamic shared memory per CTA
     iccg::QSys Q;
     // preconditioner

@@ -129,6 +129,13 @@ int iccg_ctx_set_option(iccg_ctx* c, int option, long long value)
             c->sweep_kernel = (int)value;
         } else if (option == ICCG_OPT_PDL) {
             c->pdl = value != 0;
+        } else if (option == ICCG_OPT_STAGE_KB) {
+            if (value < 0 || value > 1024) throw Error(ICCG_ERR_ARG, "ICCG_OPT_STAGE_KB takes 0 to 1024");
+            c->stage_kb = (int)value;
+            if (c->Q.two_phase && !c->Q.steps.empty()) {
+                CK(cudaStreamSynchronize(c->stream));
+                plan_staged(c);
+            }
         } else {
             throw Error(ICCG_ERR_ARG, "unknown option");
         }
@@ -355,6 +362,33 @@ int iccg_profile_read(iccg_ctx* c, int cls, double* total_ms, long long* launche
     if (total_ms) *total_ms = c->prof_ms[cls];
     if (launches) *launches = c->prof_n[cls];
     return ICCG_OK;
+}
+
+int iccg_sweep_plan(iccg_ctx* c, int storage, int fwd, int* kinds, int* grids, int cap, int* nlevels)
+{
+    return guard(c, [&] {
+        if (!nlevels || cap < 0 || (cap > 0 && (!kinds || !grids))) throw Error(ICCG_ERR_ARG, "bad argument");
+        if (storage != ICCG_STORE_FP64 && storage != ICCG_STORE_FP32) throw Error(ICCG_ERR_ARG, "bad storage");
+        require_precond(c);
+        if (c->pc_kind != ICCG_PRECOND_IC0) throw Error(ICCG_ERR_STATE, "preconditioner has no substitution sweeps");
+        prepare_path(c, storage);
+        const bool f32 = storage == ICCG_STORE_FP32;
+        if (!c->use_q) {
+            const Plan& P = fwd ? c->fwd : c->bwd;
+            *nlevels = P.nlevels;
+            for (int l = 0; l < std::min(cap, P.nlevels); ++l) {
+                kinds[l] = 4;
+                grids[l] = P.grid[(size_t)l];
+            }
+            return;
+        }
+        *nlevels = c->Q.nlevels;
+        for (int l = 0; l < std::min(cap, c->Q.nlevels); ++l) {
+            const SweepLevel s = f32 ? sweep_level<float>(c, l, fwd != 0) : sweep_level<double>(c, l, fwd != 0);
+            kinds[l] = s.kind;
+            grids[l] = s.grid;
+        }
+    });
 }
 
 }  // extern "C"

@@ -665,6 +665,66 @@ __global__ void __launch_bounds__(256) k_sweep_q(int g0, int g1, const int* __re
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(rz, red, st, ticket, slot0 + blockIdx.x, nslots);
 }
 
+// The earlier-level part of a substitution row: a - sum_j v_j prev[c_j] over
+// entries j in [j0, j1), one fused multiply-add per entry in the order of j
+// (the reference's).  KT gathers are issued before their multiply-adds, so a
+// long row waits for one gather latency per KT entries, not per entry.
+// Entry j sits at slot pb + 32 j of a SELL matrix in global memory ...
+template <int KT, class T>
+__device__ __forceinline__ double fold_ext_global(double a, int pb, int j0, int j1, const int* __restrict__ col,
+                                                  const T* __restrict__ val, const double* __restrict__ prev)
+{
+    for (int jc = j0; jc < j1; jc += KT) {
+        int c[KT];
+        T v[KT];
+        double x[KT];
+#pragma unroll
+        for (int u = 0; u < KT; ++u) {
+            const int pa = pb + 32 * (jc + u < j1 ? jc + u : jc);
+            c[u] = col[pa];
+            v[u] = val[pa];
+        }
+#pragma unroll
+        for (int u = 0; u < KT; ++u) x[u] = jc + u < j1 ? __ldg(prev + c[u]) : 0.0;
+#pragma unroll
+        for (int u = 0; u < KT; ++u)
+            if (jc + u < j1) a = fma(-(double)v[u], x[u], a);
+    }
+    return a;
+}
+
+// ... or at e + 32 j of the staged slot arrays in shared memory
+template <int KT, class T>
+__device__ __forceinline__ double fold_ext_staged(double a, int e, int j0, int j1, const int* s_col, const T* s_val,
+                                                  const double* __restrict__ prev)
+{
+    for (int jc = j0; jc < j1; jc += KT) {
+        double x[KT];
+#pragma unroll
+        for (int u = 0; u < KT; ++u) x[u] = jc + u < j1 ? __ldg(prev + s_col[e + 32 * (jc + u)]) : 0.0;
+#pragma unroll
+        for (int u = 0; u < KT; ++u)
+            if (jc + u < j1) a = fma(-(double)s_val[e + 32 * (jc + u)], x[u], a);
+    }
+    return a;
+}
+
+// the gathered values of entries [j0, j1), parked beside the staged entries
+// (the exact backward order applies them after the in-unit entries)
+template <int KT>
+__device__ __forceinline__ void park_ext_staged(int e, int j0, int j1, const int* s_col, double* s_pv,
+                                                const double* __restrict__ prev)
+{
+    for (int jc = j0; jc < j1; jc += KT) {
+        double x[KT];
+#pragma unroll
+        for (int u = 0; u < KT; ++u) x[u] = jc + u < j1 ? __ldg(prev + s_col[e + 32 * (jc + u)]) : 0.0;
+#pragma unroll
+        for (int u = 0; u < KT; ++u)
+            if (jc + u < j1) s_pv[e + 32 * (jc + u)] = x[u];
+    }
+}
+
 // Step slices of the two-phase sweeps: first Q row, SELL slot pointers of
 // the forward (S) and backward (T) matrices, and a packed word
 // rows | step << 6 | widthS << 12 | widthT << 20 (widths clamped to 255).
@@ -765,10 +825,7 @@ __global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int t
 #pragma unroll
                     for (int j = 0; j < KS; ++j)
                         if (j >= j0 && j < j1) a = fma(-(double)vj[j], xg[j], a);
-                    for (int j = max(KS, j0); j < j1; ++j) {
-                        const int pa = pb + 32 * j;
-                        a = fma(-(double)val[pa], __ldg(prev + col[pa]), a);
-                    }
+                    a = fold_ext_global<8>(a, pb, max(KS, j0), j1, col, val, prev);
                 }
                 s_acc[rr] = a;
                 if (with_r) s_rd[rr] = rq;
@@ -817,11 +874,7 @@ __global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int t
                             const int pa = p0 + 32 * (jin + k);
                             a = fma(-(double)val[pa], s_acc[base + (-col[pa] - 1) * 32], a);
                         }
-                        if (!ext_first)
-                            for (int j = ni; j < L; ++j) {
-                                const int pa = p0 + 32 * j;
-                                a = fma(-(double)val[pa], __ldg(prev + col[pa]), a);
-                            }
+                        if (!ext_first) a = fold_ext_global<8>(a, p0, ni, L, col, val, prev);
                     }
                     const double v = a / (double)s_piv[rr];
                     s_acc[rr] = v;
@@ -1065,19 +1118,13 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
                                 const double v = (double)s_val[pj ? e[k] + 32 * (j0[k] + j) : e[k]];
                                 a = pj ? fma(-v, xg[k][j], a) : a;
                             }
-                            for (int jj = j0[k] + KG; jj < j1[k]; ++jj) {
-                                const int ej = e[k] + 32 * jj;
-                                a = fma(-(double)s_val[ej], __ldg(prev + s_col[ej]), a);
-                            }
+                            a = fold_ext_staged<8>(a, e[k], j0[k] + KG, j1[k], s_col, s_val, prev);
                             s_in[rr[k]] = a;
                         } else {
 #pragma unroll
                             for (int j = 0; j < KG; ++j)
                                 if (j0[k] + j < j1[k]) s_pv[e[k] + 32 * (j0[k] + j)] = xg[k][j];
-                            for (int jj = j0[k] + KG; jj < j1[k]; ++jj) {
-                                const int ej = e[k] + 32 * jj;
-                                s_pv[ej] = __ldg(prev + s_col[ej]);
-                            }
+                            park_ext_staged<8>(e[k], j0[k] + KG, j1[k], s_col, s_pv, prev);
                         }
                     }
                 }
@@ -1138,19 +1185,13 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
 #pragma unroll
                         for (int j = 0; j < KG; ++j)
                             if (j0[u] + j < j1[u]) a = fma(-(double)s_val[e[u] + 32 * (j0[u] + j)], x[u][j], a);
-                        for (int jj = j0[u] + KG; jj < j1[u]; ++jj) {
-                            const int ej = e[u] + 32 * jj;
-                            a = fma(-(double)s_val[ej], __ldg(prev + s_col[ej]), a);
-                        }
+                        a = fold_ext_staged<8>(a, e[u], j0[u] + KG, j1[u], s_col, s_val, prev);
                         s_in[rr[u]] = a;
                     } else {
 #pragma unroll
                         for (int j = 0; j < KG; ++j)
                             if (j0[u] + j < j1[u]) s_pv[e[u] + 32 * (j0[u] + j)] = x[u][j];
-                        for (int jj = j0[u] + KG; jj < j1[u]; ++jj) {
-                            const int ej = e[u] + 32 * jj;
-                            s_pv[ej] = __ldg(prev + s_col[ej]);
-                        }
+                        park_ext_staged<8>(e[u], j0[u] + KG, j1[u], s_col, s_pv, prev);
                     }
                 }
             }

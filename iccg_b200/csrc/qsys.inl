@@ -249,7 +249,11 @@ static void allow_q2_smem(iccg_ctx* c)
 }
 
 // Grids of the staged sweeps for value type T at each level: one CTA per
-// batch up to what is resident at once at that level's buffer size.
+// batch up to what is resident at once at that level's buffer size.  The
+// staged kernel runs forward sweeps in both types and backward sweeps with
+// FP32 storage (FP64 backward sweeps use the per-slice kernel), so only
+// those buffers are sized here; levels whose batches do not fit the stage
+// budget keep grid 1 and run on the per-slice kernel.
 template <class T>
 static bool plan_staged_type(iccg_ctx* c, int k)
 {
@@ -262,21 +266,27 @@ static bool plan_staged_type(iccg_ctx* c, int k)
     const int L = Q.nlevels;
     Q.st_fgrid[k].assign((size_t)L, 1);
     Q.st_bgrid[k].assign((size_t)L, 1);
+    // the kernel's static shared memory (reduction scratch) comes on top
+    const size_t lim = (size_t)std::max(0, c->smem_optin - 2048);
     for (int l = 0; l < L; ++l) {
+        if (!Q.st_fit[(size_t)l]) continue;
         const int nb = Q.lb[(size_t)l + 1] - Q.lb[(size_t)l];
         const size_t fs = 2 * (size_t)stage_layout(Q.st_rows[(size_t)l], Q.st_slotsS[(size_t)l],
                                                    Q.st_slices[(size_t)l], (int)sizeof(T), false, false).bytes;
-        const size_t bs = 2 * (size_t)stage_layout(Q.st_rows[(size_t)l], Q.st_slotsT[(size_t)l],
-                                                   Q.st_slices[(size_t)l], (int)sizeof(T), true, exact).bytes;
-        // the kernel's static shared memory (reduction scratch) comes on top
-        const size_t lim = (size_t)std::max(0, c->smem_optin - 2048);
-        if (fs > lim || bs > lim) return false;
-        int pf = 0, pb = 0;
+        if (fs > lim) return false;
+        int pf = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf, kf, kThreads, fs));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pb, kb, kThreads, bs));
-        if (pf < 1 || pb < 1) return false;
+        if (pf < 1) return false;
         Q.st_fgrid[k][(size_t)l] = std::max(1, std::min(nb, pf * c->nsm));
-        Q.st_bgrid[k][(size_t)l] = std::max(1, std::min(nb, pb * c->nsm));
+        if (!exact) {
+            const size_t bs = 2 * (size_t)stage_layout(Q.st_rows[(size_t)l], Q.st_slotsT[(size_t)l],
+                                                       Q.st_slices[(size_t)l], (int)sizeof(T), true, false).bytes;
+            if (bs > lim) return false;
+            int pb = 0;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pb, kb, kThreads, bs));
+            if (pb < 1) return false;
+            Q.st_bgrid[k][(size_t)l] = std::max(1, std::min(nb, pb * c->nsm));
+        }
     }
     // chain-only levels: one warp per group
     int pc = 0;
@@ -295,33 +305,68 @@ static bool plan_staged_type(iccg_ctx* c, int k)
     return true;
 }
 
-// Batches of the staged sweeps: up to 16 groups of one level, about 512 rows.
+// Batches of the staged sweeps: consecutive groups of one level, at most 16
+// groups and 512 rows, and as many groups as keep the double-buffered stage
+// of every buffer the staged kernel runs with (FP64 and FP32 forward, FP32
+// backward) within the budget (ICCG_OPT_STAGE_KB, default the opt-in shared
+// memory).  A level with a group that alone exceeds the budget runs on the
+// per-slice kernel.
 static void plan_staged(iccg_ctx* c)
 {
     QSys& Q = c->Q;
     Q.staged = false;
-    const int gpc = std::max(1, std::min(16, 512 / (32 * std::max(1, Q.maxu))));
+    const int gmax = std::max(1, std::min(16, 512 / (32 * std::max(1, Q.maxu))));
+    const size_t lim = (size_t)std::max(0, c->smem_optin - 2048);
+    const size_t budget = c->stage_kb > 0 ? std::min(lim, (size_t)c->stage_kb * 1024) : lim;
     std::vector<BatchDesc> bds;
     Q.lb.assign((size_t)Q.nlevels + 1, 0);
     Q.st_rows.assign((size_t)Q.nlevels, 0);
     Q.st_slotsS.assign((size_t)Q.nlevels, 0);
     Q.st_slotsT.assign((size_t)Q.nlevels, 0);
     Q.st_slices.assign((size_t)Q.nlevels, 0);
+    Q.st_fit.assign((size_t)Q.nlevels, 1);
     Q.chainS.assign((size_t)Q.nlevels, 1);
     Q.chainT.assign((size_t)Q.nlevels, 1);
+    // groups [g, g + ng) of a level as one batch (se <= sb: not a batch)
+    auto describe = [&](int g, int ng) {
+        BatchDesc d{};
+        d.gb = g;
+        d.ng = ng;
+        d.sb = Q.h_sl0[(size_t)g];
+        d.se = Q.h_sl0[(size_t)(g + ng)];
+        if (d.se <= d.sb) return d;
+        d.qb = Q.steps[(size_t)d.sb].first;
+        d.qe = Q.steps[(size_t)d.se - 1].first + Q.steps[(size_t)d.se - 1].second;
+        d.ps0 = Q.S.h_ptr[(size_t)d.sb];
+        d.ps1 = Q.S.h_ptr[(size_t)d.se];
+        d.pt0 = Q.T.h_ptr[(size_t)d.sb];
+        d.pt1 = Q.T.h_ptr[(size_t)d.se];
+        return d;
+    };
+    // the level's buffer holds its largest batch in every dimension: the
+    // stage bytes of the level's capacities grown by batch d
+    auto stage_bytes = [&](int l, const BatchDesc& d) {
+        const int rows = std::max(Q.st_rows[(size_t)l], d.qe - d.qb);
+        const int slS = std::max(Q.st_slotsS[(size_t)l], d.ps1 - d.ps0);
+        const int slT = std::max(Q.st_slotsT[(size_t)l], d.pt1 - d.pt0);
+        const int slices = std::max(Q.st_slices[(size_t)l], d.se - d.sb);
+        return 2 * (size_t)std::max({stage_layout(rows, slS, slices, 8, false, false).bytes,
+                                     stage_layout(rows, slS, slices, 4, false, false).bytes,
+                                     stage_layout(rows, slT, slices, 4, true, false).bytes});
+    };
     for (int l = 0; l < Q.nlevels; ++l) {
         const int g1 = Q.level_g[(size_t)l + 1];
         for (int g = Q.level_g[(size_t)l]; g < g1; ++g)
             if (Q.h_glen[(size_t)g * 32] > 16) Q.chainS[(size_t)l] = Q.chainT[(size_t)l] = 0;
-        for (int g = Q.level_g[(size_t)l]; g < g1; g += gpc) {
-            BatchDesc d{};
-            d.gb = g;
-            d.ng = std::min(gpc, g1 - g);
-            d.sb = Q.h_sl0[(size_t)g];
-            d.se = Q.h_sl0[(size_t)(g + d.ng)];
+        for (int g = Q.level_g[(size_t)l]; g < g1;) {
+            BatchDesc d = describe(g, 1);
             if (d.se <= d.sb) return;
-            d.qb = Q.steps[(size_t)d.sb].first;
-            d.qe = Q.steps[(size_t)d.se - 1].first + Q.steps[(size_t)d.se - 1].second;
+            if (stage_bytes(l, d) > budget) Q.st_fit[(size_t)l] = 0;
+            while (d.ng < gmax && g + d.ng < g1 && Q.st_fit[(size_t)l]) {
+                const BatchDesc e = describe(g, d.ng + 1);
+                if (e.qe - e.qb > 512 || stage_bytes(l, e) > budget) break;
+                d = e;
+            }
             for (int s = d.sb + 1; s < d.se; ++s)
                 if (Q.steps[(size_t)s].first != Q.steps[(size_t)s - 1].first + Q.steps[(size_t)s - 1].second) return;
             // regular batch: every group full (32 units of one length) and
@@ -344,15 +389,12 @@ static void plan_staged(iccg_ctx* c)
                 if (!Q.S.unit_only[(size_t)q]) Q.chainS[(size_t)l] = 0;
                 if (!Q.T.unit_only[(size_t)q]) Q.chainT[(size_t)l] = 0;
             }
-            d.ps0 = Q.S.h_ptr[(size_t)d.sb];
-            d.ps1 = Q.S.h_ptr[(size_t)d.se];
-            d.pt0 = Q.T.h_ptr[(size_t)d.sb];
-            d.pt1 = Q.T.h_ptr[(size_t)d.se];
             Q.st_rows[(size_t)l] = std::max(Q.st_rows[(size_t)l], d.qe - d.qb);
             Q.st_slotsS[(size_t)l] = std::max(Q.st_slotsS[(size_t)l], d.ps1 - d.ps0);
             Q.st_slotsT[(size_t)l] = std::max(Q.st_slotsT[(size_t)l], d.pt1 - d.pt0);
             Q.st_slices[(size_t)l] = std::max(Q.st_slices[(size_t)l], d.se - d.sb);
             bds.push_back(d);
+            g += d.ng;
         }
         Q.lb[(size_t)l + 1] = (int)bds.size();
     }

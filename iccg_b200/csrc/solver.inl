@@ -49,7 +49,8 @@ static void apply_ic0_simple(iccg_ctx* c, const double* r, double* y, double* z,
 //    row on the previous step, in full groups of at most 16 steps;
 //  1 staged (k_sweep_st): FP32 storage, and FP64 forward sweeps -- the exact
 //    FP64 backward order would park every gathered value in the tile (twice
-//    the shared memory), where the per-slice kernel measured faster;
+//    the shared memory), where the per-slice kernel measured faster -- at
+//    levels whose batches fit the stage budget;
 //  2 per-slice two-phase (k_sweep_q2); 3 one-phase (k_sweep_q), for units of
 //    more than 64 rows.
 // The backward sweep's r.z reduction spans all its launches: slots are laid
@@ -67,7 +68,7 @@ static SweepLevel sweep_level(iccg_ctx* c, int l, bool fwd)
     const size_t l_ = (size_t)l;
     const bool st_ok = Q.staged && c->sweep_kernel == 0 && (!f32 || Q.r32_ok);
     if (st_ok && (fwd ? Q.chainS[l_] : Q.chainT[l_])) return {0, Q.ch_grid[k][l_]};
-    if (st_ok && (fwd || f32)) return {1, fwd ? Q.st_fgrid[k][l_] : Q.st_bgrid[k][l_]};
+    if (st_ok && Q.st_fit[l_] && (fwd || f32)) return {1, fwd ? Q.st_fgrid[k][l_] : Q.st_bgrid[k][l_]};
     if (Q.two_phase) return {2, Q.g2grid[l_]};
     return {3, Q.fgrid[l_]};
 }

@@ -197,10 +197,17 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
    launch, so a kernel's CTAs are placed while its predecessor drains (each
    kernel still waits for its predecessor's results).  On the 128^3 system it
    made the plain path faster and the graph-replayed fused path slower.
+   ICCG_OPT_STAGE_KB (default 0): shared memory, in KB, that a batch of the
+   staged kernel may fill with both halves of its double buffer; 0 takes
+   the device's opt-in maximum per block.  Smaller batches leave room for
+   more resident CTAs per SM.  A level with a group of units that alone
+   exceeds it runs on the per-slice kernel.  Setting it re-plans the
+   batches of a built preconditioner.
    Every choice gives the same bits with FP64 storage. */
 #define ICCG_OPT_TILED 0
 #define ICCG_OPT_SWEEP 1
 #define ICCG_OPT_PDL 2
+#define ICCG_OPT_STAGE_KB 3
 int iccg_ctx_set_option(iccg_ctx* ctx, int option, long long value);
 
 /* Uploads A_run (the matrix conjugate_gradient runs on, cg_crs.cpp:442-447):
@@ -285,6 +292,16 @@ int iccg_solve_dev(iccg_ctx* ctx, const double* b, double* x, int max_iter, doub
    the following solves with CUDA events (launches are not graphed then). */
 int iccg_profile_enable(iccg_ctx* ctx, int enable);
 int iccg_profile_read(iccg_ctx* ctx, int cls, double* total_ms, long long* launches);
+
+/* The substitution kernel that each level (color) of the IC(0) sweeps runs
+   on, for storage ICCG_STORE_FP64 / ICCG_STORE_FP32 and the forward (fwd != 0)
+   or backward sweep: kinds[l] = 0 chain-only, 1 staged, 2 per-slice
+   two-phase, 3 one-phase (units of more than 64 rows), 4 CSR (untiled
+   path); grids[l] = CTAs launched.  *nlevels receives the level count and
+   at most cap entries are written.  Sets up the FP32 copies on first use,
+   as a solve would.  No counterpart in the reference (its sweeps have one
+   OpenMP form, ic0.cpp:194-339). */
+int iccg_sweep_plan(iccg_ctx* ctx, int storage, int fwd, int* kinds, int* grids, int cap, int* nlevels);
 
 #ifdef __cplusplus
 }

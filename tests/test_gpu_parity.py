@@ -95,7 +95,7 @@ def _assert_x_parity(x, xo, P):
 
 
 @pytest.mark.parametrize("which", ["c1_mc", "abmc64_bfs", "abmc64_lin", "iccg_natural", "d27_abmc", "d27_abmc32",
-                                   "d27_abmc64", "d27_mc", "knn"])
+                                   "d27_abmc64", "abmc_b32", "p2d_abmc64", "d27_mc", "knn"])
 def test_gpu_cg_parity_vs_oracle(which):
     if which == "c1_mc":
         P = pb.config_small_mc(128, seed=0)
@@ -112,6 +112,11 @@ def test_gpu_cg_parity_vs_oracle(which):
         P = pb.config_diffusion27(32, "abmc", 32)
     elif which == "d27_abmc64":
         P = pb.config_diffusion27(32, "abmc", 64)
+    elif which == "abmc_b32":
+        # 32-row blocks of a 7-point operator: the staged kernel's batches are single 1024-row groups
+        P = pb.config_abmc_aniso(40, 32, "linear")
+    elif which == "p2d_abmc64":
+        P = pb.make(pb.poisson2d(96), "abmc", block_size=64, blocking="bfs", seed=4)
     elif which == "d27_mc":
         P = pb.config_diffusion27(40, "piccg")
     else:
@@ -353,7 +358,8 @@ def test_gpu_tiled_kernels_equal_simple_kernels(which):
     ctx.close()
 
 
-@pytest.mark.parametrize("which", ["mc2d", "abmc_lin", "abmc_bfs", "d27_abmc8", "d27_abmc32", "d27_mc", "knn_abmc"])
+@pytest.mark.parametrize("which", ["mc2d", "abmc_lin", "abmc_bfs", "d27_abmc8", "d27_abmc32", "abmc_b32", "p2d_abmc64",
+                                   "d27_mc", "knn_abmc"])
 def test_gpu_staged_sweeps_equal_per_slice_sweeps(which):
     """The staged substitution kernel (double-buffered shared-memory batches)
     against the per-slice two-phase kernel (ICCG_OPT_SWEEP = 1): the same
@@ -365,6 +371,8 @@ def test_gpu_staged_sweeps_equal_per_slice_sweeps(which):
          "abmc_bfs": lambda: pb.config_abmc_aniso(40, 16, "bfs"),
          "d27_abmc8": lambda: pb.config_diffusion27(24, "abmc", 8),
          "d27_abmc32": lambda: pb.config_diffusion27(24, "abmc", 32),
+         "abmc_b32": lambda: pb.config_abmc_aniso(40, 32, "linear"),
+         "p2d_abmc64": lambda: pb.make(pb.poisson2d(96), "abmc", block_size=64, blocking="bfs", seed=4),
          "d27_mc": lambda: pb.config_diffusion27(24, "piccg"),
          "knn_abmc": lambda: pb.config_knn(8000, seed=5, block_size=16)}[which]()
     ctx = _ctx_for(P.A_run, P.sched)
@@ -440,4 +448,62 @@ def test_gpu_pdl_launches_give_the_same_bits(which):
         assert np.array_equal(a[0], b[0])
         assert np.array_equal(a[1], b[1])
         assert a[2] == b[2]
+    ctx.close()
+
+
+@pytest.mark.parametrize("which", ["abmc_lin", "d27_mc", "d27_abmc8"])
+def test_gpu_stage_budget_keeps_fp64_bits(which):
+    """The staged kernel's batch budget (ICCG_OPT_STAGE_KB) only changes how
+    many groups a CTA stages at once, and which levels fall back to the
+    per-slice kernel: FP64 applies and solves keep their bits; FP32 storage
+    (reciprocal pivots on the staged kernel, division on the per-slice one)
+    agrees to FP32 rounding and converges to the tolerance."""
+    P = {"abmc_lin": lambda: pb.config_abmc_aniso(40, 16, "linear"),
+         "d27_mc": lambda: pb.config_diffusion27(24, "piccg"),
+         "d27_abmc8": lambda: pb.config_diffusion27(24, "abmc", 8)}[which]()
+    ctx = _ctx_for(P.A_run, P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    r = ib.gen_uniform(P.A_run.n, 31)
+    out = {}
+    plans = {}
+    for kb in (0, 48, 4):
+        ctx.set_option(ib.OPT_STAGE_KB, kb)
+        plans[kb] = [k for k, _ in ctx.sweep_plan(ib.STORE_FP32, True)]
+        res = {}
+        for st in (ib.STORE_FP64, ib.STORE_FP32):
+            x = np.zeros(P.A_run.n)
+            rr = ctx.solve(P.b_run, x, 10000, 1e-8, storage=st)
+            res[st] = (ctx.apply(r, st), x, rr)
+        out[kb] = res
+    ctx.set_option(ib.OPT_STAGE_KB, 0)
+    assert all(k in ("chain", "staged") for k in plans[0]), plans[0]
+    if which != "abmc_lin":
+        assert "two_phase" in plans[4], plans[4]   # single groups that exceed 4 KB
+    for kb in (48, 4):
+        a, b = out[0][ib.STORE_FP64], out[kb][ib.STORE_FP64]
+        assert np.array_equal(a[0], b[0])
+        assert np.array_equal(a[1], b[1])
+        assert a[2].iters == b[2].iters
+        a, b = out[0][ib.STORE_FP32], out[kb][ib.STORE_FP32]
+        assert rel_err(a[0], b[0]) < 1e-5
+        assert a[2].converged and b[2].converged and abs(a[2].iters - b[2].iters) <= 2
+        assert b[2].true_rel_resid <= 1e-8
+    ctx.close()
+
+
+def test_gpu_sweep_plan_reports_kernels():
+    """Units of 32 rows on the 27-point operator: one group's stage exceeds
+    the shared memory, so every level runs the per-slice two-phase kernel;
+    the untiled path reports the CSR kernels."""
+    P = pb.config_diffusion27(24, "abmc", 32)
+    ctx = _ctx_for(P.A_run, P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    for st in (ib.STORE_FP64, ib.STORE_FP32):
+        for fwd in (True, False):
+            plan = ctx.sweep_plan(st, fwd)
+            assert len(plan) == P.nc
+            assert all(k == "two_phase" and g >= 1 for k, g in plan), plan
+    ctx.use_tiled(False)
+    assert all(k == "csr" for k, _ in ctx.sweep_plan(ib.STORE_FP64, True))
+    ctx.use_tiled(True)
     ctx.close()
