@@ -211,7 +211,7 @@ struct iccg_ctx {
     // lane-interleaved system (default) or the simple one-thread-per-row path
     bool use_q = true;
     int sweep_kernel = 0;   // ICCG_OPT_SWEEP: 0 staged where it fits, 1 two-phase per-slice kernel
-    bool pdl = false;       // ICCG_OPT_PDL: programmatic dependent launch
+    bool pdl = true;        // ICCG_OPT_PDL: programmatic dependent launch
     int stage_kb = 0;       // ICCG_OPT_STAGE_KB: staged-sweep buffer budget (0: the opt-in maximum)
     int smem_optin = 0;     // largest dynamic shared memory per CTA
     iccg::QSys Q;

@@ -66,13 +66,15 @@ struct RedBuf {
 
 // Programmatic dependent launch: wait until the preceding kernel in the
 // stream has finished and its writes are visible (a no-op for a launch
-// without the attribute), then let the next kernel start placing its CTAs.
-// Every kernel begins with this, before any global memory access.
-__device__ __forceinline__ void grid_dep_begin()
-{
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
+// without the attribute).  Every kernel begins with this, before any global
+// memory access.
+__device__ __forceinline__ void grid_dep_begin() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Lets the next kernel start placing its CTAs once every CTA of this one has
+// called it (or exited).  The per-iteration kernels call it after their main
+// loop, before the final reduction, so the next launch overlaps only their
+// tail; the next kernel still waits for this one to finish (grid_dep_begin).
+__device__ __forceinline__ void grid_dep_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 __device__ __forceinline__ bool st_done(const SolverState* st)
 {
@@ -224,6 +226,7 @@ __global__ void __launch_bounds__(256) k_spmv(int n, const int* __restrict__ rp,
             acc2_fma(a[2], sum, sum);
         }
     }
+    grid_dep_trigger();
     if (FIN == FIN_PAP) reduce_finish<3, FIN_PAP>(a, red, st, ticket, blockIdx.x, gridDim.x);
 }
 
@@ -253,6 +256,7 @@ __global__ void __launch_bounds__(256) k_residual(int n, const int* __restrict__
         }
         if (FIN == FIN_TRUE) acc2_fma(a[0], ri, ri);
     }
+    grid_dep_trigger();
     if (FIN == FIN_INIT) reduce_finish<2, FIN_INIT>(a, red, st, ticket, blockIdx.x, gridDim.x);
     if (FIN == FIN_TRUE) {
         acc2 t[1] = {a[0]};
@@ -282,6 +286,7 @@ __global__ void __launch_bounds__(256) k_update(int n, double alpha_arg, const d
             r[k] = rk;
             if (FIN != FIN_NONE) acc2_fma(a[0], rk, rk);
         }
+        grid_dep_trigger();
         if (FIN != FIN_NONE) reduce_finish<1, FIN>(a, red, st, ticket, blockIdx.x, gridDim.x);
         return;
     }
@@ -318,6 +323,7 @@ __global__ void __launch_bounds__(256) k_update(int n, double alpha_arg, const d
         r[k] = rk;
         if (FIN != FIN_NONE) acc2_fma(a[0], rk, rk);
     }
+    grid_dep_trigger();
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(a, red, st, ticket, blockIdx.x, gridDim.x);
 }
 
@@ -352,6 +358,7 @@ __global__ void __launch_bounds__(256) k_xpay(int n, double beta_arg, const doub
         if (i < n2) pair(i);
         if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) p[n - 1] = fma(beta, p[n - 1], z[n - 1]);
     }
+    grid_dep_trigger();
     if (st && blockIdx.x == 0 && threadIdx.x == 0) {
         const int k1 = st->k + 1;
         st->k = k1;
@@ -392,6 +399,7 @@ __global__ void __launch_bounds__(256) k_dot(int n, const double* __restrict__ a
     acc2 s[1] = {{0.0, 0.0}};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         acc2_fma(s[0], a[i], b[i]);
+    grid_dep_trigger();
     reduce_finish<1, FIN_STORE>(s, red, nullptr, ticket, blockIdx.x, gridDim.x);
 }
 
@@ -411,6 +419,7 @@ __global__ void __launch_bounds__(256) k_diag_apply(int n, const double* __restr
         z[i] = zi;
         if (FIN != FIN_NONE) acc2_fma(a[0], ri, zi);
     }
+    grid_dep_trigger();
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(a, red, st, ticket, blockIdx.x, gridDim.x);
 }
 
@@ -464,6 +473,7 @@ __global__ void __launch_bounds__(256) k_sweep(SweepArgs a, int u0, int u1, int 
             if (FIN != FIN_NONE) acc2_fma(acc[0], a.rdot[i], v);
         }
     }
+    grid_dep_trigger();
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(acc, red, st, ticket, slot0 + blockIdx.x, nslots);
 }
 
@@ -563,6 +573,7 @@ __global__ void __launch_bounds__(256) k_spmv_q(int n, SellMat A, const double* 
             }
         }
     }
+    grid_dep_trigger();
     if (FIN == FIN_PAP) reduce_finish<3, FIN_PAP>(a, red, st, ticket, blockIdx.x, gridDim.x);
 }
 
@@ -600,6 +611,7 @@ __global__ void __launch_bounds__(256) k_residual_q(int n, SellMat A, const doub
             if (FIN == FIN_TRUE) acc2_fma(a[0], ri, ri);
         }
     }
+    grid_dep_trigger();
     if (FIN == FIN_INIT) reduce_finish<2, FIN_INIT>(a, red, st, ticket, blockIdx.x, gridDim.x);
     if (FIN == FIN_TRUE) {
         acc2 t[1] = {a[0]};
@@ -662,6 +674,7 @@ __global__ void __launch_bounds__(256) k_sweep_q(int g0, int g1, const int* __re
             }
         }
     }
+    grid_dep_trigger();
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(rz, red, st, ticket, slot0 + blockIdx.x, nslots);
 }
 
@@ -885,6 +898,7 @@ __global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int t
         }
         __syncthreads();
     }
+    grid_dep_trigger();
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(rz, red, st, ticket, slot0 + blockIdx.x, nslots);
 }
 
@@ -1319,6 +1333,7 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
             has_next = has_nn;
         }
     }
+    grid_dep_trigger();
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(rz, red, st, ticket, slot0 + blockIdx.x, nslots);
 }
 
@@ -1399,6 +1414,7 @@ __global__ void __launch_bounds__(256) k_sweep_chain(int g0, int g1, const int* 
             A = B;
         }
     }
+    grid_dep_trigger();
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(rz, red, st, ticket, slot0 + blockIdx.x, nslots);
 }
 

@@ -193,10 +193,11 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
    ICCG_OPT_SWEEP (default 0), lane-interleaved substitutions: 0 uses the
    staged kernel (double-buffered shared-memory batches) where a batch fits
    shared memory, 1 forces the per-slice two-phase kernel.
-   ICCG_OPT_PDL (default 0): 1 launches kernels with programmatic dependent
-   launch, so a kernel's CTAs are placed while its predecessor drains (each
-   kernel still waits for its predecessor's results).  On the 128^3 system it
-   made the plain path faster and the graph-replayed fused path slower.
+   ICCG_OPT_PDL (default 1): 1 launches kernels with programmatic dependent
+   launch: the per-iteration kernels let the next launch start once their
+   main loop is done, so it is placed while their tail (the reduction) runs;
+   every kernel still waits for its predecessor's results.  0 launches each
+   kernel after its predecessor has finished.
    ICCG_OPT_STAGE_KB (default 0): shared memory, in KB, that a batch of the
    staged kernel may fill with both halves of its double buffer; 0 takes
    the device's opt-in maximum per block.  Smaller batches leave room for
