@@ -1226,17 +1226,52 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
                     const int len = gl[k];
                     const int base = s_meta[gs[k] - cur.sb].q0 - cur.qb + lane;
                     double last = 0.0;
+                    if constexpr (EXACT) {
+                        // FP64: one step's tile words are loaded a step ahead,
+                        // so the shared-memory latency stays off a chain whose
+                        // steps end in a division (it only carries `last`)
+                        struct Row {
+                            double a, rd;
+                            T iv, piv;
+                            int iw;
+                        };
+                        auto row = [&](int t) {
+                            const int rr = base + 32 * (FWD ? t : len - 1 - t);
+                            Row q;
+                            q.a = s_in[rr];
+                            q.iv = s_iv[rr];
+                            q.iw = s_iw[rr];
+                            q.piv = s_piv[rr];
+                            q.rd = with_r ? s_rd[rr] : 0.0;
+                            return q;
+                        };
+                        Row R = len > 0 ? row(0) : Row{};
+#pragma unroll 4
+                        for (int t = 0; t < len; ++t) {
+                            const Row N = t + 1 < len ? row(t + 1) : R;
+                            const int rr = base + 32 * (FWD ? t : len - 1 - t);
+                            double a = R.a;
+                            const double x = fma(-(double)R.iv, last, a);
+                            a = (R.iw >> 16) ? x : a;
+                            const double v = a / (double)R.piv;
+                            out[cur.qb + rr] = v;
+                            if (with_r) acc2_fma(rz[0], R.rd, v);
+                            last = v;
+                            R = N;
+                        }
+                    } else {
 #pragma unroll 8
-                    for (int t = 0; t < len; ++t) {
-                        const int rr = base + 32 * (FWD ? t : len - 1 - t);
-                        double a = s_in[rr];
-                        const double x = fma(-(double)s_iv[rr], last, a);
-                        a = (s_iw[rr] >> 16) ? x : a;
-                        const double v = EXACT ? a / (double)s_piv[rr] : a * (double)s_piv[rr];
-                        s_in[rr] = v;
-                        out[cur.qb + rr] = v;
-                        if (with_r) acc2_fma(rz[0], s_rd[rr], v);
-                        last = v;
+                        for (int t = 0; t < len; ++t) {
+                            const int rr = base + 32 * (FWD ? t : len - 1 - t);
+                            double a = s_in[rr];
+                            const double x = fma(-(double)s_iv[rr], last, a);
+                            a = (s_iw[rr] >> 16) ? x : a;
+                            const double v = EXACT ? a / (double)s_piv[rr] : a * (double)s_piv[rr];
+                            s_in[rr] = v;
+                            out[cur.qb + rr] = v;
+                            if (with_r) acc2_fma(rz[0], s_rd[rr], v);
+                            last = v;
+                        }
                     }
                 }
             } else {
@@ -1318,10 +1353,23 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
                     last = v;
                     lastr = r;
                 };
-                for (int t = 0; t < maxlen; ++t) {
-                    Step A{};
-                    fetch(t, A);
-                    step(t, A);
+                if constexpr (EXACT) {
+                    // FP64: each step's tile words are fetched a step ahead
+                    // (they are the row's own, never written by the steps
+                    // before it)
+                    Step A{}, B{};
+                    fetch(0, A);
+                    for (int t = 0; t < maxlen; ++t) {
+                        if (t + 1 < maxlen) fetch(t + 1, B);
+                        step(t, A);
+                        A = B;
+                    }
+                } else {
+                    for (int t = 0; t < maxlen; ++t) {
+                        Step A{};
+                        fetch(t, A);
+                        step(t, A);
+                    }
                 }
             }
             }
