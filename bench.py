@@ -425,6 +425,8 @@ def main():
                          "Laplacian solves under a device-memory budget; diffusion27: multicolor vs "
                          "ABMC B=8/16/32 on the 27-point variable-coefficient 96^3 problem")
     ap.add_argument("--side", type=int, default=96, help="diffusion27: grid side")
+    ap.add_argument("--variant", choices=["mc", "abmc8", "abmc16", "abmc32"], default="mc",
+                    help="diffusion27 with --kernel-only: the ordering of the system")
     ap.add_argument("--systems", type=int, default=512, help="batched: number of systems")
     ap.add_argument("--threads", type=int, default=16, help="batched / serving: concurrent solves")
     ap.add_argument("--requests", type=int, default=200, help="serving: requests per arrival rate")
@@ -434,10 +436,10 @@ def main():
         run_batched(args)
     elif args.workload == "serving":
         run_serving(args)
-    elif args.workload == "diffusion27":
-        run_diffusion27(args)
     elif args.kernel_only:
         run_kernel_only(args)
+    elif args.workload == "diffusion27":
+        run_diffusion27(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
@@ -659,10 +661,18 @@ def run_diffusion27(args):
 
 
 def run_kernel_only(args):
-    """One operation of the hot path on the benchmark system, repeated."""
+    """One operation of the hot path on the benchmark system (or, with
+    --workload diffusion27, the 27-point system of --side and --variant),
+    repeated."""
     import torch
     import iccg_b200 as ib
-    P, _ = build_problem()
+    if args.workload == "diffusion27":
+        import iccg_b200.problems as pb
+        variant, B = {"mc": ("piccg", 16), "abmc8": ("abmc", 8), "abmc16": ("abmc", 16),
+                      "abmc32": ("abmc", 32)}[args.variant]
+        P = pb.config_diffusion27(args.side, variant, block_size=B, seed=0)
+    else:
+        P, _ = build_problem()
     n = P.A_run.n
     ctx = ib.Context(0)
     ctx.upload(P.A_run)
