@@ -419,11 +419,13 @@ def main():
                     help="set up the workload, then launch only this operation --reps times "
                          "(FP32 storage) and print its mean device time; for profilers")
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--workload", choices=["abmc128", "batched", "serving", "diffusion27"], default="abmc128",
+    ap.add_argument("--workload", choices=["abmc128", "batched", "serving", "diffusion27", "poisson2d"],
+                    default="abmc128",
                     help="abmc128: the headline solve (default); batched: many uneven systems with 4 "
                          "right-hand sides each, solved concurrently; serving: Poisson-arriving kNN "
                          "Laplacian solves under a device-memory budget; diffusion27: multicolor vs "
-                         "ABMC B=8/16/32 on the 27-point variable-coefficient 96^3 problem")
+                         "ABMC B=8/16/32 on the 27-point variable-coefficient 96^3 problem; poisson2d: "
+                         "plain FP64 multicolor ICCG on the 2D 5-point 128^2 Poisson problem")
     ap.add_argument("--side", type=int, default=96, help="diffusion27: grid side")
     ap.add_argument("--variant", choices=["mc", "abmc8", "abmc16", "abmc32"], default="mc",
                     help="diffusion27 with --kernel-only: the ordering of the system")
@@ -440,6 +442,8 @@ def main():
         run_kernel_only(args)
     elif args.workload == "diffusion27":
         run_diffusion27(args)
+    elif args.workload == "poisson2d":
+        run_poisson2d(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
@@ -655,6 +659,66 @@ def run_diffusion27(args):
                        "rhs": "b = A x*, x* ~ U(-1,1) splitmix64(0)", "blocking": "bfs"},
             "peak_GBps": peak, "peak_source": peak_kind, "variants": out,
             "dtype": "f64", "data": "synthetic"}
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
+def run_poisson2d(args):
+    """The small multicolor case: 2D 5-point Poisson, 128 x 128 interior grid
+    with Dirichlet boundaries (n = 16,384, nnz = 81,408), greedy multicolor
+    IC(0), b = A x*, x* ~ U(-1,1) from splitmix64(0), x0 = 0, tolerance 1e-8.
+    Everything (A, L, vectors: about 4.4 MB per iteration) stays in L2, so a
+    solve is bound by launch and reduction latency, not by HBM; it is
+    reported in ms.  Device ms per solve (CUDA events, mean over --steps after
+    --warmup) for the FP64 paths (fused, and plain: one kernel per reference
+    operation) and the mixed form, the same solve end to end through the C
+    ABI with host buffers, and the reference's OpenMP CG on the host cores.
+    """
+    import iccg_b200 as ib
+    import iccg_b200.problems as pb
+    P = pb.config_small_mc(128, seed=0)
+    n = P.A_run.n
+    ctx = ib.Context(0)
+    ctx.upload(P.A_run)
+    ctx.set_schedule(P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    out = {}
+    for name, storage, mode in (("fp64_fused", ib.STORE_FP64, ib.MODE_FUSED),
+                                ("fp64_plain", ib.STORE_FP64, ib.MODE_PLAIN),
+                                ("mixed_fused", ib.STORE_FP32, ib.MODE_FUSED)):
+        res, wall = [], []
+        for i in range(args.warmup + args.steps):
+            x = np.zeros(n)
+            t0 = time.perf_counter()
+            r = ctx.solve(P.b_run, x, 10000, TOL, mode=mode, storage=storage, rr_interval=RR)
+            if i >= args.warmup:
+                res.append(r)
+                wall.append((time.perf_counter() - t0) * 1e3)
+        out[name] = {"ms": round(statistics.mean(r.solve_ms for r in res), 4), "iters": res[-1].iters,
+                     "true_rel_resid": res[-1].true_rel_resid,
+                     "e2e_ms": round(statistics.mean(wall), 4)}
+    ctx.close()
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import bindings as ob
+        if ob.ref() is not None:
+            cores = os.cpu_count() or 1
+            ob.ref().ref_set_threads(cores)
+            R = ob.RefProblem(3, n, P.A.rowptr, P.A.colind, P.A.val, P.color, P.nc)
+            times, it = [], 0
+            for _ in range(max(3, args.steps)):
+                _, it, _, _, us = R.cg(P.b_run, np.zeros(n), 10000, TOL)
+                times.append(us / 1e3)
+            cpu = {"value": round(statistics.median(times), 4), "unit": "ms", "cores": cores, "kind": "reference",
+                   "iters": it, "sample": f"{max(3, args.steps)} full solves (median), conjugate_gradient only"}
+    line = {"workload": "poisson2d", "metric": "ICCG ms to resid 1e-8", "unit": "ms", "higher_is_better": False,
+            "steps": args.steps, "warmup": args.warmup,
+            "config": {"grid": "128^2", "stencil": "5-point", "n": n, "nnz": P.A_run.nnz, "colors": P.nc,
+                       "ordering": "greedy multicolor", "tol": TOL, "x0": "zeros",
+                       "rhs": "b = A x*, x* ~ U(-1,1) splitmix64(0)",
+                       "l2": "L2-resident (about 4.4 MB per iteration): latency-bound, reported in ms"},
+            "paths": out, "dtype": "f64", "data": "synthetic"}
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
