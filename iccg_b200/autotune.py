@@ -1,0 +1,158 @@
+"""Per-matrix tuning: the ordering of a system and the kernel options of a
+context, chosen by timing solves on the device.
+
+The reference takes its coloring or ABMC blocking from external files
+(run_mc.sh, run_abmc.sh) and runs one OpenMP code path. On the GPU the best
+ordering depends on the matrix: more, smaller units give more parallel
+chains per color but more colors and iterations. So the tuner times the
+candidates on the matrix itself.
+
+* ``tune_ordering(A, ...)`` builds every candidate ordering (multicolor,
+  ABMC with each block size) with this package's generators. It times one
+  full solve of each on the device, after a warm-up solve, and returns the
+  fastest ``Problem`` with the table of timings. Candidates differ in
+  iteration count as well as in speed per iteration; the tuner compares
+  time to tolerance.
+* ``tune_kernels(ctx, b_run, ...)`` chooses the context options of a built
+  system by coordinate search: for each option in turn it keeps the value
+  with the lowest median solve time, the others held at their best so far.
+  The options are the sweep kernel (staged or per-slice), the staged
+  kernel's shared-memory budget, and programmatic dependent launch. With
+  FP64 storage every choice gives the same bits. With FP32 storage the
+  staged and per-slice sweeps round differently (reciprocal pivots against
+  divisions), so the tuned result can differ in the last bits from an
+  untuned one. Both meet the tolerance.
+
+Timing goes through a ``timer`` callable that returns (ms, iterations,
+converged) for a candidate (by default the median device time of solves on
+the GPU), so the selection logic can be driven without a GPU.
+"""
+from __future__ import annotations
+
+import statistics
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import (CRS, MODE_FUSED, OPT_PDL, OPT_STAGE_KB, OPT_SWEEP, PRECOND_IC0, STORE_FP32, Context)
+from .problems import Problem, make
+
+# (variant, block size) candidates: multicolor and ABMC with 8, 16, 32 rows per block
+ORDERINGS: Tuple[Tuple[str, int], ...] = (("piccg", 0), ("abmc", 8), ("abmc", 16), ("abmc", 32))
+
+# option -> candidate values, in the order they are tried (the first is the default)
+KERNEL_OPTIONS: Tuple[Tuple[int, Tuple[int, ...]], ...] = (
+    (OPT_SWEEP, (0, 1)),
+    (OPT_STAGE_KB, (0, 160, 112, 80)),
+    (OPT_PDL, (1, 0)),
+)
+OPTION_NAMES = {OPT_SWEEP: "sweep", OPT_STAGE_KB: "stage_kb", OPT_PDL: "pdl"}
+
+
+@dataclass
+class Trial:
+    label: str
+    ms: float
+    iters: int
+    converged: bool
+
+
+@dataclass
+class TuneResult:
+    best: str
+    trials: List[Trial] = field(default_factory=list)
+    choice: Dict = field(default_factory=dict)
+
+    def table(self) -> List[dict]:
+        return [{"candidate": t.label, "ms": round(t.ms, 4), "iters": t.iters, "converged": t.converged}
+                for t in self.trials]
+
+
+def _label(variant: str, block: int) -> str:
+    return "mc" if variant == "piccg" else f"abmc{block}"
+
+
+def _solve_time(ctx: Context, b_run: np.ndarray, storage: int, tol: float, reps: int) -> Tuple[float, int, bool]:
+    """Median device ms of `reps` solves after one warm-up; iterations and
+    convergence of the last."""
+    ms, res = [], None
+    for i in range(reps + 1):
+        x = np.zeros(b_run.shape[0])
+        res = ctx.solve(b_run, x, 10000, tol, mode=MODE_FUSED, storage=storage)
+        if i:
+            ms.append(res.solve_ms)
+    return statistics.median(ms), res.iters, bool(res.converged)
+
+
+def pick(trials: Sequence[Trial]) -> Trial:
+    """The fastest converged trial (ties: the first); if none converged, the
+    fastest."""
+    ok = [t for t in trials if t.converged]
+    pool = ok if ok else list(trials)
+    return min(pool, key=lambda t: t.ms)
+
+
+def tune_ordering(A: CRS, candidates: Sequence[Tuple[str, int]] = ORDERINGS, storage: int = STORE_FP32,
+                  tol: float = 1e-8, seed: int = 0, device: int = 0, reps: int = 1,
+                  blocking: str = "bfs",
+                  timer: Optional[Callable[[Problem], Tuple[float, int, bool]]] = None) -> Tuple[Problem, TuneResult]:
+    """Builds each candidate ordering of A (the original, unpermuted matrix)
+    and returns the one whose solve to `tol` is fastest, with the timings.
+    `timer(P)` returns (ms, iterations, converged) for a built problem; the
+    default uploads P to a fresh context on `device` and times `reps` solves."""
+
+    def device_timer(P: Problem) -> Tuple[float, int, bool]:
+        ctx = Context(device)
+        try:
+            ctx.upload(P.A_run)
+            ctx.set_schedule(P.sched)
+            ctx.build(PRECOND_IC0, 0.0, auto_shift=True)
+            return _solve_time(ctx, P.b_run, storage, tol, reps)
+        finally:
+            ctx.close()
+
+    timer = timer or device_timer
+    trials: List[Trial] = []
+    built: Dict[str, Problem] = {}
+    for variant, block in candidates:
+        label = _label(variant, block)
+        P = make(A, variant, block_size=max(block, 1), blocking=blocking, seed=seed, name=label)
+        ms, iters, conv = timer(P)
+        trials.append(Trial(label, ms, iters, conv))
+        built[label] = P
+    best = pick(trials)
+    res = TuneResult(best=best.label, trials=trials,
+                     choice={"ordering": best.label, "ms": best.ms, "iters": best.iters})
+    return built[best.label], res
+
+
+def tune_kernels(ctx: Context, b_run: np.ndarray, storage: int = STORE_FP32, tol: float = 1e-8, reps: int = 2,
+                 options: Sequence[Tuple[int, Sequence[int]]] = KERNEL_OPTIONS,
+                 timer: Optional[Callable[[], Tuple[float, int, bool]]] = None) -> TuneResult:
+    """Coordinate search over the context options of a built system; leaves
+    the best values set on `ctx` and returns the timings.  `timer()` times
+    the current settings (default: `reps` solves of b_run after a warm-up)."""
+    timer = timer or (lambda: _solve_time(ctx, b_run, storage, tol, reps))
+    current = {opt: vals[0] for opt, vals in options}
+    for opt, v in current.items():
+        ctx.set_option(opt, v)
+    trials: List[Trial] = []
+    best_ms = None
+    for opt, vals in options:
+        scored = []
+        for v in vals:
+            ctx.set_option(opt, v)
+            ms, iters, conv = timer()
+            label = ",".join(f"{OPTION_NAMES.get(o, o)}={current[o] if o != opt else v}" for o, _ in options)
+            t = Trial(label, ms, iters, conv)
+            trials.append(t)
+            scored.append((t, v))
+        win = pick([t for t, _ in scored])
+        current[opt] = next(v for t, v in scored if t is win)
+        ctx.set_option(opt, current[opt])
+        best_ms = win.ms
+    choice = {OPTION_NAMES.get(o, str(o)): v for o, v in current.items()}
+    choice["ms"] = best_ms
+    return TuneResult(best=",".join(f"{k}={v}" for k, v in choice.items() if k != "ms"), trials=trials,
+                      choice=choice)

@@ -1,0 +1,80 @@
+"""Per-matrix tuning logic (iccg_b200.autotune) on the CPU, with fake timers.
+
+The device timings are replaced by functions of the candidate, so the tests
+check which candidate the search keeps and what it leaves set, not speed.
+"""
+import numpy as np
+
+import iccg_b200 as ib
+import iccg_b200.autotune as at
+import iccg_b200.problems as pb
+
+
+def test_pick_prefers_fastest_converged():
+    trials = [at.Trial("a", 5.0, 10, True), at.Trial("b", 3.0, 10, False), at.Trial("c", 4.0, 12, True)]
+    assert at.pick(trials).label == "c"
+    none = [at.Trial("a", 5.0, 10, False), at.Trial("b", 3.0, 10, False)]
+    assert at.pick(none).label == "b"
+    tie = [at.Trial("a", 2.0, 10, True), at.Trial("b", 2.0, 9, True)]
+    assert at.pick(tie).label == "a"
+
+
+def test_tune_ordering_builds_candidates_and_returns_the_fastest():
+    A = pb.poisson2d(24)
+    cost = {"mc": 7.0, "abmc8": 3.0, "abmc16": 4.0, "abmc32": 9.0}
+    seen = []
+
+    def timer(P):
+        seen.append((P.name, P.variant, P.nb, P.nc))
+        return cost[P.name], 40, True
+
+    P, res = at.tune_ordering(A, timer=timer)
+    assert [s[0] for s in seen] == ["mc", "abmc8", "abmc16", "abmc32"]
+    assert res.best == "abmc8" and P.name == "abmc8" and P.variant == "abmc"
+    assert P.info["block_size"] == 8 and P.nb > 0
+    assert len(res.table()) == 4
+    # the chosen problem is the one built: same b, same ordering as make()
+    ref = pb.make(A, "abmc", block_size=8, blocking="bfs", seed=0)
+    assert np.array_equal(P.new_of_old, ref.new_of_old)
+    assert np.array_equal(P.b_run, ref.b_run)
+
+
+class FakeCtx:
+    def __init__(self):
+        self.opts = {}
+        self.history = []
+
+    def set_option(self, opt, v):
+        self.opts[opt] = v
+        self.history.append((opt, v))
+
+
+def test_tune_kernels_coordinate_search_leaves_best_options_set():
+    ctx = FakeCtx()
+    # cost: per-slice sweeps faster, 112 KB stages best, PDL on better
+    def timer():
+        o = ctx.opts
+        ms = 10.0
+        ms -= 1.0 if o[ib.OPT_SWEEP] == 1 else 0.0
+        ms -= {0: 0.0, 160: 0.2, 112: 0.5, 80: 0.3}[o[ib.OPT_STAGE_KB]]
+        ms -= 0.4 if o[ib.OPT_PDL] == 1 else 0.0
+        return ms, 50, True
+
+    res = at.tune_kernels(ctx, np.zeros(4), timer=timer)
+    assert ctx.opts == {ib.OPT_SWEEP: 1, ib.OPT_STAGE_KB: 112, ib.OPT_PDL: 1}
+    assert res.choice["sweep"] == 1 and res.choice["stage_kb"] == 112 and res.choice["pdl"] == 1
+    assert abs(res.choice["ms"] - (10.0 - 1.0 - 0.5 - 0.4)) < 1e-12
+    assert len(res.trials) == 2 + 4 + 2
+
+
+def test_tune_kernels_skips_unconverged_settings():
+    ctx = FakeCtx()
+
+    def timer():
+        # the per-slice kernel "fails" here: fastest but not converged
+        if ctx.opts[ib.OPT_SWEEP] == 1:
+            return 1.0, 10000, False
+        return 5.0, 50, True
+
+    at.tune_kernels(ctx, np.zeros(4), timer=timer)
+    assert ctx.opts[ib.OPT_SWEEP] == 0
