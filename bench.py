@@ -561,8 +561,13 @@ def run_serving(args):
         st = loop.run(make_requests(f * sat)).summary()
         st["arrival_rate_per_s"] = round(f * sat, 2)
         out.append(st)
+    # the same top rate with a fresh context per request (no worker pool)
+    loop = bt.ServingLoop(budget_bytes=100 * 10**9, workers=args.threads, pool=False)
+    unpooled = loop.run(make_requests(sat)).summary()
+    unpooled["arrival_rate_per_s"] = round(sat, 2)
     line = {"workload": "serving", "requests_per_rate": len(sizes), "points": {"min": min(sizes), "max": max(sizes)},
             "threads": args.threads, "budget_bytes": 100 * 10**9, "rates": out,
+            "context_per_request_at_top_rate": unpooled,
             "one_at_a_time_ms": {"mixed_end_to_end_mean": round(statistics.mean(alone_ms), 3),
                                  "plain_fp64_solve_mean": round(statistics.mean(plain_ms), 3)},
             "plain_fp64_one_at_a_time_solves_per_s": round(1000.0 / statistics.mean(plain_ms), 2),

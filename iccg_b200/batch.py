@@ -43,12 +43,17 @@ class SolveRecord:
 
 
 class ResidentSystem:
-    """One system on the device: A_run, schedule and IC(0) factor resident."""
+    """One system on the device: A_run, schedule and IC(0) factor resident.
 
-    def __init__(self, P: Problem, device: int = 0, storage: int = STORE_FP32):
+    With `ctx` the system is loaded into that (borrowed) context, replacing
+    whatever it held; the context's device buffers are reused where they are
+    large enough, and close() leaves the context open."""
+
+    def __init__(self, P: Problem, device: int = 0, storage: int = STORE_FP32, ctx: Optional[Context] = None):
         self.P = P
         self.storage = storage
-        self.ctx = Context(device)
+        self._own = ctx is None
+        self.ctx = Context(device) if ctx is None else ctx
         self.ctx.upload(P.A_run)
         self.ctx.set_schedule(P.sched)
         self.ctx.build(P.precond_kind if P.precond_kind != 2 else PRECOND_IC0, 0.0)
@@ -65,7 +70,8 @@ class ResidentSystem:
         return x, res, (time.perf_counter() - t0) * 1e3
 
     def close(self):
-        self.ctx.close()
+        if self._own:
+            self.ctx.close()
 
 
 def solve_batch(systems: Sequence[ResidentSystem], rhs: Sequence[Sequence[np.ndarray]], threads: int = 8,
@@ -124,17 +130,26 @@ class ServingLoop:
     Requests are admitted in arrival order once they have arrived, as long as
     the admitted solves' device memory stays within `budget_bytes` and a
     worker slot is free. An admitted request builds its system (host set-up,
-    upload, IC(0) on the device), solves it, and frees the device memory
-    when done. Up to `workers` solves overlap on the GPU.
+    upload, IC(0) on the device) and solves it. Up to `workers` solves
+    overlap on the GPU.
+
+    With `pool` (the default) each worker keeps one context for the whole
+    run: a request loads its system into a free worker context, whose device
+    buffers only grow, so a steady stream of requests neither allocates nor
+    frees device memory (cudaFree would synchronise the whole device and
+    stall the other solves in flight). Without it every request creates and
+    destroys its own context. The pooled contexts hold at most `workers`
+    times the largest system served.
     """
 
     def __init__(self, budget_bytes: int, workers: int = 8, device: int = 0, storage: int = STORE_FP32,
-                 tol: float = 1e-8):
+                 tol: float = 1e-8, pool: bool = True):
         self.budget = budget_bytes
         self.workers = workers
         self.device = device
         self.storage = storage
         self.tol = tol
+        self.pool = pool
 
     def run(self, requests: Sequence[Request]) -> ServingStats:
         stats = ServingStats()
@@ -143,13 +158,28 @@ class ServingLoop:
         queue = sorted(requests, key=lambda r: r.arrival_s)
         t_start = time.perf_counter()
 
+        free_ctx: List[Context] = []
+        all_ctx: List[Context] = []
+
         def serve(req: Request):
+            ctx = None
             try:
                 P = req.build()
-                sysm = ResidentSystem(P, self.device, self.storage)
+                if self.pool:
+                    with lock:
+                        if free_ctx:
+                            ctx = free_ctx.pop()
+                        else:
+                            ctx = Context(self.device)
+                            all_ctx.append(ctx)
+                sysm = ResidentSystem(P, self.device, self.storage, ctx=ctx)
                 try:
                     with lock:
-                        stats.peak_bytes = max(stats.peak_bytes, in_use[0] - req.est_bytes + sysm.device_bytes)
+                        if self.pool:
+                            held = sum(c.device_bytes for c in all_ctx)
+                        else:
+                            held = in_use[0] - req.est_bytes + sysm.device_bytes
+                        stats.peak_bytes = max(stats.peak_bytes, held)
                     _, res, _ = sysm.solve(P.b_run, self.tol)
                 finally:
                     sysm.close()
@@ -165,6 +195,8 @@ class ServingLoop:
                     stats.failed += 1
             finally:
                 with lock:
+                    if ctx is not None:
+                        free_ctx.append(ctx)
                     in_use[0] -= req.est_bytes
                     lock.notify_all()
 
@@ -186,6 +218,8 @@ class ServingLoop:
             for f in active:
                 f.result()
         stats.elapsed_s = time.perf_counter() - t_start
+        for c in all_ctx:
+            c.close()
         return stats
 
 

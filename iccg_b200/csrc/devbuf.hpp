@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <string>
 
 #include "host.hpp"
@@ -36,24 +37,35 @@ struct DevMem {
 };
 
 // Device array of T.  Every allocation carries 16 elements of padding.
+// Grow-only: a buffer keeps its allocation when it is cleared or asked for
+// fewer elements, and grows with 25 % headroom, so a context that is reused
+// for system after system (a serving worker's) rarely calls cudaFree, which
+// synchronises the whole device, or cudaMalloc.  The memory goes back when
+// the buffer is destroyed (or release() is called).
 template <class T>
 struct Buf {
     DevMem m;
-    size_t n = 0;
+    size_t n = 0;    // elements in use
+    size_t cap = 0;  // elements allocated (plus the padding)
     T* get() const { return (T*)m.p; }
     void alloc(size_t count, long long* counter)
     {
-        if (count == n && m.p) return;
+        if (m.p && count <= cap) {
+            n = count;
+            return;
+        }
+        const size_t want = m.p ? std::max(count, cap + cap / 4) : count;
         m.release();
-        n = count;
-        const size_t bytes = (count + 16) * sizeof(T);
+        n = cap = 0;
+        const size_t bytes = (want + 16) * sizeof(T);
         cudaError_t e = cudaMalloc(&m.p, bytes);
         if (e != cudaSuccess) {
             m.p = nullptr;
-            n = 0;
             cudaGetLastError();
             throw Error(ICCG_ERR_NOMEM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
         }
+        n = count;
+        cap = want;
         m.bytes = bytes;
         m.counter = counter;
         *counter += (long long)bytes;
@@ -63,10 +75,12 @@ struct Buf {
         alloc(count, counter);
         if (count) CK(cudaMemcpyAsync(m.p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
     }
-    void free()
+    // clears the contents; the allocation stays for reuse
+    void free() { n = 0; }
+    void release()
     {
         m.release();
-        n = 0;
+        n = cap = 0;
     }
 };
 

@@ -57,3 +57,28 @@ def test_serving_loop_admits_under_budget():
     assert s["solves"] == len(sizes) and s["failed"] == 0
     assert s["p99_ms"] >= s["p50_ms"] > 0
     assert s["solves_per_s"] > 0
+
+
+@pytest.mark.parametrize("storage", [ib.STORE_FP64, ib.STORE_FP32])
+def test_reused_context_gives_the_same_bits_as_a_fresh_one(storage):
+    """A serving worker loads system after system into one context, whose
+    device buffers only grow.  A smaller system loaded after a larger one,
+    and the larger one loaded again, solve to the same bits as in fresh
+    contexts."""
+    big = pb.config_abmc_aniso(32, 16, "bfs", seed=1)
+    small = pb.make(pb.poisson2d(40), "piccg", seed=2)
+    fresh = {}
+    for name, P in (("big", big), ("small", small)):
+        s = bt.ResidentSystem(P, storage=storage)
+        fresh[name] = s.solve(P.b_run)[0]
+        s.close()
+    ctx = ib.Context(0)
+    try:
+        for name, P in (("big", big), ("small", small), ("big", big)):
+            s = bt.ResidentSystem(P, storage=storage, ctx=ctx)
+            x, res, _ = s.solve(P.b_run)
+            s.close()
+            assert res.converged
+            assert np.array_equal(x, fresh[name]), name
+    finally:
+        ctx.close()
