@@ -201,39 +201,51 @@ CRS gen_knn_laplacian(int npts, int k, double diag_shift, uint64_t seed)
         std::partial_sort(cand.begin(), cand.begin() + k, cand.end());
         for (int t = 0; t < k; ++t) nbr[(size_t)i * k + t] = cand[(size_t)t].second;
     }
-    // symmetrise
-    std::vector<std::pair<int, int>> edges;
-    edges.reserve((size_t)n * k * 2);
+    // symmetrise: row i holds its k neighbours and every point that has i
+    // among its neighbours, ascending, without repeats (per-row buckets,
+    // each sorted on its own)
+    std::vector<int> deg((size_t)n + 1, 0);
     for (int i = 0; i < n; ++i)
         for (int t = 0; t < k; ++t) {
-            const int j = nbr[(size_t)i * k + t];
-            edges.emplace_back(i, j);
-            edges.emplace_back(j, i);
+            deg[(size_t)i + 1]++;
+            deg[(size_t)nbr[(size_t)i * k + t] + 1]++;
         }
-    std::sort(edges.begin(), edges.end());
-    edges.erase(std::unique(edges.begin(), edges.end()), edges.end());
+    for (int i = 0; i < n; ++i) deg[(size_t)i + 1] += deg[(size_t)i];
+    std::vector<int> adj((size_t)deg[(size_t)n]);
+    {
+        std::vector<int> cur(deg.begin(), deg.end() - 1);
+        for (int i = 0; i < n; ++i)
+            for (int t = 0; t < k; ++t) {
+                const int j = nbr[(size_t)i * k + t];
+                adj[(size_t)cur[(size_t)i]++] = j;
+                adj[(size_t)cur[(size_t)j]++] = i;
+            }
+    }
+    std::vector<int> ulen((size_t)n);
+    for (int i = 0; i < n; ++i) {
+        auto b = adj.begin() + deg[(size_t)i], e = adj.begin() + deg[(size_t)i + 1];
+        std::sort(b, e);
+        ulen[(size_t)i] = (int)(std::unique(b, e) - b);
+    }
     CRS A;
     A.n = n;
     A.rowptr.assign((size_t)n + 1, 0);
-    for (auto& e : edges) A.rowptr[(size_t)e.first + 1]++;
-    for (int i = 0; i < n; ++i) A.rowptr[(size_t)i + 1] += A.rowptr[(size_t)i] + 1;  // + diagonal
+    for (int i = 0; i < n; ++i) A.rowptr[(size_t)i + 1] = A.rowptr[(size_t)i] + ulen[(size_t)i] + 1;  // + diagonal
     A.colind.resize((size_t)A.rowptr[(size_t)n]);
     A.val.resize((size_t)A.rowptr[(size_t)n]);
-    size_t e = 0;
     for (int i = 0; i < n; ++i) {
         int pos = A.rowptr[(size_t)i];
         double dsum = 0.0;
         int dslot = -1;
         bool placed = false;
-        while (e < edges.size() && edges[e].first == i) {
-            const int j = edges[e].second;
+        for (int t = 0; t < ulen[(size_t)i]; ++t) {
+            const int j = adj[(size_t)deg[(size_t)i] + t];
             if (!placed && j > i) { dslot = pos; A.colind[(size_t)pos++] = i; placed = true; }
             const double dx = px[(size_t)i] - px[(size_t)j], dy = py[(size_t)i] - py[(size_t)j];
             const double w = 1.0 / std::max(std::sqrt(dx * dx + dy * dy), 1e-12);
             A.colind[(size_t)pos] = j;
             A.val[(size_t)pos++] = -w;
             dsum += w;
-            ++e;
         }
         if (!placed) { dslot = pos; A.colind[(size_t)pos++] = i; }
         A.val[(size_t)dslot] = dsum + diag_shift;
