@@ -53,6 +53,7 @@ OPT_TILED = 0
 OPT_SWEEP = 1
 OPT_PDL = 2
 OPT_STAGE_KB = 3
+OPT_STAGE_BUFS = 4
 STATUS_NAMES = {0: "converged", 1: "breakdown", 2: "max_iter", 3: "nonfinite"}
 
 

@@ -17,7 +17,8 @@ candidates on the matrix itself.
   system by coordinate search: for each option in turn it keeps the value
   with the lowest median solve time, the others held at their best so far.
   The options are the sweep kernel (staged or per-slice), the staged
-  kernel's shared-memory budget, and programmatic dependent launch. With
+  kernel's buffers per CTA and shared-memory budget, and programmatic
+  dependent launch. With
   FP64 storage every choice gives the same bits. With FP32 storage the
   staged and per-slice sweeps round differently (reciprocal pivots against
   divisions), so the tuned result can differ in the last bits from an
@@ -35,7 +36,8 @@ from typing import Callable, Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
 
-from . import (CRS, MODE_FUSED, OPT_PDL, OPT_STAGE_KB, OPT_SWEEP, PRECOND_IC0, STORE_FP32, Context)
+from . import (CRS, MODE_FUSED, OPT_PDL, OPT_STAGE_BUFS, OPT_STAGE_KB, OPT_SWEEP, PRECOND_IC0, STORE_FP32,
+               Context)
 from .problems import Problem, make
 
 # (variant, block size) candidates: multicolor and ABMC with 8, 16, 32 rows per block
@@ -44,10 +46,11 @@ ORDERINGS: Tuple[Tuple[str, int], ...] = (("piccg", 0), ("abmc", 8), ("abmc", 16
 # option -> candidate values, in the order they are tried (the first is the default)
 KERNEL_OPTIONS: Tuple[Tuple[int, Tuple[int, ...]], ...] = (
     (OPT_SWEEP, (0, 1)),
+    (OPT_STAGE_BUFS, (1, 2)),
     (OPT_STAGE_KB, (0, 160, 112, 80)),
     (OPT_PDL, (1, 0)),
 )
-OPTION_NAMES = {OPT_SWEEP: "sweep", OPT_STAGE_KB: "stage_kb", OPT_PDL: "pdl"}
+OPTION_NAMES = {OPT_SWEEP: "sweep", OPT_STAGE_BUFS: "stage_bufs", OPT_STAGE_KB: "stage_kb", OPT_PDL: "pdl"}
 
 
 @dataclass

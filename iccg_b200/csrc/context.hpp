@@ -126,6 +126,7 @@ struct QSys {
     // step, in full groups of at most 16 steps: the chain-only kernel
     std::vector<int> chainS, chainT;
     std::vector<int> st_fgrid[2], st_bgrid[2];
+    std::vector<int> st1_fgrid[2], st1_bgrid[2];          // the same with one stage buffer
     std::vector<int> ch_grid[2];                          // chain-only kernel grids per level
     Buf<float> r32;                                       // FP32 reciprocal pivots
     bool r32_ok = false;
@@ -174,6 +175,8 @@ struct QSys {
             st_fgrid[k].clear();
             st_bgrid[k].clear();
             ch_grid[k].clear();
+            st1_fgrid[k].clear();
+            st1_bgrid[k].clear();
         }
         r32.free();
         r32_ok = false;
@@ -213,6 +216,7 @@ struct iccg_ctx {
     int sweep_kernel = 0;   // ICCG_OPT_SWEEP: 0 staged where it fits, 1 two-phase per-slice kernel
     bool pdl = true;        // ICCG_OPT_PDL: programmatic dependent launch
     int stage_kb = 0;       // ICCG_OPT_STAGE_KB: staged-sweep buffer budget (0: the opt-in maximum)
+    int stage_bufs = 1;     // ICCG_OPT_STAGE_BUFS: staged-sweep buffers per CTA (2: double-buffered)
     int smem_optin = 0;     // largest dynamic shared memory per CTA
     iccg::QSys Q;
     // preconditioner

@@ -129,6 +129,9 @@ int iccg_ctx_set_option(iccg_ctx* c, int option, long long value)
             c->sweep_kernel = (int)value;
         } else if (option == ICCG_OPT_PDL) {
             c->pdl = value != 0;
+        } else if (option == ICCG_OPT_STAGE_BUFS) {
+            if (value != 1 && value != 2) throw Error(ICCG_ERR_ARG, "ICCG_OPT_STAGE_BUFS takes 1 or 2");
+            c->stage_bufs = (int)value;
         } else if (option == ICCG_OPT_STAGE_KB) {
             if (value < 0 || value > 1024) throw Error(ICCG_ERR_ARG, "ICCG_OPT_STAGE_KB takes 0 to 1024");
             c->stage_kb = (int)value;

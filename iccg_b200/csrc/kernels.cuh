@@ -911,9 +911,11 @@ __global__ void __launch_bounds__(256) k_sweep_q2(int g0, int g1, int gpc, int t
 // so everything the batch reads except the earlier-level values is a handful
 // of contiguous ranges: slice metadata, inputs, r (with a reduction), pivots,
 // row words, column indices and values.  A CTA takes batches b0 + blockIdx.x,
-// + gridDim.x, ... and copies batch i + 1 into the other half of a double
-// buffer with cp.async (16-byte chunks, nothing held in registers) while it
-// works on batch i:
+// + gridDim.x, ... and copies them into shared memory with cp.async (16-byte
+// chunks, nothing held in registers).  With NB = 1 (the default) it has one
+// buffer, refilled after each batch, so twice as many CTAs fit an SM and
+// overlap each other's copies; with NB = 2 it copies batch i + 1 into the
+// other half of a double buffer while it works on batch i.  Per batch:
 //  G, all warps, one slice per warp and UG slices at a time: the
 //    earlier-level values of each row's entries are gathered (the only
 //    scattered reads) and folded into the row's partial sum in the tile, or,
@@ -1019,7 +1021,7 @@ __device__ __forceinline__ void stage_batch(unsigned char* base, const StageLayo
     cp_async_commit();
 }
 
-template <class T, bool FWD, int FIN, bool EXACT>
+template <class T, bool FWD, int FIN, bool EXACT, int NB = 2>
 __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDesc* __restrict__ bd, int rows_cap,
                                                   int slots_cap, int slices_cap, const int* __restrict__ sl0,
                                                   const int* __restrict__ glen, const SliceMeta* __restrict__ meta,
@@ -1048,8 +1050,11 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
         BatchDesc nxt = cur;
         if (has_next) nxt = bd[b + gridDim.x];
         for (int i = 0;; ++i) {
-            unsigned char* base = smem_st + (i & 1) * Ly.bytes;
-            if (has_next) stage_batch<T, FWD, with_r>(smem_st + ((i + 1) & 1) * Ly.bytes, Ly, nxt, meta, M, dg, in, rdot);
+            // NB = 2: batch i + 1 is copied into the other half while batch i
+            // is worked on; NB = 1: one buffer, refilled after each batch
+            unsigned char* base = smem_st + (NB == 2 ? (i & 1) * Ly.bytes : 0);
+            if (NB == 2 && has_next)
+                stage_batch<T, FWD, with_r>(smem_st + ((i + 1) & 1) * Ly.bytes, Ly, nxt, meta, M, dg, in, rdot);
             const bool has_nn = has_next && b + 2 * (int)gridDim.x < b1;
             BatchDesc nn = nxt;
             if (has_nn) nn = bd[b + 2 * gridDim.x];
@@ -1063,7 +1068,7 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
                     gs[k] = sl0[cur.gb + gi];
                 }
             }
-            if (has_next) cp_async_wait<1>();
+            if (NB == 2 && has_next) cp_async_wait<1>();
             else cp_async_wait<0>();
             __syncthreads();
 
@@ -1375,6 +1380,7 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
             }
             __syncthreads();
             if (!has_next) break;
+            if (NB == 1) stage_batch<T, FWD, with_r>(smem_st, Ly, nxt, meta, M, dg, in, rdot);
             b += gridDim.x;
             cur = nxt;
             nxt = nn;

@@ -261,11 +261,17 @@ static bool plan_staged_type(iccg_ctx* c, int k)
     constexpr bool exact = !std::is_same<T, float>::value;
     auto kf = k_sweep_st<T, true, FIN_NONE, exact>;
     auto kb = k_sweep_st<T, false, FIN_RZ, exact>;
+    auto kf1 = k_sweep_st<T, true, FIN_NONE, exact, 1>;
+    auto kb1 = k_sweep_st<T, false, FIN_RZ, exact, 1>;
     allow_smem(c, kf);
     allow_smem(c, kb);
+    allow_smem(c, kf1);
+    allow_smem(c, kb1);
     const int L = Q.nlevels;
     Q.st_fgrid[k].assign((size_t)L, 1);
     Q.st_bgrid[k].assign((size_t)L, 1);
+    Q.st1_fgrid[k].assign((size_t)L, 1);
+    Q.st1_bgrid[k].assign((size_t)L, 1);
     // the kernel's static shared memory (reduction scratch) comes on top
     const size_t lim = (size_t)std::max(0, c->smem_optin - 2048);
     for (int l = 0; l < L; ++l) {
@@ -274,18 +280,22 @@ static bool plan_staged_type(iccg_ctx* c, int k)
         const size_t fs = 2 * (size_t)stage_layout(Q.st_rows[(size_t)l], Q.st_slotsS[(size_t)l],
                                                    Q.st_slices[(size_t)l], (int)sizeof(T), false, false).bytes;
         if (fs > lim) return false;
-        int pf = 0;
+        int pf = 0, pf1 = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf, kf, kThreads, fs));
-        if (pf < 1) return false;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf1, kf1, kThreads, fs / 2));
+        if (pf < 1 || pf1 < 1) return false;
         Q.st_fgrid[k][(size_t)l] = std::max(1, std::min(nb, pf * c->nsm));
+        Q.st1_fgrid[k][(size_t)l] = std::max(1, std::min(nb, pf1 * c->nsm));
         if (!exact) {
             const size_t bs = 2 * (size_t)stage_layout(Q.st_rows[(size_t)l], Q.st_slotsT[(size_t)l],
                                                        Q.st_slices[(size_t)l], (int)sizeof(T), true, false).bytes;
             if (bs > lim) return false;
-            int pb = 0;
+            int pb = 0, pb1 = 0;
             CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pb, kb, kThreads, bs));
-            if (pb < 1) return false;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pb1, kb1, kThreads, bs / 2));
+            if (pb < 1 || pb1 < 1) return false;
             Q.st_bgrid[k][(size_t)l] = std::max(1, std::min(nb, pb * c->nsm));
+            Q.st1_bgrid[k][(size_t)l] = std::max(1, std::min(nb, pb1 * c->nsm));
         }
     }
     // chain-only levels: one warp per group
@@ -299,7 +309,7 @@ static bool plan_staged_type(iccg_ctx* c, int k)
     // reduction slots of a backward sweep, whichever kernels its levels use
     long long s = 0;
     for (int l = 0; l < L; ++l)
-        s += std::max({Q.st_bgrid[k][(size_t)l], Q.ch_grid[k][(size_t)l],
+        s += std::max({Q.st_bgrid[k][(size_t)l], Q.st1_bgrid[k][(size_t)l], Q.ch_grid[k][(size_t)l],
                        Q.two_phase ? Q.g2grid[(size_t)l] : 0, Q.fgrid.empty() ? 0 : Q.fgrid[(size_t)l]});
     ensure_partials(c, (size_t)std::max<long long>(s, 1));
     return true;

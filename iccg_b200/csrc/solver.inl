@@ -68,7 +68,10 @@ static SweepLevel sweep_level(iccg_ctx* c, int l, bool fwd)
     const size_t l_ = (size_t)l;
     const bool st_ok = Q.staged && c->sweep_kernel == 0 && (!f32 || Q.r32_ok);
     if (st_ok && (fwd ? Q.chainS[l_] : Q.chainT[l_])) return {0, Q.ch_grid[k][l_]};
-    if (st_ok && Q.st_fit[l_] && (fwd || f32)) return {1, fwd ? Q.st_fgrid[k][l_] : Q.st_bgrid[k][l_]};
+    if (st_ok && Q.st_fit[l_] && (fwd || f32)) {
+        if (c->stage_bufs == 1) return {1, fwd ? Q.st1_fgrid[k][l_] : Q.st1_bgrid[k][l_]};
+        return {1, fwd ? Q.st_fgrid[k][l_] : Q.st_bgrid[k][l_]};
+    }
     if (Q.two_phase) return {2, Q.g2grid[l_]};
     return {3, Q.fgrid[l_]};
 }
@@ -111,14 +114,15 @@ static void launch_sweep_level(iccg_ctx* c, int l, const SweepLevel& sl, const d
         break;
     case 1: {
         const int slots = FWD ? Q.st_slotsS[l_] : Q.st_slotsT[l_];
-        const size_t smem = 2 * (size_t)stage_layout(Q.st_rows[l_], slots, Q.st_slices[l_], (int)sizeof(T),
-                                                     FIN != FIN_NONE, !FWD && exact)
-                                    .bytes;
-        allow_smem(c, k_sweep_st<T, FWD, FIN, exact>);
-        launch_smem(c, cls, k_sweep_st<T, FWD, FIN, exact>, sl.grid, kThreads, smem, Q.lb[l_], Q.lb[l_ + 1],
-                    (const BatchDesc*)Q.bdesc.get(), Q.st_rows[l_], slots, Q.st_slices[l_], (const int*)Q.sl0.get(),
-                    (const int*)Q.glen.get(), (const SliceMeta*)Q.meta.get(), M, dg, in, out, rdot, slot0, nslots,
-                    st, red, c->ticket.get());
+        const int nbuf = c->stage_bufs == 1 ? 1 : 2;
+        const size_t smem = nbuf * (size_t)stage_layout(Q.st_rows[l_], slots, Q.st_slices[l_], (int)sizeof(T),
+                                                        FIN != FIN_NONE, !FWD && exact)
+                                       .bytes;
+        auto kern = nbuf == 1 ? k_sweep_st<T, FWD, FIN, exact, 1> : k_sweep_st<T, FWD, FIN, exact, 2>;
+        allow_smem(c, kern);
+        launch_smem(c, cls, kern, sl.grid, kThreads, smem, Q.lb[l_], Q.lb[l_ + 1], (const BatchDesc*)Q.bdesc.get(),
+                    Q.st_rows[l_], slots, Q.st_slices[l_], (const int*)Q.sl0.get(), (const int*)Q.glen.get(),
+                    (const SliceMeta*)Q.meta.get(), M, dg, in, out, rdot, slot0, nslots, st, red, c->ticket.get());
         break;
     }
     case 2:

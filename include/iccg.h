@@ -204,11 +204,17 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
    more resident CTAs per SM.  A level with a group of units that alone
    exceeds it runs on the per-slice kernel.  Setting it re-plans the
    batches of a built preconditioner.
+   ICCG_OPT_STAGE_BUFS (default 1): stage buffers per CTA of the staged
+   kernel; 1 refills a CTA's one buffer after each batch, 2 copies the next
+   batch into a second buffer while the current one is worked on.  One
+   buffer halves a CTA's shared memory, so twice as many CTAs share an SM
+   and overlap each other's copies; on the 128^3 system that was faster.
    Every choice gives the same bits with FP64 storage. */
 #define ICCG_OPT_TILED 0
 #define ICCG_OPT_SWEEP 1
 #define ICCG_OPT_PDL 2
 #define ICCG_OPT_STAGE_KB 3
+#define ICCG_OPT_STAGE_BUFS 4
 int iccg_ctx_set_option(iccg_ctx* ctx, int option, long long value);
 
 /* Uploads A_run (the matrix conjugate_gradient runs on, cg_crs.cpp:442-447):

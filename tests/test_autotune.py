@@ -61,10 +61,10 @@ def test_tune_kernels_coordinate_search_leaves_best_options_set():
         return ms, 50, True
 
     res = at.tune_kernels(ctx, np.zeros(4), timer=timer)
-    assert ctx.opts == {ib.OPT_SWEEP: 1, ib.OPT_STAGE_KB: 112, ib.OPT_PDL: 1}
+    assert ctx.opts == {ib.OPT_SWEEP: 1, ib.OPT_STAGE_BUFS: 1, ib.OPT_STAGE_KB: 112, ib.OPT_PDL: 1}
     assert res.choice["sweep"] == 1 and res.choice["stage_kb"] == 112 and res.choice["pdl"] == 1
     assert abs(res.choice["ms"] - (10.0 - 1.0 - 0.5 - 0.4)) < 1e-12
-    assert len(res.trials) == 2 + 4 + 2
+    assert len(res.trials) == 2 + 2 + 4 + 2
 
 
 def test_tune_kernels_skips_unconverged_settings():

@@ -507,3 +507,34 @@ def test_gpu_sweep_plan_reports_kernels():
     assert all(k == "csr" for k, _ in ctx.sweep_plan(ib.STORE_FP64, True))
     ctx.use_tiled(True)
     ctx.close()
+
+
+@pytest.mark.parametrize("which", ["abmc_lin32", "d27_mc", "d27_abmc8"])
+def test_gpu_single_buffered_staging_gives_the_same_bits(which):
+    """The staged kernel with one shared-memory buffer per CTA, refilled after
+    each batch (ICCG_OPT_STAGE_BUFS 1, the default), and with two (the next
+    batch copied while the current one is worked on): only when a batch's
+    copy is issued changes, so applies and solves are identical in both
+    storages."""
+    P = {"abmc_lin32": lambda: pb.config_abmc_aniso(32, 16, "linear"),
+         "d27_mc": lambda: pb.config_diffusion27(24, "piccg"),
+         "d27_abmc8": lambda: pb.config_diffusion27(24, "abmc", 8)}[which]()
+    ctx = _ctx_for(P.A_run, P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    r = ib.gen_uniform(P.A_run.n, 43)
+    out = {}
+    for bufs in (2, 1):
+        ctx.set_option(ib.OPT_STAGE_BUFS, bufs)
+        res = []
+        for st in (ib.STORE_FP64, ib.STORE_FP32):
+            x = np.zeros(P.A_run.n)
+            rr = ctx.solve(P.b_run, x, 10000, 1e-8, storage=st)
+            res.append((ctx.apply(r, st), x, rr.iters))
+        out[bufs] = res
+    ctx.set_option(ib.OPT_STAGE_BUFS, 1)
+    assert any(k == "staged" for k, _ in ctx.sweep_plan(ib.STORE_FP32, True))
+    for a, b in zip(out[2], out[1]):
+        assert np.array_equal(a[0], b[0])
+        assert np.array_equal(a[1], b[1])
+        assert a[2] == b[2]
+    ctx.close()
