@@ -627,6 +627,7 @@ def run_diffusion27(args):
                 for k, _ in ctx.sweep_plan(storage, d == "fwd"):
                     kinds[k] = kinds.get(k, 0) + 1
                 row["sweep_kernels"][f"{st_name}_{d}"] = kinds
+        x64 = None
         for st_name, storage in (("fp64", ib.STORE_FP64), ("mixed", ib.STORE_FP32)):
             res = []
             for i in range(args.warmup + args.steps):
@@ -642,6 +643,11 @@ def run_diffusion27(args):
             row[st_name] = {"ms": round(ms, 3), "iters": last.iters, "converged": last.converged,
                             "true_rel_resid": last.true_rel_resid, "iteration_GBps": round(gbs, 1),
                             "frac": round(gbs / peak, 4)}
+            xs = x_d.cpu().numpy().copy()
+            if storage == ib.STORE_FP64:
+                x64 = xs
+            else:
+                row[st_name]["err_vs_fp64_solution"] = float(np.linalg.norm(xs - x64) / np.linalg.norm(x64))
         if label == "abmc16" and not args.no_cpu_baseline:
             from oracle import bindings as ob
             if ob.ref() is not None:
@@ -705,6 +711,7 @@ def run_poisson2d(args):
     ctx.set_schedule(P.sched)
     ctx.build(ib.PRECOND_IC0, 0.0)
     out = {}
+    x64 = None
     for name, storage, mode in (("fp64_fused", ib.STORE_FP64, ib.MODE_FUSED),
                                 ("fp64_plain", ib.STORE_FP64, ib.MODE_PLAIN),
                                 ("mixed_fused", ib.STORE_FP32, ib.MODE_FUSED)):
@@ -719,6 +726,10 @@ def run_poisson2d(args):
         out[name] = {"ms": round(statistics.mean(r.solve_ms for r in res), 4), "iters": res[-1].iters,
                      "true_rel_resid": res[-1].true_rel_resid,
                      "e2e_ms": round(statistics.mean(wall), 4)}
+        if x64 is None:
+            x64 = x.copy()
+        else:
+            out[name]["err_vs_fp64_solution"] = float(np.linalg.norm(x - x64) / np.linalg.norm(x64))
     ctx.close()
     cpu = None
     if not args.no_cpu_baseline:
