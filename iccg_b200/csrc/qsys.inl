@@ -316,10 +316,10 @@ static bool plan_staged_type(iccg_ctx* c, int k)
 }
 
 // Batches of the staged sweeps: consecutive groups of one level, at most 16
-// groups and 512 rows, and as many groups as keep the double-buffered stage
-// of every buffer the staged kernel runs with (FP64 and FP32 forward, FP32
-// backward) within the budget (ICCG_OPT_STAGE_KB, default the opt-in shared
-// memory).  A level with a group that alone exceeds the budget runs on the
+// groups and 512 rows, and as many groups as keep two stage buffers of every
+// type the staged kernel runs with (FP64 and FP32 forward, FP32 backward)
+// within the budget (ICCG_OPT_STAGE_KB, default the opt-in shared memory);
+// the default single buffer per CTA then takes half of it.  A level with a group that alone exceeds the budget runs on the
 // per-slice kernel.
 static void plan_staged(iccg_ctx* c)
 {

@@ -191,16 +191,17 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
    internal row order with 32 independent units per warp, SELL-32 storage);
    0 forces the CSR kernels (one thread per row / per unit).
    ICCG_OPT_SWEEP (default 0), lane-interleaved substitutions: 0 uses the
-   staged kernel (double-buffered shared-memory batches) where a batch fits
-   shared memory, 1 forces the per-slice two-phase kernel.
+   staged kernel (batches of rows copied into shared memory) where a batch
+   fits shared memory, 1 forces the per-slice two-phase kernel.
    ICCG_OPT_PDL (default 1): 1 launches kernels with programmatic dependent
    launch: the per-iteration kernels let the next launch start once their
    main loop is done, so it is placed while their tail (the reduction) runs;
    every kernel still waits for its predecessor's results.  0 launches each
    kernel after its predecessor has finished.
-   ICCG_OPT_STAGE_KB (default 0): shared memory, in KB, that a batch of the
-   staged kernel may fill with both halves of its double buffer; 0 takes
-   the device's opt-in maximum per block.  Smaller batches leave room for
+   ICCG_OPT_STAGE_KB (default 0): shared memory, in KB, that two stage
+   buffers of the staged kernel may fill (batches are sized for two, so they
+   also fit the default single buffer); 0 takes the device's opt-in maximum
+   per block.  Smaller batches leave room for
    more resident CTAs per SM.  A level with a group of units that alone
    exceeds it runs on the per-slice kernel.  Setting it re-plans the
    batches of a built preconditioner.
