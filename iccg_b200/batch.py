@@ -1,6 +1,6 @@
 """Many independent solves on one GPU: batched systems and a serving loop.
 
-Every system gets its own context: one CUDA stream with the system's matrix,
+A system lives in a context: one CUDA stream with the system's matrix,
 schedule, IC(0) factor and work vectors resident in device memory, and the
 captured graphs of its CG iterations. Host threads drive several contexts
 at once, one context per thread at a time. Their kernels run concurrently
@@ -8,12 +8,14 @@ on the GPU, which is how small systems, too small to fill 148 SMs alone,
 share the device. A solve's arithmetic does not depend on what else runs,
 so each result is the same bits alone and in the mix.
 
-* ``solve_batch`` solves a fixed set of systems, each with several
-  right-hand sides. It returns the results plus per-solve timings.
+* ``solve_batch`` solves a fixed set of resident systems, each with several
+  right-hand sides, one context per system. It returns the results plus
+  per-solve timings.
 * ``ServingLoop`` takes requests as they arrive. It admits them while the
-  device memory held by admitted solves stays under a budget, solves them on
-  worker threads, and releases each system when its solve is done. It
-  reports p50 / p99 latency (arrival to completion) and solves/s.
+  device memory of admitted solves stays under a budget, and solves them on
+  worker threads, each worker loading request after request into its own
+  context. It reports p50 / p99 latency (arrival to completion) and
+  solves/s.
 """
 from __future__ import annotations
 
@@ -160,6 +162,7 @@ class ServingLoop:
 
         free_ctx: List[Context] = []
         all_ctx: List[Context] = []
+        held_by: dict = {}  # id(pooled context) -> its device bytes, recorded by the worker using it
 
         def serve(req: Request):
             ctx = None
@@ -167,18 +170,21 @@ class ServingLoop:
                 P = req.build()
                 if self.pool:
                     with lock:
-                        if free_ctx:
-                            ctx = free_ctx.pop()
-                        else:
-                            ctx = Context(self.device)
+                        ctx = free_ctx.pop() if free_ctx else None
+                    if ctx is None:
+                        # a new worker context, created outside the lock
+                        ctx = Context(self.device)
+                        with lock:
                             all_ctx.append(ctx)
                 sysm = ResidentSystem(P, self.device, self.storage, ctx=ctx)
                 try:
+                    mine = sysm.device_bytes  # read by the thread that uses the context
                     with lock:
                         if self.pool:
-                            held = sum(c.device_bytes for c in all_ctx)
+                            held_by[id(ctx)] = mine
+                            held = sum(held_by.values())
                         else:
-                            held = in_use[0] - req.est_bytes + sysm.device_bytes
+                            held = in_use[0] - req.est_bytes + mine
                         stats.peak_bytes = max(stats.peak_bytes, held)
                     _, res, _ = sysm.solve(P.b_run, self.tol)
                 finally:
