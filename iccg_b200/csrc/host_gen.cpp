@@ -163,7 +163,9 @@ CRS gen_knn_laplacian(int npts, int k, double diag_shift, uint64_t seed)
     std::vector<double> px((size_t)n), py((size_t)n);
     uint64_t s = seed;
     for (int i = 0; i < n; ++i) { px[(size_t)i] = u01(s); py[(size_t)i] = u01(s); }
-    const int G = std::max(1, (int)std::sqrt((double)n / 2.0));
+    // about 4 points per grid cell (the search is exact for any cell size:
+    // it widens by rings until no point outside can be nearer than the k-th)
+    const int G = std::max(1, (int)std::sqrt((double)n / 4.0));
     std::vector<int> cell_ptr((size_t)G * G + 1, 0), cell_pts((size_t)n);
     auto cell_of = [&](double v) { int c = (int)(v * G); return c >= G ? G - 1 : c; };
     for (int i = 0; i < n; ++i) cell_ptr[(size_t)cell_of(px[(size_t)i]) + (size_t)G * cell_of(py[(size_t)i]) + 1]++;
