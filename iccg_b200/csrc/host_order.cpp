@@ -4,6 +4,7 @@
 // reference's results bit for bit; each function cites the reference
 // routine whose output it must equal.
 #include <algorithm>
+#include <charconv>
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
@@ -71,6 +72,19 @@ bool parse_ll(const char*& p, const char* e, long long& v)
 {
     while (p < e && is_ws(*p)) ++p;
     if (p >= e) return false;
+    {
+        // plain decimal digits of up to 18 places end at whitespace or the
+        // line's end: read directly (strtoll gives the same value); anything
+        // else goes through strtoll below
+        const char* q = p;
+        long long x = 0;
+        while (q < e && q - p < 18 && *q >= '0' && *q <= '9') x = x * 10 + (*q++ - '0');
+        if (q > p && (q == e || is_ws(*q))) {
+            v = x;
+            p = q;
+            return true;
+        }
+    }
     char buf[64];
     size_t len = 0;
     while (p + len < e && !is_ws(p[len]) && len < 63) { buf[len] = p[len]; ++len; }
@@ -87,6 +101,18 @@ bool parse_double(const char*& p, const char* e, double& v)
 {
     while (p < e && is_ws(*p)) ++p;
     if (p >= e) return false;
+    {
+        // decimal forms: std::from_chars, correctly rounded like strtod, so
+        // the same double; a token it does not take whole (a leading '+',
+        // hexadecimal, inf / nan) goes through strtod below
+        double x;
+        const auto r = std::from_chars(p, e, x);
+        if (r.ec == std::errc() && (r.ptr == e || is_ws(*r.ptr))) {
+            v = x;
+            p = r.ptr;
+            return true;
+        }
+    }
     char buf[128];
     size_t len = 0;
     while (p + len < e && !is_ws(p[len]) && len < 127) { buf[len] = p[len]; ++len; }
@@ -187,7 +213,17 @@ CRS read_matrix_market_crs(const std::string& path)
     for (int r = 0; r < nrows; ++r) {
         int* s = ord.data() + cnt[(size_t)r];
         int* t = ord.data() + cnt[(size_t)r + 1];
-        std::stable_sort(s, t, [&](int a, int c) { return J[(size_t)a] < J[(size_t)c]; });
+        if (t - s <= 32) {
+            // short rows: stable insertion sort by column
+            for (int* a = s + 1; a < t; ++a) {
+                const int x = *a, cx = J[(size_t)x];
+                int* b = a;
+                while (b > s && J[(size_t)b[-1]] > cx) { *b = b[-1]; --b; }
+                *b = x;
+            }
+        } else {
+            std::stable_sort(s, t, [&](int a, int c) { return J[(size_t)a] < J[(size_t)c]; });
+        }
         for (int* q = s; q < t;) {
             int c = J[(size_t)*q];
             double acc = 0.0;
@@ -211,10 +247,33 @@ void write_matrix_market(const std::string& path, const CRS& A, bool symmetric_l
     std::fprintf(f, "%%%%MatrixMarket matrix coordinate real %s\n",
                  symmetric_lower ? "symmetric" : "general");
     std::fprintf(f, "%d %d %lld\n", A.n, A.n, cnt);
-    for (int i = 0; i < A.n; ++i)
+    // entry lines "i j v" with v as %.17g (std::to_chars with general format
+    // and precision 17 prints exactly what printf does), formatted into one
+    // buffer per chunk of rows and written with one call
+    std::string out;
+    out.reserve((size_t)std::min<long long>(cnt, 1 << 20) * 40 + 64);
+    char num[64];
+    auto put = [&]() {
+        if (!out.empty() && std::fwrite(out.data(), 1, out.size(), f) != out.size()) {
+            std::fclose(f);
+            throw Error(ICCG_ERR_IO, "cannot write " + path);
+        }
+        out.clear();
+    };
+    for (int i = 0; i < A.n; ++i) {
         for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k)
-            if (!symmetric_lower || A.colind[k] <= i)
-                std::fprintf(f, "%d %d %.17g\n", i + 1, A.colind[k] + 1, A.val[k]);
+            if (!symmetric_lower || A.colind[k] <= i) {
+                char* q = std::to_chars(num, num + sizeof num, i + 1).ptr;
+                *q++ = ' ';
+                q = std::to_chars(q, num + sizeof num, A.colind[k] + 1).ptr;
+                *q++ = ' ';
+                q = std::to_chars(q, num + sizeof num, A.val[k], std::chars_format::general, 17).ptr;
+                *q++ = '\n';
+                out.append(num, q);
+            }
+        if (out.size() > (32u << 20)) put();
+    }
+    put();
     std::fclose(f);
 }
 

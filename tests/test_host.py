@@ -165,6 +165,44 @@ def test_matrix_market_formats(tmp_path):
     assert list(v) == [4.0, 1.0]
 
 
+def test_matrix_market_values_parse_exactly(tmp_path):
+    """Entry values and indices read from MatrixMarket text are the doubles
+    and integers strtod / strtoll give (correctly rounded): subnormals, the
+    extremes, long mantissas, halfway cases, and the forms only strtod takes
+    (a leading '+', hexadecimal, inf / nan, trailing characters after the
+    number)."""
+    rng = np.random.default_rng(11)
+    decimal = ["0.1", "1e-310", "4.9e-324", "2.2250738585072011e-308", "1.7976931348623157e308",
+               "0.1000000000000000055511151231257827021181583404541015625",
+               "123456789012345678901234567890", "-0.0", "5.", ".5", "1E5", "-2.5e-3",
+               "9007199254740993", "1.00000000000000011102230246251565404236316680908203125"]
+    decimal += ["%.17g" % v for v in rng.standard_normal(40) * 10.0 ** rng.integers(-30, 30, 40)]
+    other = {"+1.5": 1.5, "1.5abc": 1.5, "0x1p3": 8.0, "inf": float("inf"), "-INF": float("-inf")}
+    toks = decimal + list(other)
+    lines = "".join(f"1 {k + 1} {t}\n" for k, t in enumerate(toks))
+    p = tmp_path / "v.mtx"
+    p.write_text(f"%%MatrixMarket matrix coordinate real general\n1 {len(toks)} {len(toks)}\n" + lines)
+    A = ib.read_matrix_market_crs(str(p))
+    assert list(A.colind) == list(range(len(toks)))
+    # entries are summed from 0.0 (duplicates add up, as in the reference's
+    # coo_to_crs), so -0.0 reads as +0.0
+    want = [float(t) + 0.0 for t in decimal] + list(other.values())
+    for got, w, t in zip(A.val, want, toks):
+        assert np.float64(got).tobytes() == np.float64(w).tobytes(), (t, got, w)
+    # the decimal ones also as the oracle's restatement of the reference reader
+    q = tmp_path / "d.mtx"
+    q.write_text(f"%%MatrixMarket matrix coordinate real general\n1 {len(decimal)} {len(decimal)}\n"
+                 + "".join(f"1 {k + 1} {t}\n" for k, t in enumerate(decimal)))
+    B = ib.read_matrix_market_crs(str(q))
+    n, rp, ci, v = ob.read_mm(q)
+    assert np.array_equal(B.val.view(np.int64), np.asarray(v).view(np.int64))
+    # indices: leading zeros and a sign
+    r = tmp_path / "i.mtx"
+    r.write_text("%%MatrixMarket matrix coordinate real general\n3 3 2\n001 +2 1.0\n+3 0003 2.0\n")
+    C = ib.read_matrix_market_crs(str(r))
+    assert list(C.rowptr) == [0, 1, 1, 2] and list(C.colind) == [1, 2] and list(C.val) == [1.0, 2.0]
+
+
 @pytest.mark.parametrize("text,msg", [
     ("", "Empty file"),
     ("%%MatrixMarket matrix array real general\n1 1\n1\n", "coordinate"),
