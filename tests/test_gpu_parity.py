@@ -538,3 +538,53 @@ def test_gpu_single_buffered_staging_gives_the_same_bits(which):
         assert np.array_equal(a[1], b[1])
         assert a[2] == b[2]
     ctx.close()
+
+
+def _dense_crs(rows):
+    d = np.asarray(rows, dtype=float)
+    n = d.shape[0]
+    rp, ci, v = [0], [], []
+    for i in range(n):
+        for j in range(n):
+            if d[i, j] != 0.0:
+                ci.append(j)
+                v.append(d[i, j])
+        rp.append(len(ci))
+    return ib.CRS.from_arrays(n, np.array(rp, np.int32), np.array(ci, np.int32), np.array(v))
+
+
+@pytest.mark.parametrize("which", ["n1_mc", "n2_mc", "n2_abmc", "p2d_3_mc", "l3d_3_abmc16", "l3d_3_abmc4_lin",
+                                   "natural_33", "knn_40"])
+def test_gpu_tiny_and_ragged_systems_match_oracle(which):
+    """Systems far below one 32-row slice or with ragged units: a 1x1 and a
+    2x2 matrix, 9 and 27 rows (one partial slice; 16-row blocks of which the
+    last is cut short; 4-row linear blocks), 33 rows in natural order (one
+    full slice and one row) and a 40-point k-NN graph.  Factor, apply and
+    SpMV bit for bit, FP64 CG on both paths as the oracle's, and the mixed
+    form to the true residual."""
+    P = {"n1_mc": lambda: pb.make(_dense_crs([[4.0]]), "piccg", seed=1),
+         "n2_mc": lambda: pb.make(_dense_crs([[2.0, -1.0], [-1.0, 2.0]]), "piccg", seed=2),
+         "n2_abmc": lambda: pb.make(_dense_crs([[2.0, -1.0], [-1.0, 2.0]]), "abmc", block_size=16, seed=2),
+         "p2d_3_mc": lambda: pb.make(pb.poisson2d(3), "piccg", seed=3),
+         "l3d_3_abmc16": lambda: pb.make(pb.laplace3d_aniso(3), "abmc", block_size=16, seed=4),
+         "l3d_3_abmc4_lin": lambda: pb.make(pb.laplace3d_aniso(3), "abmc", block_size=4, blocking="linear", seed=5),
+         "natural_33": lambda: pb.make(ib.gen_stencil_2d5(33, 1), "iccg", seed=6),
+         "knn_40": lambda: pb.config_knn(40, seed=7, block_size=16)}[which]()
+    ic0, xo, ito, relo, cvo = _oracle_solve(P)
+    ctx = _ctx_for(P.A_run, P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    assert np.array_equal(ctx.export_factor()[2], ic0.export()[2])
+    r = ib.gen_uniform(P.A_run.n, 13)
+    assert np.array_equal(ctx.apply(r), ic0.apply(r, P.sched))
+    A = P.A_run
+    assert np.array_equal(ctx.spmv(r), ob.spmv(A.n, A.rowptr, A.colind, A.val, r))
+    for mode in (ib.MODE_PLAIN, ib.MODE_FUSED):
+        x = np.zeros(A.n)
+        res = ctx.solve(P.b_run, x, 10000, 1e-8, mode=mode)
+        assert res.converged and cvo
+        assert abs(res.iters - ito) <= 1, (res.iters, ito)
+        _assert_x_parity(x, xo, P)
+    x = np.zeros(A.n)
+    res = ctx.solve(P.b_run, x, 10000, 1e-8, storage=ib.STORE_FP32)
+    assert res.converged and res.true_rel_resid <= 1e-8
+    ctx.close()
