@@ -523,13 +523,28 @@ def run_serving(args):
     `--threads` solves overlap. Each arrival rate reports p50 / p99 latency
     (arrival to result, host set-up included) and solves/s. The comparison is
     the same requests one at a time on the plain FP64 path.
+
+    Under torchrun (one process per GPU) every rank serves its share of the
+    stream on its own GPU (iccg_b200.batch.serve_sharded), the arrival rates
+    scale with the number of GPUs, and rank 0 prints the summary over all
+    requests.
     """
+    import torch
     import iccg_b200 as ib
     import iccg_b200.batch as bt
     import iccg_b200.problems as pb
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    local = _env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900), device_id=torch.device("cuda", local))
     rng = np.random.default_rng(5)
     lo, hi = np.log(1e3), np.log(float(args.max_points))
-    sizes = [int(np.exp(rng.uniform(lo, hi))) for _ in range(args.requests)]
+    sizes = [int(np.exp(rng.uniform(lo, hi))) for _ in range(args.requests * world)]
 
     def make_requests(rate):
         t, reqs = 0.0, []
@@ -546,34 +561,43 @@ def run_serving(args):
     for i, npts in enumerate(sample):
         t0 = time.perf_counter()
         P = pb.config_knn(npts, seed=10_000 + i)
-        s = bt.ResidentSystem(P, storage=ib.STORE_FP32)
+        s = bt.ResidentSystem(P, device=local, storage=ib.STORE_FP32)
         s.solve(P.b_run)
         alone_ms.append((time.perf_counter() - t0) * 1e3)
         s.close()
-        s = bt.ResidentSystem(P, storage=ib.STORE_FP64)
+        s = bt.ResidentSystem(P, device=local, storage=ib.STORE_FP64)
         _, _, wms = s.solve(P.b_run, mode=ib.MODE_PLAIN)
         plain_ms.append(wms)
         s.close()
-    sat = args.threads * 1000.0 / statistics.mean(alone_ms)
+    sat = world * args.threads * 1000.0 / statistics.mean(alone_ms)
+    if dist is not None:
+        box = [sat]
+        dist.broadcast_object_list(box, src=0)   # every rank uses rank 0's arrival rates
+        sat = box[0]
     out = []
     for f in (0.25, 0.5, 1.0):
-        loop = bt.ServingLoop(budget_bytes=100 * 10**9, workers=args.threads)
-        st = loop.run(make_requests(f * sat)).summary()
+        loop = bt.ServingLoop(budget_bytes=100 * 10**9, workers=args.threads, device=local)
+        st = bt.serve_sharded(make_requests(f * sat), loop, dist=dist)
         st["arrival_rate_per_s"] = round(f * sat, 2)
         out.append(st)
     # the same top rate with a fresh context per request (no worker pool)
-    loop = bt.ServingLoop(budget_bytes=100 * 10**9, workers=args.threads, pool=False)
-    unpooled = loop.run(make_requests(sat)).summary()
+    loop = bt.ServingLoop(budget_bytes=100 * 10**9, workers=args.threads, device=local, pool=False)
+    unpooled = bt.serve_sharded(make_requests(sat), loop, dist=dist)
     unpooled["arrival_rate_per_s"] = round(sat, 2)
-    line = {"workload": "serving", "requests_per_rate": len(sizes), "points": {"min": min(sizes), "max": max(sizes)},
-            "threads": args.threads, "budget_bytes": 100 * 10**9, "rates": out,
+    line = {"workload": "serving", "n_gpus": world, "requests_per_rate": len(sizes),
+            "points": {"min": min(sizes), "max": max(sizes)},
+            "threads_per_gpu": args.threads, "budget_bytes_per_gpu": 100 * 10**9, "rates": out,
             "context_per_request_at_top_rate": unpooled,
             "one_at_a_time_ms": {"mixed_end_to_end_mean": round(statistics.mean(alone_ms), 3),
                                  "plain_fp64_solve_mean": round(statistics.mean(plain_ms), 3)},
             "plain_fp64_one_at_a_time_solves_per_s": round(1000.0 / statistics.mean(plain_ms), 2),
             "storage": "fp32 A and L, fp64 vectors", "preconditioner": "IC(0), ABMC B=16",
             "data": "synthetic", "latency": "arrival to result, host set-up (kNN graph, blocking, PtAP) included"}
-    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def run_diffusion27(args):

@@ -145,13 +145,18 @@ class ServingLoop:
     """
 
     def __init__(self, budget_bytes: int, workers: int = 8, device: int = 0, storage: int = STORE_FP32,
-                 tol: float = 1e-8, pool: bool = True):
+                 tol: float = 1e-8, pool: bool = True,
+                 make_system: Callable = None, make_context: Callable = None):
         self.budget = budget_bytes
         self.workers = workers
         self.device = device
         self.storage = storage
         self.tol = tol
         self.pool = pool
+        # system(P, device, storage, ctx) and context(device) factories:
+        # ResidentSystem and Context (tests substitute stand-ins)
+        self.make_system = make_system or ResidentSystem
+        self.make_context = make_context or Context
 
     def run(self, requests: Sequence[Request]) -> ServingStats:
         stats = ServingStats()
@@ -173,10 +178,10 @@ class ServingLoop:
                         ctx = free_ctx.pop() if free_ctx else None
                     if ctx is None:
                         # a new worker context, created outside the lock
-                        ctx = Context(self.device)
+                        ctx = self.make_context(self.device)
                         with lock:
                             all_ctx.append(ctx)
-                sysm = ResidentSystem(P, self.device, self.storage, ctx=ctx)
+                sysm = self.make_system(P, self.device, self.storage, ctx=ctx)
                 try:
                     mine = sysm.device_bytes  # read by the thread that uses the context
                     with lock:
@@ -227,6 +232,37 @@ class ServingLoop:
         for c in all_ctx:
             c.close()
         return stats
+
+
+def serve_sharded(requests: Sequence[Request], loop: "ServingLoop", dist=None) -> dict:
+    """The serving loop on several GPUs, one process per GPU: rank r serves
+    every world-th request in arrival order (its share of the stream, at the
+    original arrival times) with `loop` on its own device, and the ranks
+    exchange their results once at the end (no collective on the data path).
+    Returns the summary over all requests on every rank: solves, failures,
+    p50 / p99 latency over all of them, solves/s over the slowest rank's
+    elapsed time, and each rank's solves and peak device bytes."""
+    queue = sorted(requests, key=lambda r: r.arrival_s)
+    rank = dist.get_rank() if dist is not None else 0
+    world = dist.get_world_size() if dist is not None else 1
+    mine = queue[rank::world]
+    st = loop.run(mine)
+    part = {"latencies_ms": st.latencies_ms, "iters": st.iters, "failed": st.failed, "elapsed_s": st.elapsed_s,
+            "peak_bytes": st.peak_bytes}
+    parts = [part]
+    if dist is not None and world > 1:
+        parts = [None] * world
+        dist.all_gather_object(parts, part)
+    lat = [v for p in parts for v in p["latencies_ms"]]
+    iters = [v for p in parts for v in p["iters"]]
+    elapsed = max(p["elapsed_s"] for p in parts)
+    return {"ranks": world, "solves": len(lat), "failed": sum(p["failed"] for p in parts),
+            "elapsed_s": round(elapsed, 3),
+            "solves_per_s": round(len(lat) / elapsed, 3) if elapsed > 0 else 0.0,
+            "p50_ms": round(percentile(lat, 50), 3), "p99_ms": round(percentile(lat, 99), 3),
+            "mean_iters": round(statistics.mean(iters), 1) if iters else 0.0,
+            "solves_per_rank": [len(p["latencies_ms"]) for p in parts],
+            "peak_device_bytes_per_rank": [p["peak_bytes"] for p in parts]}
 
 
 def estimate_device_bytes(n: int, nnz: int) -> int:
