@@ -252,7 +252,8 @@ void write_matrix_market(const std::string& path, const CRS& A, bool symmetric_l
     // buffer per chunk of rows and written with one call
     std::string out;
     out.reserve((size_t)std::min<long long>(cnt, 1 << 20) * 40 + 64);
-    char num[64];
+    char num[96];  // one line needs at most 11 + 1 + 11 + 1 + 24 + 1 bytes
+    char* const num_end = num + sizeof num;
     auto put = [&]() {
         if (!out.empty() && std::fwrite(out.data(), 1, out.size(), f) != out.size()) {
             std::fclose(f);
@@ -263,11 +264,12 @@ void write_matrix_market(const std::string& path, const CRS& A, bool symmetric_l
     for (int i = 0; i < A.n; ++i) {
         for (int k = A.rowptr[i]; k < A.rowptr[i + 1]; ++k)
             if (!symmetric_lower || A.colind[k] <= i) {
-                char* q = std::to_chars(num, num + sizeof num, i + 1).ptr;
+                // each conversion leaves room for the separator after it
+                char* q = std::to_chars(num, num_end - 1, i + 1).ptr;
                 *q++ = ' ';
-                q = std::to_chars(q, num + sizeof num, A.colind[k] + 1).ptr;
+                q = std::to_chars(q, num_end - 1, A.colind[k] + 1).ptr;
                 *q++ = ' ';
-                q = std::to_chars(q, num + sizeof num, A.val[k], std::chars_format::general, 17).ptr;
+                q = std::to_chars(q, num_end - 1, A.val[k], std::chars_format::general, 17).ptr;
                 *q++ = '\n';
                 out.append(num, q);
             }
