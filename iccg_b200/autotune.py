@@ -8,7 +8,7 @@ chains per color but more colors and iterations. So the tuner times the
 candidates on the matrix itself.
 
 * ``tune_ordering(A, ...)`` builds every candidate ordering (multicolor,
-  ABMC with each block size) with this package's generators. It times one
+  ABMC with each block size and blocking) with this package's generators. It times one
   full solve of each on the device, after a warm-up solve, and returns the
   fastest ``Problem`` with the table of timings. Candidates differ in
   iteration count as well as in speed per iteration; the tuner compares
@@ -40,8 +40,12 @@ from . import (CRS, MODE_FUSED, OPT_PDL, OPT_STAGE_BUFS, OPT_STAGE_KB, OPT_SWEEP
                Context)
 from .problems import Problem, make
 
-# (variant, block size) candidates: multicolor and ABMC with 8, 16, 32 rows per block
-ORDERINGS: Tuple[Tuple[str, int], ...] = (("piccg", 0), ("abmc", 8), ("abmc", 16), ("abmc", 32))
+# (variant, block size, blocking) candidates: multicolor, and ABMC with 8, 16,
+# 32 rows per block grown by breadth-first search, or 16 and 32 consecutive
+# rows (linear blocking: on structured grids it can need far fewer colors)
+ORDERINGS: Tuple[Tuple[str, int, str], ...] = (("piccg", 0, "bfs"), ("abmc", 8, "bfs"), ("abmc", 16, "bfs"),
+                                               ("abmc", 32, "bfs"), ("abmc", 16, "linear"),
+                                               ("abmc", 32, "linear"))
 
 # option -> candidate values, in the order they are tried (the first is the default)
 KERNEL_OPTIONS: Tuple[Tuple[int, Tuple[int, ...]], ...] = (
@@ -72,8 +76,10 @@ class TuneResult:
                 for t in self.trials]
 
 
-def _label(variant: str, block: int) -> str:
-    return "mc" if variant == "piccg" else f"abmc{block}"
+def _label(variant: str, block: int, blocking: str = "bfs") -> str:
+    if variant == "piccg":
+        return "mc"
+    return f"abmc{block}" + ("" if blocking == "bfs" else f"_{blocking}")
 
 
 def _solve_time(ctx: Context, b_run: np.ndarray, storage: int, tol: float, reps: int) -> Tuple[float, int, bool]:
@@ -96,14 +102,15 @@ def pick(trials: Sequence[Trial]) -> Trial:
     return min(pool, key=lambda t: t.ms)
 
 
-def tune_ordering(A: CRS, candidates: Sequence[Tuple[str, int]] = ORDERINGS, storage: int = STORE_FP32,
+def tune_ordering(A: CRS, candidates: Sequence[Tuple] = ORDERINGS, storage: int = STORE_FP32,
                   tol: float = 1e-8, seed: int = 0, device: int = 0, reps: int = 1,
-                  blocking: str = "bfs",
                   timer: Optional[Callable[[Problem], Tuple[float, int, bool]]] = None) -> Tuple[Problem, TuneResult]:
     """Builds each candidate ordering of A (the original, unpermuted matrix)
     and returns the one whose solve to `tol` is fastest, with the timings.
-    `timer(P)` returns (ms, iterations, converged) for a built problem; the
-    default uploads P to a fresh context on `device` and times `reps` solves."""
+    A candidate is (variant, block size[, blocking]), blocking "bfs" when
+    omitted. `timer(P)` returns (ms, iterations, converged) for a built
+    problem; the default uploads P to a fresh context on `device` and times
+    `reps` solves."""
 
     def device_timer(P: Problem) -> Tuple[float, int, bool]:
         ctx = Context(device)
@@ -118,8 +125,10 @@ def tune_ordering(A: CRS, candidates: Sequence[Tuple[str, int]] = ORDERINGS, sto
     timer = timer or device_timer
     trials: List[Trial] = []
     built: Dict[str, Problem] = {}
-    for variant, block in candidates:
-        label = _label(variant, block)
+    for cand in candidates:
+        variant, block = cand[0], cand[1]
+        blocking = cand[2] if len(cand) > 2 else "bfs"
+        label = _label(variant, block, blocking)
         P = make(A, variant, block_size=max(block, 1), blocking=blocking, seed=seed, name=label)
         ms, iters, conv = timer(P)
         trials.append(Trial(label, ms, iters, conv))

@@ -21,18 +21,22 @@ def test_pick_prefers_fastest_converged():
 
 def test_tune_ordering_builds_candidates_and_returns_the_fastest():
     A = pb.poisson2d(24)
-    cost = {"mc": 7.0, "abmc8": 3.0, "abmc16": 4.0, "abmc32": 9.0}
+    cost = {"mc": 7.0, "abmc8": 3.0, "abmc16": 4.0, "abmc32": 9.0, "abmc16_linear": 3.5, "abmc32_linear": 8.0}
     seen = []
 
     def timer(P):
-        seen.append((P.name, P.variant, P.nb, P.nc))
+        seen.append((P.name, P.variant, P.nb, P.nc, P.info.get("blocking")))
         return cost[P.name], 40, True
 
     P, res = at.tune_ordering(A, timer=timer)
-    assert [s[0] for s in seen] == ["mc", "abmc8", "abmc16", "abmc32"]
+    assert [s[0] for s in seen] == ["mc", "abmc8", "abmc16", "abmc32", "abmc16_linear", "abmc32_linear"]
+    assert seen[4][4] == "linear" and seen[1][4] == "bfs"
     assert res.best == "abmc8" and P.name == "abmc8" and P.variant == "abmc"
     assert P.info["block_size"] == 8 and P.nb > 0
-    assert len(res.table()) == 4
+    assert len(res.table()) == 6
+    # two-element candidates default to breadth-first blocking
+    P2, res2 = at.tune_ordering(A, candidates=(("abmc", 16),), timer=timer)
+    assert res2.best == "abmc16" and P2.info["blocking"] == "bfs"
     # the chosen problem is the one built: same b, same ordering as make()
     ref = pb.make(A, "abmc", block_size=8, blocking="bfs", seed=0)
     assert np.array_equal(P.new_of_old, ref.new_of_old)
