@@ -149,8 +149,10 @@ int iccg_ctx_set_option(iccg_ctx* c, int option, long long value)
 int iccg_matrix_upload(iccg_ctx* c, int n, const int* rowptr, const int* colind, const double* val)
 {
     return guard(c, [&] {
+        SetupPhase all("upload");
         if (n <= 0 || !rowptr || !colind || !val) throw Error(ICCG_ERR_ARG, "bad matrix arguments");
         if (rowptr[0] != 0) throw Error(ICCG_ERR_ARG, "rowptr[0] must be 0");
+        SetupPhase* v = new SetupPhase("upload.validate");
         for (int i = 0; i < n; ++i) {
             if (rowptr[i + 1] < rowptr[i]) throw Error(ICCG_ERR_ARG, "rowptr must be nondecreasing");
             for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
@@ -159,25 +161,33 @@ int iccg_matrix_upload(iccg_ctx* c, int n, const int* rowptr, const int* colind,
                     throw Error(ICCG_ERR_ARG, "columns must be strictly ascending within each row");
             }
         }
+        delete v;
         drop_graph(c);
         const int nnz = rowptr[n];
         c->n = n;
         c->nnz = nnz;
-        c->h_rowptr.assign(rowptr, rowptr + n + 1);
-        c->h_colind.assign(colind, colind + nnz);
-        c->h_val.assign(val, val + nnz);
-        c->rowptr.upload(rowptr, (size_t)n + 1, &c->dev_bytes, c->stream);
-        c->colind.upload(colind, (size_t)nnz, &c->dev_bytes, c->stream);
-        c->val64.upload(val, (size_t)nnz, &c->dev_bytes, c->stream);
-        c->val32.free();
-        c->has_val32 = false;
-        ensure_vectors(c);
+        {
+            SetupPhase t("upload.copy");
+            c->h_rowptr.assign(rowptr, rowptr + n + 1);
+            c->h_colind.assign(colind, colind + nnz);
+            c->h_val.assign(val, val + nnz);
+            c->rowptr.upload(rowptr, (size_t)n + 1, &c->dev_bytes, c->stream);
+            c->colind.upload(colind, (size_t)nnz, &c->dev_bytes, c->stream);
+            c->val64.upload(val, (size_t)nnz, &c->dev_bytes, c->stream);
+            c->val32.free();
+            c->has_val32 = false;
+            ensure_vectors(c);
+            CK(cudaStreamSynchronize(c->stream));
+        }
         // a new matrix invalidates the schedule and the preconditioner
         c->pc_kind = -1;
         c->F.reset();
         c->Q.reset();
         c->sched_kind = ICCG_SCHED_NONE;
-        build_plans_none(c);
+        {
+            SetupPhase t("upload.natural_order_plans");
+            build_plans_none(c);
+        }
         c->sched_version++;
         c->factor_version++;
         CK(cudaStreamSynchronize(c->stream));
@@ -245,6 +255,7 @@ int iccg_precond_build(iccg_ctx* c, int kind, double shift, int auto_shift)
             c->inv_diag.upload(inv.data(), inv.size(), &c->dev_bytes, c->stream);
             CK(cudaStreamSynchronize(c->stream));
         } else if (kind == ICCG_PRECOND_IC0) {
+            SetupPhase t("precond_build.ic0");
             build_ic0(c, shift, auto_shift != 0);
         } else {
             throw Error(ICCG_ERR_ARG, "unknown preconditioner kind");

@@ -3,6 +3,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <string>
 
 #include "host.hpp"
@@ -81,6 +84,31 @@ struct Buf {
     {
         m.release();
         n = cap = 0;
+    }
+};
+
+// Set-up tracing: with ICCG_TRACE_SETUP set in the environment, each traced
+// phase of a context's set-up prints its wall time to stderr as
+// "[iccg setup] <phase> <ms> ms" when it ends.  Phases that end with a
+// stream synchronisation include their device work.
+inline bool trace_setup()
+{
+    static const bool on = std::getenv("ICCG_TRACE_SETUP") != nullptr;
+    return on;
+}
+
+struct SetupPhase {
+    const char* name;
+    std::chrono::steady_clock::time_point t0;
+    explicit SetupPhase(const char* n) : name(n), t0(std::chrono::steady_clock::now()) {}
+    SetupPhase(const SetupPhase&) = delete;
+    SetupPhase& operator=(const SetupPhase&) = delete;
+    ~SetupPhase()
+    {
+        if (!trace_setup()) return;
+        const double ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        std::fprintf(stderr, "[iccg setup] %s %.2f ms\n", name, ms);
     }
 };
 

@@ -100,7 +100,12 @@ static void build_ic0(iccg_ctx* c, double shift, bool auto_shift)
     Factor& F = c->F;
     F.built = false;
     F.has32 = false;
-    build_factor_pattern(c);
+    {
+        SetupPhase t("ic0.pattern");
+        build_factor_pattern(c);
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    SetupPhase* tf = new SetupPhase("ic0.factor");
     std::vector<double> Lx0((size_t)F.nnzL);
     CK(cudaMemcpyAsync(Lx0.data(), F.dLx.get(), sizeof(double) * Lx0.size(), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -128,6 +133,9 @@ static void build_ic0(iccg_ctx* c, double shift, bool auto_shift)
         throw Error(ICCG_ERR_PIVOT_NONPOS, "IC(0): non-positive pivot at row " + std::to_string(rep));
     }
     F.shift = s;
+    CK(cudaStreamSynchronize(c->stream));
+    delete tf;
+    SetupPhase tsw("ic0.sweep_arrays");
     // sweep arrays
     std::vector<int> dsrc(F.dpos);
     F.dSp.upload(F.Sp.data(), F.Sp.size(), &c->dev_bytes, c->stream);

@@ -408,6 +408,7 @@ static void plan_staged(iccg_ctx* c)
         }
         Q.lb[(size_t)l + 1] = (int)bds.size();
     }
+    SetupPhase t("q.factor.staged_grids");
     if (!plan_staged_type<double>(c, 0) || !plan_staged_type<float>(c, 1)) return;
     Q.bdesc.upload(bds.data(), bds.size(), &c->dev_bytes, c->stream);
     CK(cudaStreamSynchronize(c->stream));
@@ -504,6 +505,7 @@ static void ensure_q(iccg_ctx* c)
 {
     QSys& Q = c->Q;
     if (!Q.ok || Q.version != c->sched_version) {
+        SetupPhase t("q.order");
         Q.reset();
         build_q_order(c);
         Q.version = c->sched_version;
@@ -511,7 +513,10 @@ static void ensure_q(iccg_ctx* c)
     }
     if (Q.factor_version != c->factor_version) {
         // a new preconditioner since the last build
-        if (c->pc_kind == ICCG_PRECOND_IC0 && c->F.built) build_q_factor(c);
+        if (c->pc_kind == ICCG_PRECOND_IC0 && c->F.built) {
+            SetupPhase t("q.factor");
+            build_q_factor(c);
+        }
         if (c->pc_kind == ICCG_PRECOND_JACOBI) {
             Q.inv_diag.alloc((size_t)c->n, &c->dev_bytes);
             launch(c, 3, k_gather<double>, grid_for(c, c->n), kThreads, (long long)c->n, (const int*)Q.dq2r.get(),
@@ -524,6 +529,7 @@ static void ensure_q(iccg_ctx* c)
 
 static void ensure_q32(iccg_ctx* c)
 {
+    SetupPhase t("q.fp32_copies");
     QSys& Q = c->Q;
     sell_f32(c, Q.A);
     if (c->pc_kind == ICCG_PRECOND_IC0 && c->F.built) {

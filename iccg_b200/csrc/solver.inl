@@ -375,6 +375,7 @@ static void solve_fused(iccg_ctx* c, const double* b, double* x, int max_iter, d
             if (g.mask == mk) return g;
         cudaGraph_t graph = nullptr;
         const long long before = c->launches;
+        SetupPhase tg("solve.graph_capture");
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         try {
             one_batch(mk);
