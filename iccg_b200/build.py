@@ -20,7 +20,7 @@ LIBDIR = PKG / "_lib"
 LIB = LIBDIR / "libiccg_b200.so"
 
 CUDA_SOURCES = ["ctx.cu", "noalloc.cu"]
-HOST_SOURCES = ["host_order.cpp", "host_gen.cpp", "host_capi.cpp"]
+HOST_SOURCES = ["host_order.cpp", "host_gen.cpp", "host_layout.cpp", "host_capi.cpp"]
 HEADERS = ["dd.cuh", "kernels.cuh", "host.hpp", "devbuf.hpp", "context.hpp", "plan.inl", "factor.inl", "qsys.inl", "solver.inl"]
 
 NVCC_FLAGS = [

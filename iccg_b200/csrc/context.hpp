@@ -28,11 +28,10 @@ struct Plan {
 
 // IC(0) factor in the reference's layout (L rows, A_run numbering) plus the
 // strict-lower / strict-upper split used by the substitutions.
-struct Factor {
+struct Factor : Ic0Layout {
     bool built = false;
     int nnzL = 0;
     double shift = 0.0;
-    std::vector<int> Lp, Li, dpos, Up, Ui, ut_src, Sp, Si, s_src, Tp, Ti, t_src;
     Buf<int> dLp, dLi, ddpos;
     Buf<double> dLx;
     // simple-path arrays (A_run numbering)
@@ -54,20 +53,13 @@ struct Factor {
 };
 
 // A SELL-32 matrix over Q rows (see kernels.cuh, "Lane-interleaved kernels").
-struct SellDev {
+// The host arrays (SellLayout) keep h_ptr, src, prev_only and unit_only;
+// h_col and h_len are released once they are on the device.
+struct SellDev : SellLayout {
     Buf<int> ptr, col, len;
     Buf<double> v64;
     Buf<float> v32;
     bool has32 = false;
-    long long slots = 0;
-    int max_nin = 0;       // most in-unit entries of a row (encoded matrices)
-    std::vector<int> h_ptr;  // host copy of ptr
-    std::vector<int> src;  // host: CRS value index of each slot (-1: padding)
-    // host, encoded matrices: per Q row, 1 when the row has at most one
-    // in-unit entry and that entry is the unit's row one step before it in
-    // the sweep's order
-    std::vector<unsigned char> prev_only;
-    std::vector<unsigned char> unit_only;  // host, encoded matrices: 1 when every entry of the row is in-unit
     SellMat view(bool fp32) const
     {
         return SellMat{ptr.get(), col.get(), fp32 ? (const void*)v32.get() : (const void*)v64.get(), len.get()};
@@ -82,6 +74,8 @@ struct SellDev {
         max_nin = 0;
         src.clear();
         h_ptr.clear();
+        h_col.clear();
+        h_len.clear();
         prev_only.clear();
         unit_only.clear();
     }

@@ -168,9 +168,12 @@ int iccg_matrix_upload(iccg_ctx* c, int n, const int* rowptr, const int* colind,
         c->nnz = nnz;
         {
             SetupPhase t("upload.copy");
-            c->h_rowptr.assign(rowptr, rowptr + n + 1);
-            c->h_colind.assign(colind, colind + nnz);
-            c->h_val.assign(val, val + nnz);
+            size_for_fill(c->h_rowptr, (size_t)n + 1);
+            size_for_fill(c->h_colind, (size_t)nnz);
+            size_for_fill(c->h_val, (size_t)nnz);
+            std::copy(rowptr, rowptr + n + 1, c->h_rowptr.begin());
+            std::copy(colind, colind + nnz, c->h_colind.begin());
+            std::copy(val, val + nnz, c->h_val.begin());
             c->rowptr.upload(rowptr, (size_t)n + 1, &c->dev_bytes, c->stream);
             c->colind.upload(colind, (size_t)nnz, &c->dev_bytes, c->stream);
             c->val64.upload(val, (size_t)nnz, &c->dev_bytes, c->stream);

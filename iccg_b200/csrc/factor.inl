@@ -4,70 +4,15 @@
 // ---------------------------------------------------------------------------
 // IC(0) on the device
 // ---------------------------------------------------------------------------
-static void build_factor_pattern(iccg_ctx* c)
+// L's layout, on the host and the device, and its initial values Lx0 (the
+// lower part of A, ic0.cpp:42-44)
+static void build_factor_pattern(iccg_ctx* c, std::vector<double>& Lx0)
 {
     Factor& F = c->F;
     const int n = c->n;
-    // extract_lower_with_diag (ic0.cpp:14-38) and diag_pos (ic0.cpp:47-54)
-    F.Lp.assign((size_t)n + 1, 0);
-    F.Li.clear();
-    std::vector<int> src;
-    for (int i = 0; i < n; ++i) {
-        F.Lp[(size_t)i] = (int)F.Li.size();
-        for (int k = c->h_rowptr[(size_t)i]; k < c->h_rowptr[(size_t)i + 1]; ++k)
-            if (c->h_colind[(size_t)k] <= i) { F.Li.push_back(c->h_colind[(size_t)k]); src.push_back(k); }
-    }
-    F.Lp[(size_t)n] = (int)F.Li.size();
+    build_ic0_layout(n, c->h_rowptr.data(), c->h_colind.data(), c->h_val.data(), F, Lx0,
+                     layout_threads((long long)c->h_colind.size()));
     F.nnzL = (int)F.Li.size();
-    F.dpos.assign((size_t)n, -1);
-    for (int i = 0; i < n; ++i) {
-        for (int k = F.Lp[(size_t)i]; k < F.Lp[(size_t)i + 1]; ++k)
-            if (F.Li[(size_t)k] == i) { F.dpos[(size_t)i] = k; break; }
-        if (F.dpos[(size_t)i] < 0)
-            throw Error(ICCG_ERR_DIAG, "IC(0): diagonal missing at row " + std::to_string(i));
-    }
-    // CSC of L (build_csc_from_crs, ic0.cpp:118-151)
-    F.Up.assign((size_t)n + 1, 0);
-    for (int k = 0; k < F.nnzL; ++k) F.Up[(size_t)F.Li[(size_t)k] + 1]++;
-    for (int i = 0; i < n; ++i) F.Up[(size_t)i + 1] += F.Up[(size_t)i];
-    F.Ui.assign((size_t)F.nnzL, 0);
-    F.ut_src.assign((size_t)F.nnzL, 0);
-    {
-        std::vector<int> cur(F.Up.begin(), F.Up.end() - 1);
-        for (int i = 0; i < n; ++i)
-            for (int k = F.Lp[(size_t)i]; k < F.Lp[(size_t)i + 1]; ++k) {
-                const int pos = cur[(size_t)F.Li[(size_t)k]]++;
-                F.Ui[(size_t)pos] = i;
-                F.ut_src[(size_t)pos] = k;
-            }
-    }
-    // sweep layout: strict lower part of L rows, strict upper part of L^T rows
-    F.Sp.assign((size_t)n + 1, 0);
-    F.Si.clear();
-    F.s_src.clear();
-    for (int i = 0; i < n; ++i) {
-        F.Sp[(size_t)i] = (int)F.Si.size();
-        for (int k = F.Lp[(size_t)i]; k < F.Lp[(size_t)i + 1]; ++k) {
-            const int j = F.Li[(size_t)k];
-            if (j < i) { F.Si.push_back(j); F.s_src.push_back(k); }
-            else break;
-        }
-    }
-    F.Sp[(size_t)n] = (int)F.Si.size();
-    F.Tp.assign((size_t)n + 1, 0);
-    F.Ti.clear();
-    F.t_src.clear();
-    for (int i = 0; i < n; ++i) {
-        F.Tp[(size_t)i] = (int)F.Ti.size();
-        for (int k = F.Up[(size_t)i]; k < F.Up[(size_t)i + 1]; ++k) {
-            const int j = F.Ui[(size_t)k];
-            if (j > i) { F.Ti.push_back(j); F.t_src.push_back(F.ut_src[(size_t)k]); }
-        }
-    }
-    F.Tp[(size_t)n] = (int)F.Ti.size();
-    // initial values of L = lower part of A (ic0.cpp:42-44)
-    std::vector<double> Lx0((size_t)F.nnzL);
-    for (size_t k = 0; k < src.size(); ++k) Lx0[k] = c->h_val[(size_t)src[k]];
     F.dLp.upload(F.Lp.data(), F.Lp.size(), &c->dev_bytes, c->stream);
     F.dLi.upload(F.Li.data(), F.Li.size(), &c->dev_bytes, c->stream);
     F.ddpos.upload(F.dpos.data(), F.dpos.size(), &c->dev_bytes, c->stream);
@@ -100,15 +45,12 @@ static void build_ic0(iccg_ctx* c, double shift, bool auto_shift)
     Factor& F = c->F;
     F.built = false;
     F.has32 = false;
+    std::vector<double> Lx0;  // A's lower entries: the factor's initial values
     {
         SetupPhase t("ic0.pattern");
-        build_factor_pattern(c);
-        CK(cudaStreamSynchronize(c->stream));
+        build_factor_pattern(c, Lx0);
     }
     SetupPhase* tf = new SetupPhase("ic0.factor");
-    std::vector<double> Lx0((size_t)F.nnzL);
-    CK(cudaMemcpyAsync(Lx0.data(), F.dLx.get(), sizeof(double) * Lx0.size(), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
     double max_aii = 0.0;
     for (int i = 0; i < c->n; ++i) max_aii = std::max(max_aii, std::fabs(Lx0[(size_t)F.dpos[(size_t)i]]));
     double s = shift;
@@ -137,7 +79,6 @@ static void build_ic0(iccg_ctx* c, double shift, bool auto_shift)
     delete tf;
     SetupPhase tsw("ic0.sweep_arrays");
     // sweep arrays
-    std::vector<int> dsrc(F.dpos);
     F.dSp.upload(F.Sp.data(), F.Sp.size(), &c->dev_bytes, c->stream);
     F.dSi.upload(F.Si.data(), F.Si.size(), &c->dev_bytes, c->stream);
     F.dTp.upload(F.Tp.data(), F.Tp.size(), &c->dev_bytes, c->stream);
@@ -153,7 +94,7 @@ static void build_ic0(iccg_ctx* c, double shift, bool auto_shift)
     };
     gather(F.s_src, F.S64);
     gather(F.t_src, F.T64);
-    gather(dsrc, F.d64);
+    gather(F.dpos, F.d64);
     idx.free();
     CK(cudaStreamSynchronize(c->stream));
     F.built = true;

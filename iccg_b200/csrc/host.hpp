@@ -6,9 +6,12 @@
 // file:line of the reference function each one stands in for is given at
 // its definition.
 #pragma once
+#include <sys/mman.h>
+
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace iccg {
@@ -70,6 +73,77 @@ int block_partition(int n, const int* rowptr, const int* colind, int B, int meth
                     int* block_of_old);
 int color_blocks(int n, const int* rowptr, const int* colind, const int* block_of_old, int nb,
                  int* block_color);
+
+// Sizes v to `count` elements for a caller that then writes all of them.
+// A vector that must grow is reallocated without copying its old contents,
+// and its range is advised for transparent huge pages before the first
+// touch: on a large system the set-up is bound by faults on fresh host
+// pages, and a 2 MB page is one fault instead of 512.
+template <class T>
+void size_for_fill(std::vector<T>& v, size_t count)
+{
+    if (v.capacity() < count) {
+        std::vector<T>().swap(v);
+        v.reserve(count);
+        const uintptr_t huge = (uintptr_t)2 << 20, a = (uintptr_t)v.data();
+        const uintptr_t b = (a + huge - 1) & ~(huge - 1), e = (a + count * sizeof(T)) & ~(huge - 1);
+        if (e > b) (void)madvise((void*)b, e - b, MADV_HUGEPAGE);
+    }
+    v.resize(count);
+}
+
+// ---- IC(0) layout ----
+// The sparsity layout of IC(0) on A's lower triangle: L's rows (Lp, Li) and
+// diagonal places (dpos), its columns (Up, Ui, ut_src = each column entry's
+// index into Li), the strictly lower part of L's rows (Sp, Si, s_src) and
+// the strictly upper part of L^T's rows (Tp, Ti, t_src).
+struct Ic0Layout {
+    std::vector<int> Lp, Li, dpos, Up, Ui, ut_src, Sp, Si, s_src, Tp, Ti, t_src;
+};
+// Builds L's layout and its initial values Lx0 (A's lower entries) on
+// `threads` host threads; the result is the same for every thread count.
+// Throws Error(ICCG_ERR_DIAG) naming the first row without a diagonal entry.
+void build_ic0_layout(int n, const int* rowptr, const int* colind, const double* val, Ic0Layout& out,
+                      std::vector<double>& Lx0, int threads);
+// host threads worth using for a layout over a matrix with nnz entries
+int layout_threads(long long nnz);
+
+// ---- SELL-32 layout ----
+// The row order of a lane-interleaved matrix: Q row q holds CRS row q2r[q]
+// (r2q is its inverse), of unit unit_of[r] at step step_of[r] of the unit.
+struct SellOrder {
+    int nq = 0;
+    const int* q2r = nullptr;
+    const int* r2q = nullptr;
+    const int* unit_of = nullptr;
+    const int* step_of = nullptr;
+};
+// Host arrays of a SELL-32 matrix.  Slice s (32 Q rows) occupies slots
+// [h_ptr[s], h_ptr[s+1]); entry j of the slice's lane l sits at slot
+// h_ptr[s] + 32 j + l.  h_col is a Q column, or -(step + 1) for an entry of
+// the row's own unit in an encoded matrix; src is the entry's CRS value
+// index (-1 on padding); h_len[q] = row length | in-unit entries << 16.
+struct SellLayout {
+    long long slots = 0;
+    int max_nin = 0;           // most in-unit entries of a row (encoded matrices)
+    std::vector<int> h_ptr;    // slices + 1
+    std::vector<int> h_col;    // slots
+    std::vector<int> h_len;    // Q rows
+    std::vector<int> src;      // slots
+    // encoded matrices, per Q row: 1 when the row has at most one in-unit
+    // entry and that entry is the unit's row one step before it in the
+    // sweep's order
+    std::vector<unsigned char> prev_only;
+    std::vector<unsigned char> unit_only;  // encoded: 1 when every entry of the row is in-unit
+};
+// Fills M for the rows of `slices` ((first Q row, rows) pairs) of the CRS
+// pattern (rp, ci); src_map, when given, maps a CRS entry to its value
+// index.  encode 1 (forward) or 2 (backward) marks in-unit entries, which
+// must come last (1) or first (2) in every row; otherwise it returns false
+// and leaves M as it was.  Throws Error(ICCG_ERR_ARG) when the slots
+// overflow int32 or a row is longer than 65535 entries.
+bool build_sell_layout(const std::vector<std::pair<int, int>>& slices, const int* rp, const int* ci,
+                       const int* src_map, const SellOrder& order, int encode, SellLayout& M, int threads);
 
 // splitmix64 step
 inline uint64_t splitmix64(uint64_t& s)

@@ -17,76 +17,18 @@ static bool sell_build(iccg_ctx* c, const std::vector<std::pair<int, int>>& slic
                        const std::vector<int>& ci, const std::vector<int>* src_map, SellDev& M, int encode = 0)
 {
     const QSys& Q = c->Q;
-    if (encode) {
-        for (size_t s = 0; s < slices.size(); ++s)
-            for (int l = 0; l < slices[s].second; ++l) {
-                const int r = Q.q2r[(size_t)(slices[s].first + l)];
-                const int b = rp[(size_t)r], L = rp[(size_t)r + 1] - b;
-                bool seen_in = false, seen_out = false;
-                for (int j = 0; j < L; ++j) {
-                    const bool inside = Q.unit_of[(size_t)ci[(size_t)b + j]] == Q.unit_of[(size_t)r];
-                    if (encode == 1 && seen_in && !inside) return false;   // forward: in-unit entries last
-                    if (encode == 2 && seen_out && inside) return false;   // backward: in-unit entries first
-                    seen_in |= inside;
-                    seen_out |= !inside;
-                }
-            }
-    }
-    const int n = (int)Q.q2r.size();
-    std::vector<int> ptr(slices.size() + 1), len((size_t)n, 0);
-    long long slot = 0;
-    for (size_t s = 0; s < slices.size(); ++s) {
-        if (slot > 2147483647LL) throw Error(ICCG_ERR_ARG, "matrix too large for int32 SELL slots");
-        ptr[s] = (int)slot;
-        int w = 0;
-        for (int l = 0; l < slices[s].second; ++l) {
-            const int r = Q.q2r[(size_t)(slices[s].first + l)];
-            w = std::max(w, rp[(size_t)r + 1] - rp[(size_t)r]);
-        }
-        slot += 32LL * w;
-    }
-    if (slot > 2147483647LL) throw Error(ICCG_ERR_ARG, "matrix too large for int32 SELL slots");
-    ptr[slices.size()] = (int)slot;
-    std::vector<int> col((size_t)slot, 0);
-    M.src.assign((size_t)slot, -1);
-    M.max_nin = 0;
-    M.prev_only.assign(encode ? (size_t)n : 0, 0);
-    M.unit_only.assign(encode ? (size_t)n : 0, 0);
-    for (size_t s = 0; s < slices.size(); ++s)
-        for (int l = 0; l < slices[s].second; ++l) {
-            const int q = slices[s].first + l;
-            const int r = Q.q2r[(size_t)q];
-            const int b = rp[(size_t)r], L = rp[(size_t)r + 1] - b;
-            if (L > 0xffff) throw Error(ICCG_ERR_ARG, "row longer than 65535 entries");
-            int nin = 0;
-            bool prev = true;
-            for (int j = 0; j < L; ++j) {
-                const size_t pos = (size_t)ptr[s] + 32 * (size_t)j + (size_t)l;
-                const int cj = ci[(size_t)b + j];
-                if (encode && Q.unit_of[(size_t)cj] == Q.unit_of[(size_t)r]) {
-                    col[pos] = -(Q.step_of[(size_t)cj] + 1);
-                    ++nin;
-                    prev = prev && Q.step_of[(size_t)cj] == Q.step_of[(size_t)r] + (encode == 1 ? -1 : 1);
-                } else {
-                    col[pos] = Q.r2q[(size_t)cj];
-                }
-                M.src[pos] = src_map ? (*src_map)[(size_t)b + j] : b + j;
-            }
-            len[(size_t)q] = L | (nin << 16);
-            M.max_nin = std::max(M.max_nin, nin);
-            if (encode) {
-                M.prev_only[(size_t)q] = (unsigned char)(prev && nin <= 1);
-                M.unit_only[(size_t)q] = (unsigned char)(nin == L);
-            }
-        }
-    M.ptr.upload(ptr.data(), ptr.size(), &c->dev_bytes, c->stream);
-    M.h_ptr = ptr;
-    M.col.upload(col.data(), col.size(), &c->dev_bytes, c->stream);
-    M.len.upload(len.data(), len.size(), &c->dev_bytes, c->stream);
-    M.slots = slot;
+    const SellOrder order{(int)Q.q2r.size(), Q.q2r.data(), Q.r2q.data(), Q.unit_of.data(), Q.step_of.data()};
+    if (!build_sell_layout(slices, rp.data(), ci.data(), src_map ? src_map->data() : nullptr, order, encode, M,
+                           layout_threads((long long)ci.size())))
+        return false;
+    M.ptr.upload(M.h_ptr.data(), M.h_ptr.size(), &c->dev_bytes, c->stream);
+    M.col.upload(M.h_col.data(), M.h_col.size(), &c->dev_bytes, c->stream);
+    M.len.upload(M.h_len.data(), M.h_len.size(), &c->dev_bytes, c->stream);
     M.has32 = false;
     M.v32.free();
     CK(cudaStreamSynchronize(c->stream));
+    std::vector<int>().swap(M.h_col);
+    std::vector<int>().swap(M.h_len);
     return true;
 }
 
