@@ -203,6 +203,9 @@ struct iccg_ctx {
     bool has_val32 = false;
     // schedule
     int sched_kind = ICCG_SCHED_NONE;
+    // the natural-order plans are due but not built: an upload leaves them
+    // to the first call that needs them, since a schedule usually follows
+    bool plans_pending = false;
     int sched_version = 0;
     iccg::Plan fwd, bwd;
     // lane-interleaved system (default) or the simple one-thread-per-row path

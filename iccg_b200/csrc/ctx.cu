@@ -167,13 +167,16 @@ int iccg_matrix_upload(iccg_ctx* c, int n, const int* rowptr, const int* colind,
         c->n = n;
         c->nnz = nnz;
         {
-            SetupPhase t("upload.copy");
+            SetupPhase t("upload.host_copy");
             size_for_fill(c->h_rowptr, (size_t)n + 1);
             size_for_fill(c->h_colind, (size_t)nnz);
             size_for_fill(c->h_val, (size_t)nnz);
             std::copy(rowptr, rowptr + n + 1, c->h_rowptr.begin());
             std::copy(colind, colind + nnz, c->h_colind.begin());
             std::copy(val, val + nnz, c->h_val.begin());
+        }
+        {
+            SetupPhase t("upload.device_copy");
             c->rowptr.upload(rowptr, (size_t)n + 1, &c->dev_bytes, c->stream);
             c->colind.upload(colind, (size_t)nnz, &c->dev_bytes, c->stream);
             c->val64.upload(val, (size_t)nnz, &c->dev_bytes, c->stream);
@@ -187,10 +190,7 @@ int iccg_matrix_upload(iccg_ctx* c, int n, const int* rowptr, const int* colind,
         c->F.reset();
         c->Q.reset();
         c->sched_kind = ICCG_SCHED_NONE;
-        {
-            SetupPhase t("upload.natural_order_plans");
-            build_plans_none(c);
-        }
+        c->plans_pending = true;
         c->sched_version++;
         c->factor_version++;
         CK(cudaStreamSynchronize(c->stream));
@@ -200,11 +200,15 @@ int iccg_matrix_upload(iccg_ctx* c, int n, const int* rowptr, const int* colind,
 int iccg_schedule_mc(iccg_ctx* c, int nc, const int* color_ptr, const int* rows_of_color)
 {
     return guard(c, [&] {
-        require_matrix(c);
+        require_uploaded(c);
         drop_graph(c);
-        build_plans_mc(c, nc, color_ptr, rows_of_color);
-        c->sched_kind = ICCG_SCHED_MC;
+        // until the new plans are complete the context is in the natural order
+        c->sched_kind = ICCG_SCHED_NONE;
+        c->plans_pending = true;
         c->sched_version++;
+        build_plans_mc(c, nc, color_ptr, rows_of_color);
+        c->plans_pending = false;
+        c->sched_kind = ICCG_SCHED_MC;
         CK(cudaStreamSynchronize(c->stream));
     });
 }
@@ -213,11 +217,15 @@ int iccg_schedule_abmc(iccg_ctx* c, int nc, int nb, const int* color_ptr_blk, co
                        const int* block_ptr, const int* rows_of_block)
 {
     return guard(c, [&] {
-        require_matrix(c);
+        require_uploaded(c);
         drop_graph(c);
-        build_plans_abmc(c, nc, nb, color_ptr_blk, blocks_of_color, block_ptr, rows_of_block);
-        c->sched_kind = ICCG_SCHED_ABMC;
+        // until the new plans are complete the context is in the natural order
+        c->sched_kind = ICCG_SCHED_NONE;
+        c->plans_pending = true;
         c->sched_version++;
+        build_plans_abmc(c, nc, nb, color_ptr_blk, blocks_of_color, block_ptr, rows_of_block);
+        c->plans_pending = false;
+        c->sched_kind = ICCG_SCHED_ABMC;
         CK(cudaStreamSynchronize(c->stream));
     });
 }
@@ -225,9 +233,10 @@ int iccg_schedule_abmc(iccg_ctx* c, int nc, int nb, const int* color_ptr_blk, co
 int iccg_schedule_none(iccg_ctx* c)
 {
     return guard(c, [&] {
-        require_matrix(c);
+        require_uploaded(c);
         drop_graph(c);
         build_plans_none(c);
+        c->plans_pending = false;
         c->sched_kind = ICCG_SCHED_NONE;
         c->sched_version++;
         CK(cudaStreamSynchronize(c->stream));

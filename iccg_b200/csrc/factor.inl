@@ -124,9 +124,21 @@ static void ensure_val32(iccg_ctx* c)
     c->has_val32 = true;
 }
 
-static void require_matrix(iccg_ctx* c)
+static void require_uploaded(iccg_ctx* c)
 {
     if (c->n <= 0 && c->h_rowptr.empty()) throw Error(ICCG_ERR_STATE, "no matrix uploaded");
+}
+
+// a matrix with its sweep plans: the natural-order ones are built here when
+// no schedule has replaced them since the upload
+static void require_matrix(iccg_ctx* c)
+{
+    require_uploaded(c);
+    if (c->plans_pending) {
+        SetupPhase t("natural_order_plans");
+        build_plans_none(c);
+        c->plans_pending = false;
+    }
 }
 
 static void require_precond(iccg_ctx* c)

@@ -253,6 +253,29 @@ def test_gpu_rejects_racy_schedule():
     ctx.close()
 
 
+def test_gpu_failed_schedule_falls_back_to_natural_order():
+    # a schedule that fails part-way leaves the context in the natural order,
+    # whatever schedule it held before
+    A = pb.poisson2d(8)
+    color, nc = ib.color_greedy(A)
+    cp = np.zeros(nc + 1, np.int32)
+    for c in range(nc):
+        cp[c + 1] = cp[c] + np.sum(color == c)
+    rows = np.concatenate([np.nonzero(color == c)[0] for c in range(nc)]).astype(np.int32)
+    bad = ib.ColorSchedule(nc=nc, color_ptr=cp, rows_of_color=rows[::-1].copy())
+    r = np.random.default_rng(7).standard_normal(A.n)
+    want = ob.OracleIC0(A.n, A.rowptr, A.colind, A.val).apply(r)
+    ctx = ib.Context(0)
+    ctx.upload(A)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    np.testing.assert_array_equal(ctx.apply(r), want)
+    with pytest.raises(ib.IccgError):
+        ctx.set_schedule(bad)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    np.testing.assert_array_equal(ctx.apply(r), want)
+    ctx.close()
+
+
 def test_gpu_state_errors():
     ctx = ib.Context(0)
     with pytest.raises(ib.IccgError) as e:
