@@ -11,7 +11,7 @@ static void build_factor_pattern(iccg_ctx* c, std::vector<double>& Lx0)
     Factor& F = c->F;
     const int n = c->n;
     build_ic0_layout(n, c->h_rowptr.data(), c->h_colind.data(), c->h_val.data(), F, Lx0,
-                     layout_threads((long long)c->h_colind.size()));
+                     host_threads((long long)c->h_colind.size()));
     F.nnzL = (int)F.Li.size();
     F.dLp.upload(F.Lp.data(), F.Lp.size(), &c->dev_bytes, c->stream);
     F.dLi.upload(F.Li.data(), F.Li.size(), &c->dev_bytes, c->stream);

@@ -8,9 +8,12 @@
 #pragma once
 #include <sys/mman.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -54,7 +57,9 @@ std::vector<int> build_permutation_by_color(const std::vector<int>& color);
 std::vector<int> build_permutation_by_block_color(const std::vector<int>& block_of_old,
                                                   const std::vector<int>& block_color);
 CRS permute_ptap_lower(const CRS& A, const std::vector<int>& new_of_old);
+CRS permute_ptap_lower(int n, const int* rowptr, const int* colind, const double* val, const int* new_of_old);
 CRS expand_lower_to_full(const CRS& L);
+CRS expand_lower_to_full(int n, const int* rowptr, const int* colind, const double* val);
 void build_color_schedule(const std::vector<int>& color, int nc,
                           const std::vector<int>& new_of_old, std::vector<int>& color_ptr,
                           std::vector<int>& rows_of_color);
@@ -73,6 +78,65 @@ int block_partition(int n, const int* rowptr, const int* colind, int B, int meth
                     int* block_of_old);
 int color_blocks(int n, const int* rowptr, const int* colind, const int* block_of_old, int nb,
                  int* block_color);
+
+// ---- host threads ----
+// Threads worth using for a host pass over `work` matrix entries: 1 below
+// about a million, else up to 16.  ICCG_HOST_THREADS in the environment
+// sets the count instead (results never depend on it).
+inline int host_threads(long long work)
+{
+    if (const char* e = std::getenv("ICCG_HOST_THREADS")) {
+        const int t = std::atoi(e);
+        if (t > 0) return std::min(t, 256);
+    }
+    if (work < (1ll << 20)) return 1;
+    const long long hw = std::max(1u, std::thread::hardware_concurrency());
+    return (int)std::min({hw, 16ll, work >> 18});
+}
+
+// fn(t) for t = 0..T-1 on T threads (the caller's is one).  Parts whose
+// thread cannot be started run on the caller's thread.  fn must not throw.
+template <class Fn>
+void run_parts(int T, const Fn& fn)
+{
+    if (T <= 1) {
+        fn(0);
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve((size_t)T - 1);
+    int started = 1;
+    try {
+        for (; started < T; ++started) th.emplace_back(fn, started);
+    } catch (...) {
+    }
+    fn(0);
+    for (int t = started; t < T; ++t) fn(t);
+    for (auto& x : th) x.join();
+}
+
+// s[1..T] holds per-part sums; makes s[t] the sum of the parts before t
+inline void scan_parts(std::vector<long long>& s)
+{
+    for (size_t t = 1; t < s.size(); ++t) s[t] += s[t - 1];
+}
+
+// T + 1 row boundaries splitting rows [0, n) into parts with about equal
+// numbers of entries of rowptr
+inline std::vector<int> row_parts(int n, const int* rowptr, int T)
+{
+    std::vector<int> rb((size_t)T + 1, 0);
+    const long long nnz = n > 0 ? rowptr[n] : 0;
+    for (int t = 1; t <= T; ++t) {
+        rb[(size_t)t] = t == T ? n : (int)(std::lower_bound(rowptr, rowptr + n, (int)(nnz * t / T)) - rowptr);
+        rb[(size_t)t] = std::max(rb[(size_t)t], rb[(size_t)t - 1]);
+    }
+    return rb;
+}
+
+// memcpy split over T threads (a fresh destination faults its pages in
+// parallel)
+void parallel_copy(void* dst, const void* src, size_t bytes, int T);
 
 // Sizes v to `count` elements for a caller that then writes all of them.
 // A vector that must grow is reallocated without copying its old contents,
@@ -105,8 +169,6 @@ struct Ic0Layout {
 // Throws Error(ICCG_ERR_DIAG) naming the first row without a diagonal entry.
 void build_ic0_layout(int n, const int* rowptr, const int* colind, const double* val, Ic0Layout& out,
                       std::vector<double>& Lx0, int threads);
-// host threads worth using for a layout over a matrix with nnz entries
-int layout_threads(long long nnz);
 
 // ---- SELL-32 layout ----
 // The row order of a lane-interleaved matrix: Q row q holds CRS row q2r[q]

@@ -32,6 +32,24 @@ int guarded(F&& f)
     }
 }
 
+// the argument checks of wrap() without its copy
+static void check_crs(int n, const int* rowptr, const int* colind, const double* val)
+{
+    if (n < 0 || !rowptr) throw Error(ICCG_ERR_ARG, "bad CRS arguments");
+    const int nnz = rowptr[n];
+    if (nnz < 0 || rowptr[0] != 0) throw Error(ICCG_ERR_ARG, "bad rowptr");
+    if (nnz > 0 && (!colind || !val)) throw Error(ICCG_ERR_ARG, "null colind/val");
+}
+
+// a result matrix into the caller's arrays, on host threads
+static void copy_out(const CRS& B, int* rowptr, int* colind, double* val)
+{
+    const int T = host_threads(B.nnz());
+    parallel_copy(rowptr, B.rowptr.data(), sizeof(int) * B.rowptr.size(), T);
+    parallel_copy(colind, B.colind.data(), sizeof(int) * B.colind.size(), T);
+    parallel_copy(val, B.val.data(), sizeof(double) * B.val.size(), T);
+}
+
 static CRS wrap(int n, const int* rowptr, const int* colind, const double* val)
 {
     if (n < 0 || !rowptr) throw Error(ICCG_ERR_ARG, "bad CRS arguments");
@@ -143,13 +161,11 @@ int iccg_ptap_lower(int n, const int* rowptr, const int* colind, const double* v
                     double* out_val, int* out_nnz)
 {
     return guarded([&] {
-        iccg::CRS A = iccg::wrap(n, rowptr, colind, val);
-        std::vector<int> p(new_of_old, new_of_old + n);
-        iccg::CRS B = iccg::permute_ptap_lower(A, p);
+        iccg::check_crs(n, rowptr, colind, val);
+        if (n > 0 && !new_of_old) throw iccg::Error(ICCG_ERR_ARG, "null new_of_old");
+        iccg::CRS B = iccg::permute_ptap_lower(n, rowptr, colind, val, new_of_old);
         if (B.nnz() > cap) throw iccg::Error(ICCG_ERR_ARG, "output capacity too small");
-        std::memcpy(out_rowptr, B.rowptr.data(), sizeof(int) * (size_t)(n + 1));
-        std::memcpy(out_colind, B.colind.data(), sizeof(int) * (size_t)B.nnz());
-        std::memcpy(out_val, B.val.data(), sizeof(double) * (size_t)B.nnz());
+        iccg::copy_out(B, out_rowptr, out_colind, out_val);
         *out_nnz = B.nnz();
     });
 }
@@ -169,10 +185,8 @@ int iccg_expand_lower_to_full(int n, const int* rowptr, const int* colind, const
                               int* out_rowptr, int* out_colind, double* out_val)
 {
     return guarded([&] {
-        iccg::CRS F = iccg::expand_lower_to_full(iccg::wrap(n, rowptr, colind, val));
-        std::memcpy(out_rowptr, F.rowptr.data(), sizeof(int) * (size_t)(n + 1));
-        std::memcpy(out_colind, F.colind.data(), sizeof(int) * (size_t)F.nnz());
-        std::memcpy(out_val, F.val.data(), sizeof(double) * (size_t)F.nnz());
+        iccg::check_crs(n, rowptr, colind, val);
+        iccg::copy_out(iccg::expand_lower_to_full(n, rowptr, colind, val), out_rowptr, out_colind, out_val);
     });
 }
 

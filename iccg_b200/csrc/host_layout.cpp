@@ -11,51 +11,12 @@
 // single thread would write, so the result does not depend on the number of
 // threads.
 #include <algorithm>
-#include <thread>
+#include <cstring>
 
 #include "host.hpp"
 #include "../../include/iccg.h"
 
 namespace iccg {
-
-namespace {
-
-// fn(t) for t = 0..T-1 on T threads (the caller's is one).  Parts whose
-// thread cannot be started run on the caller's thread.
-template <class Fn>
-void run_parts(int T, const Fn& fn)
-{
-    if (T <= 1) {
-        fn(0);
-        return;
-    }
-    std::vector<std::thread> th;
-    th.reserve((size_t)T - 1);
-    int started = 1;
-    try {
-        for (; started < T; ++started) th.emplace_back(fn, started);
-    } catch (...) {
-    }
-    fn(0);
-    for (int t = started; t < T; ++t) fn(t);
-    for (auto& x : th) x.join();
-}
-
-// exclusive scan of per-part sums held in s[1..T]
-void scan_parts(std::vector<long long>& s)
-{
-    for (size_t t = 1; t < s.size(); ++t) s[t] += s[t - 1];
-}
-
-}  // namespace
-
-int layout_threads(long long nnz)
-{
-    // below about a million entries the threads cost more than they save
-    if (nnz < (1ll << 20)) return 1;
-    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
-    return (int)std::min<long long>({(long long)hw, 16ll, nnz >> 18});
-}
 
 // extract_lower_with_diag (ic0.cpp:14-38), diag_pos (ic0.cpp:47-54) and
 // build_csc_from_crs (ic0.cpp:118-151) of the reference, plus the strict
@@ -64,14 +25,10 @@ void build_ic0_layout(int n, const int* rp, const int* ci, const double* val, Ic
                       std::vector<double>& Lx0, int threads)
 {
     const int T = std::max(1, std::min(threads, n));
-    const long long nnz = n > 0 ? rp[n] : 0;
     // row parts: about nnz / T of A's entries each; column parts: n / T columns
-    std::vector<int> rb((size_t)T + 1, 0), cb((size_t)T + 1, 0);
-    for (int t = 1; t <= T; ++t) {
-        cb[(size_t)t] = (int)((long long)n * t / T);
-        rb[(size_t)t] = t == T ? n : (int)(std::lower_bound(rp, rp + n, (int)(nnz * t / T)) - rp);
-        rb[(size_t)t] = std::max(rb[(size_t)t], rb[(size_t)t - 1]);
-    }
+    const std::vector<int> rb = row_parts(n, rp, T);
+    std::vector<int> cb((size_t)T + 1, 0);
+    for (int t = 1; t <= T; ++t) cb[(size_t)t] = (int)((long long)n * t / T);
 
     // rows: entries of L (columns <= i), the strictly lower ones before the
     // first diagonal entry, and that entry's place in the row
@@ -321,6 +278,15 @@ bool build_sell_layout(const std::vector<std::pair<int, int>>& slices, const int
     });
     M.max_nin = *std::max_element(nin_max.begin(), nin_max.end());
     return true;
+}
+
+void parallel_copy(void* dst, const void* src, size_t bytes, int T)
+{
+    T = std::max(1, T);
+    run_parts(T, [&](int t) {
+        const size_t b0 = bytes * (size_t)t / (size_t)T, b1 = bytes * (size_t)(t + 1) / (size_t)T;
+        if (b1 > b0) std::memcpy((char*)dst + b0, (const char*)src + b0, b1 - b0);
+    });
 }
 
 }  // namespace iccg

@@ -391,128 +391,239 @@ std::vector<int> build_permutation_by_block_color(const std::vector<int>& block_
     return new_of_old;
 }
 
+namespace {
+
+// Places the entries that a scan over input rows produces into the rows of
+// a CRS matrix, keeping in each output row the order of a single scan over
+// all input rows.  The input rows are split into parts; each part counts its
+// entries per output row, and a part's entries land after those of the
+// parts before it.  scan(i0, i1, put) calls put(row, col, val) for every
+// entry that input rows [i0, i1) produce, in order.
+template <class Scan>
+void scatter_rows(int n_out, const std::vector<int>& parts, const Scan& scan, std::vector<int>& ptr,
+                  std::vector<int>& col, std::vector<double>& val)
+{
+    const int T = (int)parts.size() - 1;
+    std::vector<std::vector<int>> at((size_t)T);
+    for (auto& a : at) a.reserve((size_t)n_out);  // filled (and first touched) by each part's thread
+    run_parts(T, [&](int t) {
+        std::vector<int>& c = at[(size_t)t];
+        c.resize((size_t)n_out);
+        scan(parts[(size_t)t], parts[(size_t)t + 1], [&](int r, int, double) { ++c[(size_t)r]; });
+    });
+    std::vector<int> ob((size_t)T + 1);
+    for (int t = 0; t <= T; ++t) ob[(size_t)t] = (int)((long long)n_out * t / T);
+    std::vector<long long> tot((size_t)T + 1, 0);
+    run_parts(T, [&](int t) {
+        long long s = 0;
+        for (int r = ob[(size_t)t]; r < ob[(size_t)t + 1]; ++r)
+            for (int u = 0; u < T; ++u) s += at[(size_t)u][(size_t)r];
+        tot[(size_t)t + 1] = s;
+    });
+    scan_parts(tot);
+    if (tot[(size_t)T] > 2147483647LL) throw Error(ICCG_ERR_ARG, "matrix exceeds int32 nnz");
+    size_for_fill(ptr, (size_t)n_out + 1);
+    // each part's count becomes the slot of its first entry in the row
+    run_parts(T, [&](int t) {
+        int a = (int)tot[(size_t)t];
+        for (int r = ob[(size_t)t]; r < ob[(size_t)t + 1]; ++r) {
+            ptr[(size_t)r] = a;
+            for (int u = 0; u < T; ++u) {
+                const int c = at[(size_t)u][(size_t)r];
+                at[(size_t)u][(size_t)r] = a;
+                a += c;
+            }
+        }
+    });
+    ptr[(size_t)n_out] = (int)tot[(size_t)T];
+    size_for_fill(col, (size_t)tot[(size_t)T]);
+    size_for_fill(val, (size_t)tot[(size_t)T]);
+    run_parts(T, [&](int t) {
+        std::vector<int>& next = at[(size_t)t];
+        scan(parts[(size_t)t], parts[(size_t)t + 1], [&](int r, int c, double v) {
+            const int p = next[(size_t)r]++;
+            col[(size_t)p] = c;
+            val[(size_t)p] = v;
+        });
+    });
+}
+
+// stable insertion sort of (col, val)[b, e) by column
+void sort_row_short(int* col, double* val, int b, int e)
+{
+    for (int t = b + 1; t < e; ++t) {
+        const int c = col[t];
+        const double v = val[t];
+        int u = t - 1;
+        while (u >= b && col[u] > c) {
+            col[u + 1] = col[u];
+            val[u + 1] = val[u];
+            --u;
+        }
+        col[u + 1] = c;
+        val[u + 1] = v;
+    }
+}
+
+void check_indices(int n, const int* rp, const int* ci, const int* perm, const std::vector<int>& parts,
+                   const char* what)
+{
+    const int T = (int)parts.size() - 1;
+    std::vector<unsigned char> bad((size_t)T, 0);
+    run_parts(T, [&](int t) {
+        for (int i = parts[(size_t)t]; i < parts[(size_t)t + 1]; ++i) {
+            if (perm && (perm[i] < 0 || perm[i] >= n)) bad[(size_t)t] = 1;
+            for (int k = rp[i]; k < rp[i + 1]; ++k)
+                if (ci[k] < 0 || ci[k] >= n) bad[(size_t)t] = 1;
+        }
+    });
+    for (int t = 0; t < T; ++t)
+        if (bad[(size_t)t]) throw Error(ICCG_ERR_ARG, std::string(what) + ": index out of range");
+}
+
+}  // namespace
+
 // Permute_PtAP_LowerCRS_to_LowerCRS (color.cpp:66-141).  Uses only j <= i of
 // the input, folds each entry to (max(ip,jp), min(ip,jp)), sorts every row by
 // column, sums duplicate columns (in input order) and drops sums equal to 0.0.
+CRS permute_ptap_lower(int n, const int* rp, const int* ci, const double* v, const int* new_of_old)
+{
+    const int T = std::max(1, std::min(host_threads(n > 0 ? rp[n] : 0), n));
+    const std::vector<int> parts = row_parts(n, rp, T);
+    check_indices(n, rp, ci, new_of_old, parts, "Permute_PtAP");
+    std::vector<int> bp, bc;
+    std::vector<double> bv;
+    scatter_rows(n, parts, [&](int i0, int i1, auto&& put) {
+        for (int i = i0; i < i1; ++i) {
+            const int ip = new_of_old[i];
+            for (int k = rp[i]; k < rp[i + 1]; ++k) {
+                const int j = ci[k];
+                if (j > i) continue;
+                const int jp = new_of_old[j];
+                put(std::max(ip, jp), std::min(ip, jp), v[k]);
+            }
+        }
+    }, bp, bc, bv);
+    // each row: sorted by column, equal columns summed in order, zero sums
+    // dropped; the kept entries move to the front of the row's range
+    CRS B;
+    B.n = n;
+    size_for_fill(B.rowptr, (size_t)n + 1);
+    std::vector<int> ob((size_t)T + 1);
+    for (int t = 0; t <= T; ++t) ob[(size_t)t] = (int)((long long)n * t / T);
+    std::vector<long long> kept((size_t)T + 1, 0);
+    run_parts(T, [&](int t) {
+        long long s = 0;
+        for (int r = ob[(size_t)t]; r < ob[(size_t)t + 1]; ++r) {
+            const int b = bp[(size_t)r], e = bp[(size_t)r + 1];
+            sort_row_short(bc.data(), bv.data(), b, e);
+            int w = b;
+            if (e > b) {
+                int cur_c = bc[(size_t)b];
+                double acc = bv[(size_t)b];
+                for (int q = b + 1; q < e; ++q) {
+                    if (bc[(size_t)q] == cur_c) {
+                        acc += bv[(size_t)q];
+                    } else {
+                        if (acc != 0.0) { bc[(size_t)w] = cur_c; bv[(size_t)w] = acc; ++w; }
+                        cur_c = bc[(size_t)q];
+                        acc = bv[(size_t)q];
+                    }
+                }
+                if (acc != 0.0) { bc[(size_t)w] = cur_c; bv[(size_t)w] = acc; ++w; }
+            }
+            B.rowptr[(size_t)r] = w - b;
+            s += w - b;
+        }
+        kept[(size_t)t + 1] = s;
+    });
+    scan_parts(kept);
+    run_parts(T, [&](int t) {
+        int a = (int)kept[(size_t)t];
+        for (int r = ob[(size_t)t]; r < ob[(size_t)t + 1]; ++r) {
+            const int c = B.rowptr[(size_t)r];
+            B.rowptr[(size_t)r] = a;
+            a += c;
+        }
+    });
+    B.rowptr[(size_t)n] = (int)kept[(size_t)T];
+    size_for_fill(B.colind, (size_t)kept[(size_t)T]);
+    size_for_fill(B.val, (size_t)kept[(size_t)T]);
+    run_parts(T, [&](int t) {
+        for (int r = ob[(size_t)t]; r < ob[(size_t)t + 1]; ++r) {
+            const int d = B.rowptr[(size_t)r], m = B.rowptr[(size_t)r + 1] - d, b = bp[(size_t)r];
+            std::copy(bc.begin() + b, bc.begin() + b + m, B.colind.begin() + d);
+            std::copy(bv.begin() + b, bv.begin() + b + m, B.val.begin() + d);
+        }
+    });
+    return B;
+}
+
 CRS permute_ptap_lower(const CRS& A, const std::vector<int>& new_of_old)
 {
     const int n = A.n;
     if ((int)new_of_old.size() != n) throw Error(ICCG_ERR_ARG, "Permute_PtAP: new_of_old size mismatch");
     if ((int)A.rowptr.size() != n + 1) throw Error(ICCG_ERR_ARG, "Permute_PtAP: A.rowptr size mismatch");
-    std::vector<int> cnt((size_t)n + 1, 0);
-    for (int i = 0; i < n; ++i) {
-        const int ip = new_of_old[(size_t)i];
-        for (int k = A.rowptr[(size_t)i]; k < A.rowptr[(size_t)i + 1]; ++k) {
-            const int j = A.colind[(size_t)k];
-            if (j > i) continue;
-            const int jp = new_of_old[(size_t)j];
-            cnt[(size_t)std::max(ip, jp) + 1]++;
-        }
-    }
-    for (int r = 0; r < n; ++r) cnt[(size_t)r + 1] += cnt[(size_t)r];
-    const size_t m = (size_t)cnt[(size_t)n];
-    std::vector<int> bc(m);
-    std::vector<double> bv(m);
-    {
-        std::vector<int> cur(cnt.begin(), cnt.end() - 1);
-        for (int i = 0; i < n; ++i) {
-            const int ip = new_of_old[(size_t)i];
-            for (int k = A.rowptr[(size_t)i]; k < A.rowptr[(size_t)i + 1]; ++k) {
-                const int j = A.colind[(size_t)k];
-                if (j > i) continue;
-                const int jp = new_of_old[(size_t)j];
-                const int r = std::max(ip, jp), c = std::min(ip, jp);
-                const int pos = cur[(size_t)r]++;
-                bc[(size_t)pos] = c;
-                bv[(size_t)pos] = A.val[(size_t)k];
-            }
-        }
-    }
-    CRS B;
-    B.n = n;
-    B.rowptr.assign((size_t)n + 1, 0);
-    B.colind.reserve(m);
-    B.val.reserve(m);
-    std::vector<std::pair<int, double>> tmp;
-    for (int r = 0; r < n; ++r) {
-        const int s = cnt[(size_t)r], e = cnt[(size_t)r + 1];
-        if (e > s) {
-            // stable insertion sort by column (rows are short)
-            for (int t = s + 1; t < e; ++t) {
-                int c = bc[(size_t)t];
-                double v = bv[(size_t)t];
-                int u = t - 1;
-                while (u >= s && bc[(size_t)u] > c) { bc[(size_t)u + 1] = bc[(size_t)u]; bv[(size_t)u + 1] = bv[(size_t)u]; --u; }
-                bc[(size_t)u + 1] = c;
-                bv[(size_t)u + 1] = v;
-            }
-            int cur_c = bc[(size_t)s];
-            double acc = bv[(size_t)s];
-            for (int t = s + 1; t < e; ++t) {
-                if (bc[(size_t)t] == cur_c) {
-                    acc += bv[(size_t)t];
-                } else {
-                    if (acc != 0.0) { B.colind.push_back(cur_c); B.val.push_back(acc); }
-                    cur_c = bc[(size_t)t];
-                    acc = bv[(size_t)t];
-                }
-            }
-            if (acc != 0.0) { B.colind.push_back(cur_c); B.val.push_back(acc); }
-        }
-        B.rowptr[(size_t)r + 1] = (int)B.colind.size();
-    }
-    return B;
+    return permute_ptap_lower(n, A.rowptr.data(), A.colind.data(), A.val.data(), new_of_old.data());
 }
 
 // expand_lower_to_full (crs_io.cpp:163-227): diagonal once, (i,j) and (j,i)
 // for each off-diagonal; columns sorted per row.  Row i of the output is
-// (lower part of row i) followed by (transposed entries from rows k > i), and
-// both parts arrive already ascending, so a merge replaces the sort.
-CRS expand_lower_to_full(const CRS& L)
+// (lower part of row i) followed by (transposed entries from rows k > i); for
+// a lower, sorted input both arrive ascending and no row needs sorting.
+CRS expand_lower_to_full(int n, const int* rp, const int* ci, const double* v)
 {
-    const int n = L.n;
+    const int T = std::max(1, std::min(host_threads(n > 0 ? 2ll * rp[n] : 0), n));
+    const std::vector<int> parts = row_parts(n, rp, T);
+    check_indices(n, rp, ci, nullptr, parts, "expand_lower_to_full");
     CRS F;
     F.n = n;
-    std::vector<int> cnt((size_t)n + 1, 0);
-    for (int i = 0; i < n; ++i)
-        for (int k = L.rowptr[(size_t)i]; k < L.rowptr[(size_t)i + 1]; ++k) {
-            const int j = L.colind[(size_t)k];
-            cnt[(size_t)i + 1]++;
-            if (j != i) cnt[(size_t)j + 1]++;
-        }
-    for (int i = 0; i < n; ++i) cnt[(size_t)i + 1] += cnt[(size_t)i];
-    const size_t m = (size_t)cnt[(size_t)n];
-    F.rowptr = cnt;
-    F.colind.resize(m);
-    F.val.resize(m);
-    std::vector<int> cur(cnt.begin(), cnt.end() - 1);
-    for (int i = 0; i < n; ++i)
-        for (int k = L.rowptr[(size_t)i]; k < L.rowptr[(size_t)i + 1]; ++k) {
-            const int j = L.colind[(size_t)k];
-            const double v = L.val[(size_t)k];
-            const int p = cur[(size_t)i]++;
-            F.colind[(size_t)p] = j;
-            F.val[(size_t)p] = v;
-            if (j != i) {
-                const int q = cur[(size_t)j]++;
-                F.colind[(size_t)q] = i;
-                F.val[(size_t)q] = v;
+    scatter_rows(n, parts, [&](int i0, int i1, auto&& put) {
+        for (int i = i0; i < i1; ++i)
+            for (int k = rp[i]; k < rp[i + 1]; ++k) {
+                const int j = ci[k];
+                put(i, j, v[k]);
+                if (j != i) put(j, i, v[k]);
             }
-        }
+    }, F.rowptr, F.colind, F.val);
     // per-row stable sort by column (the reference's index sort)
-    std::vector<std::pair<int, double>> row;
-    for (int i = 0; i < n; ++i) {
-        const int s = F.rowptr[(size_t)i], e = F.rowptr[(size_t)i + 1];
-        bool sorted = true;
-        for (int t = s + 1; t < e; ++t)
-            if (F.colind[(size_t)t] < F.colind[(size_t)t - 1]) { sorted = false; break; }
-        if (sorted) continue;
-        row.clear();
-        for (int t = s; t < e; ++t) row.emplace_back(F.colind[(size_t)t], F.val[(size_t)t]);
-        std::stable_sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-        for (int t = s; t < e; ++t) { F.colind[(size_t)t] = row[(size_t)(t - s)].first; F.val[(size_t)t] = row[(size_t)(t - s)].second; }
-    }
+    std::vector<int> ob((size_t)T + 1);
+    for (int t = 0; t <= T; ++t) ob[(size_t)t] = (int)((long long)n * t / T);
+    std::vector<unsigned char> failed((size_t)T, 0);
+    run_parts(T, [&](int t) {
+        try {
+            std::vector<std::pair<int, double>> row;
+            for (int i = ob[(size_t)t]; i < ob[(size_t)t + 1]; ++i) {
+                const int s = F.rowptr[(size_t)i], e = F.rowptr[(size_t)i + 1];
+                bool sorted = true;
+                for (int q = s + 1; q < e; ++q)
+                    if (F.colind[(size_t)q] < F.colind[(size_t)q - 1]) { sorted = false; break; }
+                if (sorted) continue;
+                if (e - s <= 64) {
+                    sort_row_short(F.colind.data(), F.val.data(), s, e);
+                    continue;
+                }
+                row.clear();
+                for (int q = s; q < e; ++q) row.emplace_back(F.colind[(size_t)q], F.val[(size_t)q]);
+                std::stable_sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+                for (int q = s; q < e; ++q) {
+                    F.colind[(size_t)q] = row[(size_t)(q - s)].first;
+                    F.val[(size_t)q] = row[(size_t)(q - s)].second;
+                }
+            }
+        } catch (...) {
+            failed[(size_t)t] = 1;
+        }
+    });
+    for (int t = 0; t < T; ++t)
+        if (failed[(size_t)t]) throw Error(ICCG_ERR_NOMEM, "expand_lower_to_full: out of host memory");
     return F;
+}
+
+CRS expand_lower_to_full(const CRS& L)
+{
+    if ((int)L.rowptr.size() != L.n + 1) throw Error(ICCG_ERR_ARG, "expand_lower_to_full: rowptr size mismatch");
+    return expand_lower_to_full(L.n, L.rowptr.data(), L.colind.data(), L.val.data());
 }
 
 // BuildColorPtrRows_FromPermutationAndColor (color.cpp:164-197)

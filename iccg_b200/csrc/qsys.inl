@@ -19,7 +19,7 @@ static bool sell_build(iccg_ctx* c, const std::vector<std::pair<int, int>>& slic
     const QSys& Q = c->Q;
     const SellOrder order{(int)Q.q2r.size(), Q.q2r.data(), Q.r2q.data(), Q.unit_of.data(), Q.step_of.data()};
     if (!build_sell_layout(slices, rp.data(), ci.data(), src_map ? src_map->data() : nullptr, order, encode, M,
-                           layout_threads((long long)ci.size())))
+                           host_threads((long long)ci.size())))
         return false;
     M.ptr.upload(M.h_ptr.data(), M.h_ptr.size(), &c->dev_bytes, c->stream);
     M.col.upload(M.h_col.data(), M.h_col.size(), &c->dev_bytes, c->stream);

@@ -116,6 +116,50 @@ def test_permutations_and_ptap_match_oracle(seed):
         assert np.array_equal(a, b)
 
 
+def _unsorted_rows(n, seed):
+    """Rows in random order with repeated columns, entries on both sides of
+    the diagonal and a few rows longer than 64 entries."""
+    rng = np.random.default_rng(seed)
+    rp, ci = [0], []
+    for i in range(n):
+        row = list(rng.integers(0, n, int(rng.integers(0, 6)))) + [i]
+        if i % 37 == 5:
+            row += list(rng.integers(0, n, 90))
+        rng.shuffle(row)
+        ci += row
+        rp.append(len(ci))
+    v = rng.integers(-3, 4, len(ci)) / 2.0  # exact sums, some of them zero
+    return ib.CRS.from_arrays(n, rp, ci, v)
+
+
+@pytest.mark.parametrize("threads", ["1", "2", "3", "7"])
+def test_ptap_and_expand_match_oracle_on_every_thread_count(monkeypatch, threads):
+    # ICCG_HOST_THREADS forces the thread count, so small inputs take the
+    # multi-threaded passes too
+    monkeypatch.setenv("ICCG_HOST_THREADS", threads)
+    rng = np.random.default_rng(int(threads))
+    for A in (_random_sym(150, 0.05, 3, zeros=True), _unsorted_rows(400, int(threads)), pb.laplace3d_aniso(9)):
+        for p in (rng.permutation(A.n).astype(np.int32), np.arange(A.n, dtype=np.int32)):
+            L = ib.Permute_PtAP_LowerCRS_to_LowerCRS(A, p)
+            orp, oci, ov = ob.ptap_lower(A.n, A.rowptr, A.colind, A.val, p)
+            assert np.array_equal(L.rowptr, orp) and np.array_equal(L.colind, oci) and np.array_equal(L.val, ov)
+        for M in (L, A):
+            F = ib.expand_lower_to_full(M)
+            frp, fci, fv = ob.expand_lower_to_full(M.n, M.rowptr, M.colind, M.val)
+            assert np.array_equal(F.rowptr, frp) and np.array_equal(F.colind, fci) and np.array_equal(F.val, fv)
+
+
+def test_ptap_and_expand_reject_indices_out_of_range():
+    A = ib.CRS.from_arrays(3, [0, 1, 3, 4], [0, 0, 5, 2], [1.0, 1.0, 1.0, 1.0])
+    with pytest.raises(ib.IccgError) as e:
+        ib.expand_lower_to_full(A)
+    assert e.value.code == ib.ERR_ARG
+    B = ib.CRS.from_arrays(3, [0, 1, 3, 4], [0, 0, 1, 2], [1.0, 1.0, 1.0, 1.0])
+    with pytest.raises(ib.IccgError) as e:
+        ib.Permute_PtAP_LowerCRS_to_LowerCRS(B, np.array([0, 3, 1], np.int32))
+    assert e.value.code == ib.ERR_ARG
+
+
 def test_abmc_schedule_with_empty_block():
     # a block with no rows leaves -1 at the tail of blocks_of_color (block.cpp:141)
     blk = np.array([0, 0, 2, 2, 0], np.int32)
