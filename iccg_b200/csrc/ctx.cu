@@ -152,7 +152,7 @@ int iccg_matrix_upload(iccg_ctx* c, int n, const int* rowptr, const int* colind,
         SetupPhase all("upload");
         if (n <= 0 || !rowptr || !colind || !val) throw Error(ICCG_ERR_ARG, "bad matrix arguments");
         if (rowptr[0] != 0) throw Error(ICCG_ERR_ARG, "rowptr[0] must be 0");
-        SetupPhase* v = new SetupPhase("upload.validate");
+        std::optional<SetupPhase> v(std::in_place, "upload.validate");
         for (int i = 0; i < n; ++i) {
             if (rowptr[i + 1] < rowptr[i]) throw Error(ICCG_ERR_ARG, "rowptr must be nondecreasing");
             for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
@@ -161,7 +161,7 @@ int iccg_matrix_upload(iccg_ctx* c, int n, const int* rowptr, const int* colind,
                     throw Error(ICCG_ERR_ARG, "columns must be strictly ascending within each row");
             }
         }
-        delete v;
+        v.reset();
         drop_graph(c);
         const int nnz = rowptr[n];
         c->n = n;

@@ -50,7 +50,7 @@ static void build_ic0(iccg_ctx* c, double shift, bool auto_shift)
         SetupPhase t("ic0.pattern");
         build_factor_pattern(c, Lx0);
     }
-    SetupPhase* tf = new SetupPhase("ic0.factor");
+    std::optional<SetupPhase> tf(std::in_place, "ic0.factor");
     double max_aii = 0.0;
     for (int i = 0; i < c->n; ++i) max_aii = std::max(max_aii, std::fabs(Lx0[(size_t)F.dpos[(size_t)i]]));
     double s = shift;
@@ -76,7 +76,7 @@ static void build_ic0(iccg_ctx* c, double shift, bool auto_shift)
     }
     F.shift = s;
     CK(cudaStreamSynchronize(c->stream));
-    delete tf;
+    tf.reset();
     SetupPhase tsw("ic0.sweep_arrays");
     // sweep arrays
     F.dSp.upload(F.Sp.data(), F.Sp.size(), &c->dev_bytes, c->stream);
