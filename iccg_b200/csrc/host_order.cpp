@@ -448,6 +448,14 @@ void scatter_rows(int n_out, const std::vector<int>& parts, const Scan& scan, st
     });
 }
 
+// threads for scatter_rows over `entries` entries into n_out rows: each
+// thread holds n_out counters, so their total stays within twice the entries
+int scatter_threads(int n_out, long long entries)
+{
+    const long long cap = std::max(1ll, 2 * entries / std::max(1, n_out));
+    return (int)std::max(1ll, std::min({(long long)host_threads(entries), (long long)std::max(1, n_out), cap}));
+}
+
 // stable insertion sort of (col, val)[b, e) by column
 void sort_row_short(int* col, double* val, int b, int e)
 {
@@ -488,7 +496,7 @@ void check_indices(int n, const int* rp, const int* ci, const int* perm, const s
 // column, sums duplicate columns (in input order) and drops sums equal to 0.0.
 CRS permute_ptap_lower(int n, const int* rp, const int* ci, const double* v, const int* new_of_old)
 {
-    const int T = std::max(1, std::min(host_threads(n > 0 ? rp[n] : 0), n));
+    const int T = scatter_threads(n, n > 0 ? rp[n] : 0);
     const std::vector<int> parts = row_parts(n, rp, T);
     check_indices(n, rp, ci, new_of_old, parts, "Permute_PtAP");
     std::vector<int> bp, bc;
@@ -573,7 +581,7 @@ CRS permute_ptap_lower(const CRS& A, const std::vector<int>& new_of_old)
 // a lower, sorted input both arrive ascending and no row needs sorting.
 CRS expand_lower_to_full(int n, const int* rp, const int* ci, const double* v)
 {
-    const int T = std::max(1, std::min(host_threads(n > 0 ? 2ll * rp[n] : 0), n));
+    const int T = scatter_threads(n, n > 0 ? 2ll * rp[n] : 0);
     const std::vector<int> parts = row_parts(n, rp, T);
     check_indices(n, rp, ci, nullptr, parts, "expand_lower_to_full");
     CRS F;
