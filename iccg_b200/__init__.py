@@ -296,7 +296,9 @@ def Permute_PtAP_LowerCRS_to_LowerCRS(A: CRS, new_of_old) -> CRS:
     nnz = C.c_int()
     _check(lib().iccg_ptap_lower(A.n, _ptr(A.rowptr), _ptr(A.colind), _ptr(A.val), _ptr(p), cap,
                                  _ptr(rp), _ptr(ci), _ptr(v), C.byref(nnz)))
-    return CRS(A.n, rp, ci[: nnz.value].copy(), v[: nnz.value].copy())
+    # views of the leading entries: the result is short-lived (expanded to
+    # the full matrix next), so the unused tail is kept rather than copied
+    return CRS(A.n, rp, ci[: nnz.value], v[: nnz.value])
 
 
 def BuildColorPtrRows_FromPermutationAndColor(color, nc: int, new_of_old):
