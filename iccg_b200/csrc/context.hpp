@@ -184,6 +184,23 @@ struct QSys {
     }
 };
 
+// What a captured iteration graph was recorded for: a graph is replayed
+// only for a solve whose key equals it field by field (the graphs bake in
+// the system, its kernels and the x / b device pointers).
+struct GraphKey {
+    int sched_version = -1, factor_version = -1, storage = -1, rri = -1, use_q = -1, m = -1, pc_kind = -1,
+        sweep_kernel = -1;
+    const void* x = nullptr;
+    const void* b = nullptr;
+    bool operator==(const GraphKey& o) const
+    {
+        return sched_version == o.sched_version && factor_version == o.factor_version && storage == o.storage &&
+               rri == o.rri && use_q == o.use_q && m == o.m && pc_kind == o.pc_kind &&
+               sweep_kernel == o.sweep_kernel && x == o.x && b == o.b;
+    }
+    bool operator!=(const GraphKey& o) const { return !(*this == o); }
+};
+
 }  // namespace iccg
 
 struct iccg_ctx {
@@ -242,7 +259,8 @@ struct iccg_ctx {
         int kernels;
     };
     std::vector<GraphEntry> graphs;
-    long long gkey = -1;
+    bool gkey_valid = false;
+    iccg::GraphKey gkey;
     // events
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evs[2] = {nullptr, nullptr};
     // profiling

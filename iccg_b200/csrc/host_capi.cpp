@@ -33,12 +33,17 @@ int guarded(F&& f)
 }
 
 // the argument checks of wrap() without its copy
-static void check_crs(int n, const int* rowptr, const int* colind, const double* val)
+static void check_crs(int n, const int* rowptr, const int* colind, const double* val, bool need_val = true)
 {
     if (n < 0 || !rowptr) throw Error(ICCG_ERR_ARG, "bad CRS arguments");
     const int nnz = rowptr[n];
     if (nnz < 0 || rowptr[0] != 0) throw Error(ICCG_ERR_ARG, "bad rowptr");
-    if (nnz > 0 && (!colind || !val)) throw Error(ICCG_ERR_ARG, "null colind/val");
+    // every row range inside [0, nnz]: the routines below read colind[k] for
+    // k in [rowptr[i], rowptr[i+1])
+    for (int i = 0; i < n; ++i)
+        if (rowptr[i + 1] < rowptr[i] || rowptr[i + 1] > nnz)
+            throw Error(ICCG_ERR_ARG, "rowptr must be nondecreasing and end at nnz");
+    if (nnz > 0 && (!colind || (need_val && !val))) throw Error(ICCG_ERR_ARG, "null colind/val");
 }
 
 // a result matrix into the caller's arrays, on host threads
@@ -173,6 +178,8 @@ int iccg_ptap_lower(int n, const int* rowptr, const int* colind, const double* v
 int iccg_expand_lower_nnz(int n, const int* rowptr, const int* colind, int* out_nnz)
 {
     return guarded([&] {
+        if (!out_nnz) throw iccg::Error(ICCG_ERR_ARG, "null out_nnz");
+        iccg::check_crs(n, rowptr, colind, nullptr, false);
         long long nz = 0;
         for (int i = 0; i < n; ++i)
             for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) nz += (colind[k] == i) ? 1 : 2;

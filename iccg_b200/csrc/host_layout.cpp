@@ -102,47 +102,57 @@ void build_ic0_layout(int n, const int* rp, const int* ci, const double* val, Ic
         }
     });
 
-    // columns of L (its CSC): the entries of column j lie in rows i >= j, so
-    // the part owning columns [c0, c1) scans rows c0..n-1, in row order
+    // columns of L (its CSC), by row parts: part u counts, per column, the
+    // entries of its rows; a column's entries from part u follow those of
+    // the parts before it, so every column lists its rows in ascending order,
+    // as a single scan of the rows would.  Each part holds n counters, so the
+    // parts are capped at about twice the entries per column.
     size_for_fill(L.Up, (size_t)n + 1);
     size_for_fill(L.Tp, (size_t)n + 1);
+    const int TU = (int)std::max(1ll, std::min<long long>(T, 2ll * nnzL / std::max(1, n)));
+    const std::vector<int> ub = row_parts(n, L.Lp.data(), TU);
+    std::vector<std::vector<int>> at((size_t)TU);
+    run_parts(TU, [&](int u) {
+        std::vector<int>& c = at[(size_t)u];
+        c.assign((size_t)n, 0);
+        for (int k = L.Lp[(size_t)ub[(size_t)u]]; k < L.Lp[(size_t)ub[(size_t)u + 1]]; ++k) ++c[(size_t)L.Li[(size_t)k]];
+    });
     std::vector<long long> su((size_t)T + 1, 0), st((size_t)T + 1, 0);
     run_parts(T, [&](int t) {
-        const int c0 = cb[(size_t)t], c1 = cb[(size_t)t + 1];
-        std::fill(L.Up.begin() + c0, L.Up.begin() + c1, 0);
-        for (int k = L.Lp[(size_t)c0]; k < nnzL; ++k) {
-            const int j = L.Li[(size_t)k];
-            if (j >= c0 && j < c1) ++L.Up[(size_t)j];
-        }
         long long s = 0;
-        for (int j = c0; j < c1; ++j) s += L.Up[(size_t)j];
+        for (int j = cb[(size_t)t]; j < cb[(size_t)t + 1]; ++j)
+            for (int u = 0; u < TU; ++u) s += at[(size_t)u][(size_t)j];
         su[(size_t)t + 1] = s;
     });
     scan_parts(su);
-    std::vector<int> next((size_t)n);
+    // each part's count becomes the slot of its first entry in the column
     run_parts(T, [&](int t) {
         int a = (int)su[(size_t)t];
         for (int j = cb[(size_t)t]; j < cb[(size_t)t + 1]; ++j) {
-            const int c = L.Up[(size_t)j];
-            L.Up[(size_t)j] = next[(size_t)j] = a;
-            a += c;
+            L.Up[(size_t)j] = a;
+            for (int u = 0; u < TU; ++u) {
+                const int c = at[(size_t)u][(size_t)j];
+                at[(size_t)u][(size_t)j] = a;
+                a += c;
+            }
         }
     });
     L.Up[(size_t)n] = nnzL;
     size_for_fill(L.Ui, (size_t)nnzL);
     size_for_fill(L.ut_src, (size_t)nnzL);
+    run_parts(TU, [&](int u) {
+        std::vector<int>& next = at[(size_t)u];
+        for (int i = ub[(size_t)u]; i < ub[(size_t)u + 1]; ++i)
+            for (int k = L.Lp[(size_t)i]; k < L.Lp[(size_t)i + 1]; ++k) {
+                const int p = next[(size_t)L.Li[(size_t)k]]++;
+                L.Ui[(size_t)p] = i;
+                L.ut_src[(size_t)p] = k;
+            }
+    });
+    std::vector<std::vector<int>>().swap(at);
     run_parts(T, [&](int t) {
         const int c0 = cb[(size_t)t], c1 = cb[(size_t)t + 1];
         if (c0 >= c1) return;
-        for (int i = c0; i < n; ++i)
-            for (int k = L.Lp[(size_t)i]; k < L.Lp[(size_t)i + 1]; ++k) {
-                const int j = L.Li[(size_t)k];
-                if (j >= c0 && j < c1) {
-                    const int p = next[(size_t)j]++;
-                    L.Ui[(size_t)p] = i;
-                    L.ut_src[(size_t)p] = k;
-                }
-            }
         // rows of L^T: the strictly upper entries of each column
         long long s = 0;
         for (int j = c0; j < c1; ++j) {

@@ -130,11 +130,69 @@ std::string lower(std::string s)
     return s;
 }
 
+// true if some (row, column) occurs three or more times in the entry list
+bool has_triple_entry(int nrows, const std::vector<int>& I, const std::vector<int>& J)
+{
+    const size_t m = I.size();
+    std::vector<int> cnt((size_t)nrows + 1, 0);
+    for (size_t t = 0; t < m; ++t) cnt[(size_t)I[t] + 1]++;
+    for (int r = 0; r < nrows; ++r) cnt[(size_t)r + 1] += cnt[(size_t)r];
+    std::vector<int> cols(m);
+    {
+        std::vector<int> cur(cnt.begin(), cnt.end() - 1);
+        for (size_t t = 0; t < m; ++t) cols[(size_t)cur[(size_t)I[t]]++] = J[t];
+    }
+    for (int r = 0; r < nrows; ++r) {
+        int* s = cols.data() + cnt[(size_t)r];
+        int* e = cols.data() + cnt[(size_t)r + 1];
+        if (e - s < 3) continue;
+        std::sort(s, e);
+        for (int* q = s + 2; q < e; ++q)
+            if (q[0] == q[-2]) return true;
+    }
+    return false;
+}
+
+// coo_to_crs (crs_io.cpp:19-70) step for step: one std::sort of the entry
+// indices by (row, column) with the reference's comparator, then the
+// duplicates of each (row, column) summed in the order the sort left them.
+// The same libstdc++ std::sort on the same sequence and comparator makes
+// the same moves, so triples are summed in the reference's order.
+CRS coo_to_crs_like_reference(int nrows, const std::vector<int>& I, const std::vector<int>& J,
+                              const std::vector<double>& V)
+{
+    const size_t nnz = I.size();
+    std::vector<size_t> ord(nnz);
+    std::iota(ord.begin(), ord.end(), (size_t)0);
+    std::sort(ord.begin(), ord.end(), [&](size_t a, size_t b) {
+        if (I[a] != I[b]) return I[a] < I[b];
+        return J[a] < J[b];
+    });
+    CRS A;
+    A.n = nrows;
+    A.rowptr.assign((size_t)nrows + 1, 0);
+    A.colind.reserve(nnz);
+    A.val.reserve(nnz);
+    for (size_t idx = 0; idx < nnz;) {
+        const int r = I[ord[idx]], c = J[ord[idx]];
+        double s = 0.0;
+        do {
+            s += V[ord[idx]];
+            ++idx;
+        } while (idx < nnz && I[ord[idx]] == r && J[ord[idx]] == c);
+        A.colind.push_back(c);
+        A.val.push_back(s);
+        A.rowptr[(size_t)r + 1]++;
+    }
+    for (int i = 0; i < nrows; ++i) A.rowptr[(size_t)i + 1] += A.rowptr[(size_t)i];
+    return A;
+}
+
 }  // namespace
 
 // read_matrix_market_crs (crs_io.cpp:73-159) with coo_to_crs (crs_io.cpp:19-70).
 // Same accepted formats and error cases; parsing is a single pass over the
-// file in memory.  Duplicate entries are summed in file order.
+// file in memory.  Duplicate entries are summed in the reference's order.
 CRS read_matrix_market_crs(const std::string& path)
 {
     std::string buf = slurp(path);
@@ -195,10 +253,15 @@ CRS read_matrix_market_crs(const std::string& path)
         if (sym && i != j) push(j, i, v);
     }
     // COO -> CRS: bucket by row (stable), sort each row by column (stable),
-    // sum duplicates in order.
+    // sum duplicates in order.  Two entries of one (row, column) sum to the
+    // same double in either order; three or more may not, and the reference
+    // sums them in the order its std::sort over the whole entry list leaves
+    // them (crs_io.cpp:27-45; introsort does not keep input order), so that
+    // case is redone with the same call.
     CRS A;
     A.n = nrows;
     const size_t m = I.size();
+    if (has_triple_entry(nrows, I, J)) return coo_to_crs_like_reference(nrows, I, J, V);
     std::vector<int> cnt((size_t)nrows + 1, 0);
     for (size_t t = 0; t < m; ++t) cnt[(size_t)I[t] + 1]++;
     for (int r = 0; r < nrows; ++r) cnt[(size_t)r + 1] += cnt[(size_t)r];
@@ -473,6 +536,27 @@ void sort_row_short(int* col, double* val, int b, int e)
     }
 }
 
+// Sorts (col, val)[b, e) by column as the reference's per-row std::sort of
+// (column, value) pairs does (color.cpp:111-112): up to 16 entries that
+// sort is an insertion sort, which keeps equal columns in input order (the
+// routine above); longer rows go through the same std::sort call on the
+// same sequence, so equal columns end in the reference's order and a long
+// row costs O(m log m).
+void sort_row_like_reference(int* col, double* val, int b, int e, std::vector<std::pair<int, double>>& tmp)
+{
+    if (e - b <= 16) {
+        sort_row_short(col, val, b, e);
+        return;
+    }
+    tmp.resize((size_t)(e - b));
+    for (int q = b; q < e; ++q) tmp[(size_t)(q - b)] = {col[q], val[q]};
+    std::sort(tmp.begin(), tmp.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+    for (int q = b; q < e; ++q) {
+        col[q] = tmp[(size_t)(q - b)].first;
+        val[q] = tmp[(size_t)(q - b)].second;
+    }
+}
+
 void check_indices(int n, const int* rp, const int* ci, const int* perm, const std::vector<int>& parts,
                    const char* what)
 {
@@ -493,7 +577,8 @@ void check_indices(int n, const int* rp, const int* ci, const int* perm, const s
 
 // Permute_PtAP_LowerCRS_to_LowerCRS (color.cpp:66-141).  Uses only j <= i of
 // the input, folds each entry to (max(ip,jp), min(ip,jp)), sorts every row by
-// column, sums duplicate columns (in input order) and drops sums equal to 0.0.
+// column as the reference's std::sort does, sums duplicate columns in that
+// order and drops sums equal to 0.0.
 CRS permute_ptap_lower(int n, const int* rp, const int* ci, const double* v, const int* new_of_old)
 {
     const int T = scatter_threads(n, n > 0 ? rp[n] : 0);
@@ -520,11 +605,14 @@ CRS permute_ptap_lower(int n, const int* rp, const int* ci, const double* v, con
     std::vector<int> ob((size_t)T + 1);
     for (int t = 0; t <= T; ++t) ob[(size_t)t] = (int)((long long)n * t / T);
     std::vector<long long> kept((size_t)T + 1, 0);
+    std::vector<unsigned char> failed((size_t)T, 0);
     run_parts(T, [&](int t) {
+      try {
+        std::vector<std::pair<int, double>> tmp;
         long long s = 0;
         for (int r = ob[(size_t)t]; r < ob[(size_t)t + 1]; ++r) {
             const int b = bp[(size_t)r], e = bp[(size_t)r + 1];
-            sort_row_short(bc.data(), bv.data(), b, e);
+            sort_row_like_reference(bc.data(), bv.data(), b, e, tmp);
             int w = b;
             if (e > b) {
                 int cur_c = bc[(size_t)b];
@@ -544,7 +632,12 @@ CRS permute_ptap_lower(int n, const int* rp, const int* ci, const double* v, con
             s += w - b;
         }
         kept[(size_t)t + 1] = s;
+      } catch (...) {
+        failed[(size_t)t] = 1;
+      }
     });
+    for (int t = 0; t < T; ++t)
+        if (failed[(size_t)t]) throw Error(ICCG_ERR_NOMEM, "Permute_PtAP: out of host memory");
     scan_parts(kept);
     run_parts(T, [&](int t) {
         int a = (int)kept[(size_t)t];
@@ -594,26 +687,44 @@ CRS expand_lower_to_full(int n, const int* rp, const int* ci, const double* v)
                 if (j != i) put(j, i, v[k]);
             }
     }, F.rowptr, F.colind, F.val);
-    // per-row stable sort by column (the reference's index sort)
+    // per-row sort by column, as the reference's index sort (crs_io.cpp:
+    // 203-219): rows of up to 16 entries are insertion-sorted by that
+    // std::sort, which keeps equal columns in input order; a longer row with
+    // equal columns goes through the same std::sort call on the same index
+    // sequence, so its equal columns end in the reference's order; a row with
+    // distinct columns has one sorted order
     std::vector<int> ob((size_t)T + 1);
     for (int t = 0; t <= T; ++t) ob[(size_t)t] = (int)((long long)n * t / T);
     std::vector<unsigned char> failed((size_t)T, 0);
     run_parts(T, [&](int t) {
         try {
             std::vector<std::pair<int, double>> row;
+            std::vector<int> idx;
             for (int i = ob[(size_t)t]; i < ob[(size_t)t + 1]; ++i) {
                 const int s = F.rowptr[(size_t)i], e = F.rowptr[(size_t)i + 1];
-                bool sorted = true;
-                for (int q = s + 1; q < e; ++q)
-                    if (F.colind[(size_t)q] < F.colind[(size_t)q - 1]) { sorted = false; break; }
-                if (sorted) continue;
-                if (e - s <= 64) {
+                bool sorted = true, distinct = true;
+                for (int q = s + 1; q < e; ++q) {
+                    if (F.colind[(size_t)q] < F.colind[(size_t)q - 1]) sorted = false;
+                    if (F.colind[(size_t)q] == F.colind[(size_t)q - 1]) distinct = false;
+                }
+                if (sorted && (distinct || e - s <= 16)) continue;
+                if (e - s <= 16) {
                     sort_row_short(F.colind.data(), F.val.data(), s, e);
                     continue;
                 }
                 row.clear();
                 for (int q = s; q < e; ++q) row.emplace_back(F.colind[(size_t)q], F.val[(size_t)q]);
-                std::stable_sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+                if (distinct) {
+                    std::sort(row.begin(), row.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+                } else {
+                    idx.resize((size_t)(e - s));
+                    std::iota(idx.begin(), idx.end(), 0);
+                    std::sort(idx.begin(), idx.end(),
+                              [&](int a, int b) { return row[(size_t)a].first < row[(size_t)b].first; });
+                    std::vector<std::pair<int, double>> srt(idx.size());
+                    for (size_t k = 0; k < idx.size(); ++k) srt[k] = row[(size_t)idx[k]];
+                    row.swap(srt);
+                }
                 for (int q = s; q < e; ++q) {
                     F.colind[(size_t)q] = row[(size_t)(q - s)].first;
                     F.val[(size_t)q] = row[(size_t)(q - s)].second;

@@ -320,7 +320,7 @@ static void drop_graph(iccg_ctx* c)
     for (auto& g : c->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     c->graphs.clear();
-    c->gkey = -1;
+    c->gkey_valid = false;
 }
 
 static void solve_fused(iccg_ctx* c, const double* b, double* x, int max_iter, double tol, const iccg_solve_opts& o,
@@ -362,13 +362,21 @@ static void solve_fused(iccg_ctx* c, const double* b, double* x, int max_iter, d
     auto one_batch = [&](unsigned mk) {
         for (int it = 0; it < m; ++it) fused_iteration(c, storage, it < 32 && ((mk >> it) & 1u), b, x);
     };
-    const long long key = ((long long)c->sched_version << 24) ^ ((long long)c->factor_version << 36) ^
-                          ((long long)storage << 20) ^ ((long long)rri << 8) ^ ((long long)c->use_q << 18) ^
-                          ((long long)m << 4) ^ (long long)c->pc_kind ^ ((long long)(uintptr_t)x << 32) ^
-                          ((long long)(uintptr_t)b << 40) ^ ((long long)c->sweep_kernel << 50);
-    if (use_graph && c->gkey != key) {
+    GraphKey key;
+    key.sched_version = c->sched_version;
+    key.factor_version = c->factor_version;
+    key.storage = storage;
+    key.rri = rri;
+    key.use_q = c->use_q ? 1 : 0;
+    key.m = m;
+    key.pc_kind = c->pc_kind;
+    key.sweep_kernel = c->sweep_kernel;
+    key.x = x;
+    key.b = b;
+    if (use_graph && (!c->gkey_valid || c->gkey != key)) {
         drop_graph(c);
         c->gkey = key;
+        c->gkey_valid = true;
     }
     auto graph_for = [&](unsigned mk) -> iccg_ctx::GraphEntry& {
         for (auto& g : c->graphs)

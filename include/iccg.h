@@ -282,7 +282,10 @@ int iccg_dot_dev(iccg_ctx* ctx, int n, const double* a, const double* b, double*
    and clears its counter, synchronising `stream`); make it before any
    stream capture.  Calls that overlap in time on one device (two host
    threads, or two streams running concurrently) share the scratch and race:
-   serialise them. */
+   serialise them.  The scratch address found by that set-up is kept for the
+   life of the process: after cudaDeviceReset (or any teardown of the
+   device's primary context) the library's device image is loaded anew, and
+   this entry point must not be called on that device again. */
 #define ICCG_NOALLOC_MAX_N 16777216
 int iccg_dot_dev_noalloc(int n, const double* a, const double* b, double* out, void* stream);
 

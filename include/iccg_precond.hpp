@@ -43,24 +43,49 @@ public:
     GpuSystem(const GpuSystem&) = delete;
     GpuSystem& operator=(const GpuSystem&) = delete;
 
-    // IC0::apply's dispatch on the schedule (ic0.cpp:366-393)
+    // IC0::apply's dispatch on the schedule (ic0.cpp:366-393).  The
+    // schedule is sent to the device again whenever its contents differ from
+    // the last one sent: the same object refilled, or another object at a
+    // reused address, is not taken for the old schedule.  The check copies
+    // and compares the schedule's arrays (O(n) host work per call).
     template <class Sched>
     void set_schedule(const Sched* s)
     {
-        if (s == last_) return;
-        last_ = s;
-        if (!s || s->nc <= 0) {
-            check(iccg_schedule_none(ctx_), ctx_);
-        } else if (s->mode == Sched::ABMC_BLOCK && s->color_ptr_blk && s->blocks_of_color && s->block_ptr &&
-                   s->rows_of_block) {
+        std::vector<int> key;
+        int mode = 0;  // 0 none, 1 MC, 2 ABMC
+        if (s && s->nc > 0) {
+            if (s->mode == Sched::ABMC_BLOCK && s->color_ptr_blk && s->blocks_of_color && s->block_ptr &&
+                s->rows_of_block)
+                mode = 2;
+            else if (s->color_ptr && s->rows_of_color)
+                mode = 1;
+        }
+        key.push_back(mode);
+        if (mode == 1) {
+            key.push_back(s->nc);
+            key.insert(key.end(), s->color_ptr, s->color_ptr + s->nc + 1);
+            key.insert(key.end(), s->rows_of_color, s->rows_of_color + n_);
+        } else if (mode == 2) {
+            key.push_back(s->nc);
+            key.push_back(s->nb);
+            key.insert(key.end(), s->color_ptr_blk, s->color_ptr_blk + s->nc + 1);
+            key.insert(key.end(), s->blocks_of_color, s->blocks_of_color + s->nb);
+            key.insert(key.end(), s->block_ptr, s->block_ptr + s->nb + 1);
+            key.insert(key.end(), s->rows_of_block, s->rows_of_block + n_);
+        }
+        if (have_key_ && key == key_) return;
+        have_key_ = false;
+        if (mode == 2) {
             check(iccg_schedule_abmc(ctx_, s->nc, s->nb, s->color_ptr_blk, s->blocks_of_color, s->block_ptr,
                                      s->rows_of_block),
                   ctx_);
-        } else if (s->color_ptr && s->rows_of_color) {
+        } else if (mode == 1) {
             check(iccg_schedule_mc(ctx_, s->nc, s->color_ptr, s->rows_of_color), ctx_);
         } else {
             check(iccg_schedule_none(ctx_), ctx_);
         }
+        key_.swap(key);
+        have_key_ = true;
     }
     iccg_ctx* ctx() const { return ctx_; }
     int n() const { return n_; }
@@ -68,7 +93,8 @@ public:
 private:
     iccg_ctx* ctx_ = nullptr;
     int n_ = 0;
-    const void* last_ = reinterpret_cast<const void*>(1);
+    bool have_key_ = false;
+    std::vector<int> key_;  // mode, sizes and arrays of the schedule on the device
 };
 
 // Precond::apply over the device; z is resized like the reference does.

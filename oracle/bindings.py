@@ -137,6 +137,8 @@ def ref() -> Optional[C.CDLL]:
         "ref_crs_copy": (None, [_P, _P, _P, _P]),
         "ref_crs_free": (None, [_P]),
         "ref_read_assignment": (_I, [_I, C.c_char_p, _I, _P, C.POINTER(_I)]),
+        "ref_ptap_lower": (_P, [_I, _P, _P, _P, _P]),
+        "ref_expand_lower_to_full": (_P, [_I, _P, _P, _P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -412,6 +414,29 @@ def ref_read_mm(path):
     L.ref_crs_copy(h, _ptr(rp), _ptr(ci), _ptr(v))
     L.ref_crs_free(h)
     return n, rp, ci, v
+
+
+def _ref_crs_take(h):
+    L = ref()
+    if not h:
+        raise RuntimeError(L.ref_last_error().decode())
+    n, nnz = L.ref_crs_n(h), L.ref_crs_nnz(h)
+    rp, ci, v = np.zeros(n + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
+    L.ref_crs_copy(h, _ptr(rp), _ptr(ci), _ptr(v))
+    L.ref_crs_free(h)
+    return rp, ci, v
+
+
+def ref_ptap_lower(n, rowptr, colind, val, new_of_old):
+    """The reference's Permute_PtAP_LowerCRS_to_LowerCRS (color.cpp:66-141)."""
+    rp, ci, v, p = _i32(rowptr), _i32(colind), _f64(val), _i32(new_of_old)
+    return _ref_crs_take(ref().ref_ptap_lower(n, _ptr(rp), _ptr(ci), _ptr(v), _ptr(p)))
+
+
+def ref_expand_lower_to_full(n, rowptr, colind, val):
+    """The reference's expand_lower_to_full (crs_io.cpp:163-227)."""
+    rp, ci, v = _i32(rowptr), _i32(colind), _f64(val)
+    return _ref_crs_take(ref().ref_expand_lower_to_full(n, _ptr(rp), _ptr(ci), _ptr(v)))
 
 
 def ref_read_assignment(kind, path, n_expected):

@@ -20,6 +20,15 @@
  * this directory) and against the committed fixtures in tests/golden/ that
  * were produced from that build.
  *
+ * Known gap: where the reference sorts with std::sort (per PtAP row,
+ * color.cpp:111-112; per expanded row, crs_io.cpp:203-219; the whole COO
+ * list of the MatrixMarket reader, crs_io.cpp:27-30) this file keeps equal
+ * keys in input order.  libstdc++'s std::sort does the same for ranges of
+ * at most 16 elements (it insertion-sorts them) but not for longer ones, so
+ * a row of more than 16 entries that repeats a column (three or more times
+ * for the summing routines) can come out in a different order here.  Those
+ * inputs are checked against the compiled reference instead.
+ *
  * All functions return 0 on success or a negative error code; where the
  * reference throws std::runtime_error the restatement returns ORC_E*.
  */
@@ -130,7 +139,7 @@ int orc_perm_by_block_color(int n, const int* block_of_old, const int* block_col
 /* (color.cpp:123,132).  The output capacity must be >= the number of lower   */
 /* input entries; *out_nnz receives the actual count.                        */
 /* Ties between duplicate columns are summed in insertion order (the          */
-/* reference's std::sort is stable for rows of <= 16 entries).               */
+/* reference's std::sort keeps that order for rows of <= 16 entries only).   */
 /* ------------------------------------------------------------------------ */
 int orc_ptap_lower(int n, const int* rowptr, const int* colind, const double* val,
                    const int* new_of_old, int cap,

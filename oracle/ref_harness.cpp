@@ -285,6 +285,29 @@ void ref_crs_copy(void* h, int* rowptr, int* colind, double* val)
 }
 void ref_crs_free(void* h) { delete static_cast<CRS*>(h); }
 
+// Permute_PtAP_LowerCRS_to_LowerCRS (color.cpp:66-141) and
+// expand_lower_to_full (crs_io.cpp:163-227) themselves, on caller arrays;
+// the result is returned as a heap CRS handle (ref_crs_* accessors).
+void* ref_ptap_lower(int n, const int* rowptr, const int* colind, const double* val, const int* new_of_old)
+{
+    CRS* B = new CRS;
+    int rc = guarded([&] {
+        CRS A = make_crs(n, rowptr, colind, val);
+        std::vector<int> p(new_of_old, new_of_old + n);
+        *B = Permute_PtAP_LowerCRS_to_LowerCRS(A, p);
+    });
+    if (rc) { delete B; return nullptr; }
+    return B;
+}
+
+void* ref_expand_lower_to_full(int n, const int* rowptr, const int* colind, const double* val)
+{
+    CRS* B = new CRS;
+    int rc = guarded([&] { *B = expand_lower_to_full(make_crs(n, rowptr, colind, val)); });
+    if (rc) { delete B; return nullptr; }
+    return B;
+}
+
 // kind: 0 color file, 1 block file, 2 block-color file
 int ref_read_assignment(int kind, const char* path, int n_expected, int* out, int* k_out)
 {

@@ -17,6 +17,7 @@ Run from the repository root:  python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
+import os
 import sys
 from pathlib import Path
 
@@ -29,7 +30,8 @@ from oracle import bindings as ob  # noqa: E402
 import iccg_b200 as ib  # noqa: E402
 from iccg_b200 import problems as pb  # noqa: E402
 
-REF_DIR = Path("/root/reference")
+# the reference checkout: ICCG_REFERENCE_DIR, else `reference` beside the repository
+REF_DIR = Path(os.environ.get("ICCG_REFERENCE_DIR", str(ROOT.parent / "reference")))
 OUT = Path(__file__).resolve().parent
 VARIANT_ID = {"cg": 0, "dcg": 1, "iccg": 2, "piccg": 3, "abmc": 4}
 

@@ -611,3 +611,35 @@ def test_gpu_tiny_and_ragged_systems_match_oracle(which):
     res = ctx.solve(P.b_run, x, 10000, 1e-8, storage=ib.STORE_FP32)
     assert res.converged and res.true_rel_resid <= 1e-8
     ctx.close()
+
+
+@pytest.mark.parametrize("tiled", [False, True])
+def test_gpu_solve_dev_on_alternating_buffer_pairs(tiled):
+    """solve_dev straight on caller buffers (the untiled path passes b and x
+    to the captured iteration graphs as they are): alternating between two
+    (b, x) pairs must re-record the graphs for each pair, so every solve
+    writes its own x and matches the oracle's."""
+    torch = pytest.importorskip("torch")
+    P = pb.config_abmc_aniso(24, 16, "bfs", seed=0)
+    n = P.A_run.n
+    ic0, xo, ito, relo, cvo = _oracle_solve(P)
+    b2 = ib.gen_uniform(n, 77)
+    ic0b = ob.OracleIC0(n, P.A_run.rowptr, P.A_run.colind, P.A_run.val, 0.0)
+    xo2, ito2, _, _, _ = ob.cg(n, P.A_run.rowptr, P.A_run.colind, P.A_run.val, b2, np.zeros(n), 2, 10000, 1e-8,
+                               ic0b, P.sched)
+    ctx = _ctx_for(P.A_run, P.sched)
+    ctx.use_tiled(tiled)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    pairs = [(torch.from_numpy(P.b_run).cuda(), torch.zeros(n, dtype=torch.float64, device="cuda"), xo, ito),
+             (torch.from_numpy(b2).cuda(), torch.zeros(n, dtype=torch.float64, device="cuda"), xo2, ito2)]
+    for k in (0, 1, 0, 1):
+        bd, xd, want, it = pairs[k]
+        xd.zero_()
+        torch.cuda.synchronize()
+        res = ctx.solve_dev(bd.data_ptr(), xd.data_ptr(), 10000, 1e-8)
+        assert res.converged and abs(res.iters - it) <= 1
+        assert rel_err(xd.cpu().numpy(), want) <= X_TOL
+        # the other pair's x holds its own solution (or zeros), never this one
+        other = pairs[1 - k][1].cpu().numpy()
+        assert not other.any() or rel_err(other, want) > 1e-3
+    ctx.close()

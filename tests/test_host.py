@@ -132,21 +132,136 @@ def _unsorted_rows(n, seed):
     return ib.CRS.from_arrays(n, rp, ci, v)
 
 
+def _ties_in_long_rows(M):
+    """True if a row of more than 16 entries repeats a column.  The
+    reference sorts rows with std::sort, which keeps equal columns in input
+    order only for ranges of up to 16 entries (libstdc++ sorts those by
+    insertion); the oracle keeps input order always, so such rows are
+    checked against the compiled reference instead."""
+    for i in range(M.n):
+        c = M.colind[M.rowptr[i]:M.rowptr[i + 1]]
+        if len(c) > 16 and len(np.unique(c)) < len(c):
+            return True
+    return False
+
+
+def _same(F, arrays):
+    return all(np.array_equal(a, b) for a, b in zip((F.rowptr, F.colind, F.val), arrays))
+
+
 @pytest.mark.parametrize("threads", ["1", "2", "3", "7"])
 def test_ptap_and_expand_match_oracle_on_every_thread_count(monkeypatch, threads):
     # ICCG_HOST_THREADS forces the thread count, so small inputs take the
     # multi-threaded passes too
     monkeypatch.setenv("ICCG_HOST_THREADS", threads)
     rng = np.random.default_rng(int(threads))
+    have_ref = ob.ref() is not None
     for A in (_random_sym(150, 0.05, 3, zeros=True), _unsorted_rows(400, int(threads)), pb.laplace3d_aniso(9)):
         for p in (rng.permutation(A.n).astype(np.int32), np.arange(A.n, dtype=np.int32)):
             L = ib.Permute_PtAP_LowerCRS_to_LowerCRS(A, p)
-            orp, oci, ov = ob.ptap_lower(A.n, A.rowptr, A.colind, A.val, p)
-            assert np.array_equal(L.rowptr, orp) and np.array_equal(L.colind, oci) and np.array_equal(L.val, ov)
+            assert _same(L, ob.ptap_lower(A.n, A.rowptr, A.colind, A.val, p))
+            if have_ref:
+                assert _same(L, ob.ref_ptap_lower(A.n, A.rowptr, A.colind, A.val, p))
         for M in (L, A):
             F = ib.expand_lower_to_full(M)
-            frp, fci, fv = ob.expand_lower_to_full(M.n, M.rowptr, M.colind, M.val)
-            assert np.array_equal(F.rowptr, frp) and np.array_equal(F.colind, fci) and np.array_equal(F.val, fv)
+            if not _ties_in_long_rows(M):
+                assert _same(F, ob.expand_lower_to_full(M.n, M.rowptr, M.colind, M.val))
+            if have_ref:
+                assert _same(F, ob.ref_expand_lower_to_full(M.n, M.rowptr, M.colind, M.val))
+
+
+def _triple_row_input(n=40, row=30, reps=24, seed=0):
+    """A lower CRS whose row `row` gets, after P^T A P with the identity,
+    `reps` entries of one column whose sum depends on the order they are
+    added in (magnitudes 1e16 and 1), among other columns: a row longer than
+    16 entries with 3 or more duplicates."""
+    rng = np.random.default_rng(seed)
+    rp, ci, v = [0], [], []
+    for i in range(n):
+        cols = [i]
+        vals = [4.0]
+        if i == row:
+            for k in range(reps):
+                cols.append(3)
+                vals.append([1e16, 1.0, -1e16, 1.0, 3.0, -2.0][k % 6] * (1 + k // 6))
+            for c in rng.permutation(np.arange(5, row))[:12]:
+                cols.append(int(c))
+                vals.append(float(rng.standard_normal()))
+        order = rng.permutation(len(cols))
+        ci += [cols[k] for k in order]
+        v += [vals[k] for k in order]
+        rp.append(len(ci))
+    return ib.CRS.from_arrays(n, rp, ci, v)
+
+
+@pytest.mark.skipif(ob.ref() is None, reason="compiled reference not built (needs the reference checkout)")
+@pytest.mark.parametrize("seed", range(4))
+def test_duplicate_entries_in_long_rows_match_compiled_reference(seed, tmp_path):
+    """Three or more duplicates of one entry in a row longer than 16: the
+    reference sums them in the order its std::sort leaves them (color.cpp:
+    111-112 per PtAP row; crs_io.cpp:27-30 over the whole COO list of the
+    MatrixMarket reader).  PtAP, expand_lower_to_full and the reader must
+    give the compiled reference's bits."""
+    A = _triple_row_input(seed=seed)
+    for p in (np.arange(A.n, dtype=np.int32), np.random.default_rng(seed).permutation(A.n).astype(np.int32)):
+        L = ib.Permute_PtAP_LowerCRS_to_LowerCRS(A, p)
+        assert _same(L, ob.ref_ptap_lower(A.n, A.rowptr, A.colind, A.val, p))
+    F = ib.expand_lower_to_full(A)
+    assert _same(F, ob.ref_expand_lower_to_full(A.n, A.rowptr, A.colind, A.val))
+    # the reader: a general file listing one entry many times among others
+    rng = np.random.default_rng(seed)
+    lines = []
+    for k in range(60):
+        lines.append((7, 5, [1e16, 1.0, -1e16, 1.0, 3.0, -2.0][k % 6] * (1 + k // 6)))
+    for k in range(200):
+        lines.append((int(rng.integers(1, 21)), int(rng.integers(1, 21)), float(rng.standard_normal())))
+    rng.shuffle(lines)
+    path = tmp_path / "dups.mtx"
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real general\n")
+        f.write(f"20 20 {len(lines)}\n")
+        for i, j, x in lines:
+            f.write(f"{i} {j} {x!r}\n")
+    mine = ib.read_matrix_market_crs(str(path))
+    assert _same(mine, ob.ref_read_mm(path)[1:])
+
+
+def test_ptap_long_dense_row_is_not_quadratic():
+    """One row of 100 000 entries in reverse column order: the per-row sort
+    is O(m log m), as the reference's std::sort is."""
+    import time
+    n = 100_001
+    rp = np.zeros(n + 1, np.int64)
+    ci, v = [], []
+    for i in range(n - 1):
+        ci.append(i)
+        v.append(4.0)
+        rp[i + 1] = len(ci)
+    last = n - 1
+    ci += list(range(last, -1, -1))
+    v += [1.0] * (last) + [4.0]
+    v[-1 - last] = 4.0
+    rp[n] = len(ci)
+    A = ib.CRS.from_arrays(n, rp.astype(np.int32), np.array(ci, np.int32), np.array(v))
+    # the long row stays the last row; its columns arrive in random order
+    p = np.concatenate([np.random.default_rng(1).permutation(n - 1), [n - 1]]).astype(np.int32)
+    t0 = time.perf_counter()
+    L = ib.Permute_PtAP_LowerCRS_to_LowerCRS(A, p)
+    dt = time.perf_counter() - t0
+    assert dt < 5.0, dt
+    assert L.rowptr[-1] == 2 * n - 1
+    o = ob.ptap_lower(A.n, A.rowptr, A.colind, A.val, p)
+    assert _same(L, o)
+
+
+def test_ptap_and_expand_reject_decreasing_rowptr():
+    A = ib.CRS.from_arrays(3, [0, 2, 1, 3], [0, 0, 1], [1.0, 1.0, 1.0])
+    with pytest.raises(ib.IccgError) as e:
+        ib.expand_lower_to_full(A)
+    assert e.value.code == ib.ERR_ARG
+    with pytest.raises(ib.IccgError) as e:
+        ib.Permute_PtAP_LowerCRS_to_LowerCRS(A, np.array([0, 1, 2], np.int32))
+    assert e.value.code == ib.ERR_ARG
 
 
 def test_ptap_and_expand_reject_indices_out_of_range():
