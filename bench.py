@@ -429,6 +429,8 @@ def main():
                     help="set up the workload, then launch only this operation --reps times "
                          "(FP32 storage) and print its mean device time; for profilers")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--persist", type=int, choices=[0, 1], default=1,
+                    help="1: each IC(0) apply as one persistent launch (the default); 0: one launch per level")
     ap.add_argument("--workload", choices=["abmc128", "batched", "serving", "diffusion27", "poisson2d"],
                     default="abmc128",
                     help="abmc128: the headline solve (default); batched: many uneven systems with 4 "
@@ -808,6 +810,7 @@ def run_kernel_only(args):
     ctx.upload(P.A_run)
     ctx.set_schedule(P.sched)
     ctx.build(ib.PRECOND_IC0, 0.0)
+    ctx.set_option(ib.OPT_PERSIST, args.persist)
     dev = torch.device("cuda", 0)
     a = torch.from_numpy(ib.gen_uniform(n, 5)).to(dev)
     b = torch.zeros(n, dtype=torch.float64, device=dev)
@@ -829,7 +832,8 @@ def run_kernel_only(args):
         rc = fn(ctx.h, ib.C.c_void_p(a.data_ptr()), ib.C.c_void_p(b.data_ptr()), ib.STORE_FP32)
         ms.append((time.perf_counter() - t0) * 1e3)
         assert rc == 0, L.iccg_ctx_last_error(ctx.h)
-    print(json.dumps({"kernel_only": args.kernel_only, "reps": args.reps, "host_ms": ms}))
+    print(json.dumps({"kernel_only": args.kernel_only, "reps": args.reps, "host_ms": ms,
+                      "sweep_plan_fp32_fwd": ctx.sweep_plan(ib.STORE_FP32, True)[:4]}))
     ctx.close()
 
 

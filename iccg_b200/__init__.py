@@ -54,6 +54,7 @@ OPT_SWEEP = 1
 OPT_PDL = 2
 OPT_STAGE_KB = 3
 OPT_STAGE_BUFS = 4
+OPT_PERSIST = 5
 STATUS_NAMES = {0: "converged", 1: "breakdown", 2: "max_iter", 3: "nonfinite"}
 
 
@@ -579,7 +580,7 @@ class Context:
         self._ck(lib().iccg_profile_read(self.h, cls, C.byref(ms), C.byref(n)))
         return ms.value, n.value
 
-    SWEEP_KINDS = ("chain", "staged", "two_phase", "one_phase", "csr")
+    SWEEP_KINDS = ("chain", "staged", "two_phase", "one_phase", "csr", "persistent")
 
     def sweep_plan(self, storage: int = STORE_FP64, fwd: bool = True):
         """[(kind name, CTAs)] per level of the IC(0) sweep in that direction."""

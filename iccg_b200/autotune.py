@@ -36,8 +36,8 @@ from typing import Callable, Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
 
-from . import (CRS, MODE_FUSED, OPT_PDL, OPT_STAGE_BUFS, OPT_STAGE_KB, OPT_SWEEP, PRECOND_IC0, STORE_FP32,
-               Context)
+from . import (CRS, MODE_FUSED, OPT_PDL, OPT_PERSIST, OPT_STAGE_BUFS, OPT_STAGE_KB, OPT_SWEEP, PRECOND_IC0,
+               STORE_FP32, Context)
 from .problems import Problem, make
 
 # (variant, block size, blocking) candidates: multicolor, and ABMC with 8, 16,
@@ -49,12 +49,14 @@ ORDERINGS: Tuple[Tuple[str, int, str], ...] = (("piccg", 0, "bfs"), ("abmc", 8, 
 
 # option -> candidate values, in the order they are tried (the first is the default)
 KERNEL_OPTIONS: Tuple[Tuple[int, Tuple[int, ...]], ...] = (
+    (OPT_PERSIST, (0, 1)),
     (OPT_SWEEP, (0, 1)),
     (OPT_STAGE_BUFS, (1, 2)),
     (OPT_STAGE_KB, (0, 160, 112, 80)),
     (OPT_PDL, (1, 0)),
 )
-OPTION_NAMES = {OPT_SWEEP: "sweep", OPT_STAGE_BUFS: "stage_bufs", OPT_STAGE_KB: "stage_kb", OPT_PDL: "pdl"}
+OPTION_NAMES = {OPT_PERSIST: "persist", OPT_SWEEP: "sweep", OPT_STAGE_BUFS: "stage_bufs", OPT_STAGE_KB: "stage_kb",
+                OPT_PDL: "pdl"}
 
 
 @dataclass

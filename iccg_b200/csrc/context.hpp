@@ -8,6 +8,7 @@
 
 #include "devbuf.hpp"
 #include "kernels.cuh"
+#include "persist.cuh"
 
 namespace iccg {
 
@@ -81,6 +82,39 @@ struct SellDev : SellLayout {
     }
 };
 
+// The persistent IC(0) apply (persist.cuh): its work items, their
+// dependencies, and per launch configuration the ticket counter, done
+// flags and reduction slots.
+struct PersistVar {
+    Buf<PCtl> ctl;
+    Buf<unsigned int> flags;
+    Buf<dd> slot;
+    int grid = 0;
+    size_t smem = 0;
+    bool ready = false;
+};
+
+struct PersistPlan {
+    bool ok = false;
+    bool used = false;   // launched since the error word was last read
+    int nitems = 0;
+    size_t smem[2] = {0, 0};  // dynamic shared memory per CTA: [0] FP64, [1] FP32
+    long long ndeps = 0;
+    Buf<int> dep_ptr, dep_idx;
+    Buf<unsigned int> err;
+    PersistVar var[8];
+    void reset()
+    {
+        ok = used = false;
+        nitems = 0;
+        smem[0] = smem[1] = 0;
+        ndeps = 0;
+        dep_ptr.free();
+        dep_idx.free();
+        for (auto& v : var) v.ready = false;
+    }
+};
+
 // The lane-interleaved device system.
 struct QSys {
     bool ok = false;
@@ -113,6 +147,7 @@ struct QSys {
     // ([0] FP64, [1] FP32)
     bool staged = false;
     Buf<BatchDesc> bdesc;
+    std::vector<BatchDesc> h_bdesc;                       // the batches, host copy (persistent apply plan)
     std::vector<int> lb;                                  // first batch of each level (nlevels + 1)
     std::vector<int> st_rows, st_slotsS, st_slotsT, st_slices;
     std::vector<int> st_fit;                              // 1: the level's batches fit the stage budget
@@ -129,8 +164,10 @@ struct QSys {
     Buf<double> d64, inv_diag;
     Buf<float> d32;
     bool d32_ok = false;
+    PersistPlan pp;
     void reset()
     {
+        pp.reset();
         ok = false;
         version = factor_version = -1;
         q2r.clear();
@@ -163,6 +200,7 @@ struct QSys {
         b2nslots = 0;
         staged = false;
         bdesc.free();
+        h_bdesc.clear();
         lb.clear();
         for (auto* v : {&st_rows, &st_slotsS, &st_slotsT, &st_slices, &st_fit, &chainS, &chainT}) v->clear();
         for (int k = 0; k < 2; ++k) {
@@ -232,6 +270,7 @@ struct iccg_ctx {
     int stage_kb = 0;       // ICCG_OPT_STAGE_KB: staged-sweep buffer budget (0: the opt-in maximum)
     int stage_bufs = 1;     // ICCG_OPT_STAGE_BUFS: staged-sweep buffers per CTA (1 or 2)
     int smem_optin = 0;     // largest dynamic shared memory per CTA
+    bool persist = false;   // ICCG_OPT_PERSIST: the IC(0) apply as one persistent launch where planned
     iccg::QSys Q;
     // preconditioner
     int pc_kind = -1;
@@ -268,6 +307,6 @@ struct iccg_ctx {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
     size_t ev_used = 0;
     std::vector<int> ev_cls;
-    double prof_ms[5] = {0, 0, 0, 0, 0};
-    long long prof_n[5] = {0, 0, 0, 0, 0};
+    double prof_ms[6] = {0, 0, 0, 0, 0, 0};
+    long long prof_n[6] = {0, 0, 0, 0, 0, 0};
 };

@@ -26,6 +26,7 @@ extern thread_local std::string g_host_err;  // host_capi.cpp
 #include "plan.inl"
 #include "factor.inl"
 #include "qsys.inl"
+#include "persist.inl"
 #include "solver.inl"
 
 template <class F>
@@ -129,6 +130,8 @@ int iccg_ctx_set_option(iccg_ctx* c, int option, long long value)
             c->sweep_kernel = (int)value;
         } else if (option == ICCG_OPT_PDL) {
             c->pdl = value != 0;
+        } else if (option == ICCG_OPT_PERSIST) {
+            c->persist = value != 0;
         } else if (option == ICCG_OPT_STAGE_BUFS) {
             if (value != 1 && value != 2) throw Error(ICCG_ERR_ARG, "ICCG_OPT_STAGE_BUFS takes 1 or 2");
             c->stage_bufs = (int)value;
@@ -138,6 +141,7 @@ int iccg_ctx_set_option(iccg_ctx* c, int option, long long value)
             if (c->Q.two_phase && !c->Q.steps.empty()) {
                 CK(cudaStreamSynchronize(c->stream));
                 plan_staged(c);
+                build_persist(c);
             }
         } else {
             throw Error(ICCG_ERR_ARG, "unknown option");
@@ -375,7 +379,7 @@ int iccg_profile_enable(iccg_ctx* c, int enable)
 {
     return guard(c, [&] {
         c->profile = enable != 0;
-        for (int k = 0; k < 5; ++k) {
+        for (int k = 0; k < 6; ++k) {
             c->prof_ms[k] = 0.0;
             c->prof_n[k] = 0;
         }
@@ -384,7 +388,7 @@ int iccg_profile_enable(iccg_ctx* c, int enable)
 
 int iccg_profile_read(iccg_ctx* c, int cls, double* total_ms, long long* launches)
 {
-    if (!c || cls < 0 || cls >= 5) return ICCG_ERR_ARG;
+    if (!c || cls < 0 || cls >= 6) return ICCG_ERR_ARG;
     if (total_ms) *total_ms = c->prof_ms[cls];
     if (launches) *launches = c->prof_n[cls];
     return ICCG_OK;
@@ -409,6 +413,16 @@ int iccg_sweep_plan(iccg_ctx* c, int storage, int fwd, int* kinds, int* grids, i
             return;
         }
         *nlevels = c->Q.nlevels;
+        if (use_persist(c, storage)) {
+            // every level in the one persistent launch
+            const PersistVar& V = f32 ? persist_var<float, false, FIN_NONE>(c, 4 + PK_PLAIN)
+                                      : persist_var<double, false, FIN_NONE>(c, PK_PLAIN);
+            for (int l = 0; l < std::min(cap, c->Q.nlevels); ++l) {
+                kinds[l] = 5;
+                grids[l] = V.grid;
+            }
+            return;
+        }
         for (int l = 0; l < std::min(cap, c->Q.nlevels); ++l) {
             const SweepLevel s = f32 ? sweep_level<float>(c, l, fwd != 0) : sweep_level<double>(c, l, fwd != 0);
             kinds[l] = s.kind;

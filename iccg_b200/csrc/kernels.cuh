@@ -43,7 +43,8 @@ struct SolverState {
     int rr_interval;  // 0: FP64 path, no replacement
     int rr_flag;      // replacement requested by the update step
     int n_rr;
-    int pad;
+    int pend;         // a stop decided by the persistent apply's own reductions (kRunning: none);
+                      // the p update that follows the apply moves it into `status`
     unsigned int ticket;
     unsigned int pad2;
 };
@@ -81,14 +82,18 @@ __device__ __forceinline__ bool st_done(const SolverState* st)
     return st != nullptr && *(volatile const int*)&st->status != kRunning;
 }
 
-// CG scalar logic of cg_crs.cpp:108-159, run by one thread.
-template <int FIN>
+// CG scalar logic of cg_crs.cpp:108-159, run by one thread.  With DEFER a
+// stop is recorded in st->pend instead of st->status: the persistent apply
+// (persist.cuh) gates every warp on st->status, which must not change while
+// it runs, so its own reductions defer their decisions to the p update.
+template <int FIN, bool DEFER = false>
 __device__ void finish(const double* v, SolverState* st, double* out)
 {
     if (FIN == FIN_STORE) {
         out[0] = v[0];
         return;
     }
+    int& status = DEFER ? st->pend : st->status;
     if (FIN == FIN_INIT) {
         double normb = sqrt(v[0]);
         if (normb == 0.0) normb = 1.0;
@@ -96,8 +101,8 @@ __device__ void finish(const double* v, SolverState* st, double* out)
         double rel = sqrt(v[1]) / normb;
         st->rel_resid = rel;
         st->iters = 0;
-        if (rel < st->tol) st->status = kConverged;
-        else if (st->max_iter <= 0) st->status = kMaxIter;
+        if (rel < st->tol) status = kConverged;
+        else if (st->max_iter <= 0) status = kMaxIter;
         return;
     }
     if (FIN == FIN_RZ0) {
@@ -110,12 +115,12 @@ __device__ void finish(const double* v, SolverState* st, double* out)
         const double thr = eps * sqrt(v[1]) * sqrt(v[2]);
         if (pAp <= thr) {
             st->iters = st->k;
-            st->status = kBreakdown;
+            status = kBreakdown;
             return;
         }
         if (!isfinite(pAp)) {
             st->iters = st->k;
-            st->status = kNonFinite;
+            status = kNonFinite;
             return;
         }
         st->alpha = st->rz_old / pAp;
@@ -125,11 +130,11 @@ __device__ void finish(const double* v, SolverState* st, double* out)
         const double rel = sqrt(v[0]) / st->normb;
         st->iters = st->k + 1;
         st->rel_resid = rel;
-        if (!isfinite(rel)) { st->status = kNonFinite; return; }
+        if (!isfinite(rel)) { status = kNonFinite; return; }
         if (st->rr_interval <= 0) {
-            if (rel < st->tol) st->status = kConverged;
+            if (rel < st->tol) status = kConverged;
         } else if (rel < st->tol) {
-            st->status = kTrueCheck;
+            status = kTrueCheck;
         } else if ((st->k + 1) % st->rr_interval == 0) {
             st->rr_flag = 1;
         }
@@ -140,14 +145,14 @@ __device__ void finish(const double* v, SolverState* st, double* out)
         st->rel_resid = rel;
         st->rr_flag = 0;
         st->n_rr += 1;
-        if (rel < st->tol) st->status = kConverged;
+        if (rel < st->tol) status = kConverged;
         return;
     }
     if (FIN == FIN_RZ) {
         const double rz = v[0];
         st->beta = rz / st->rz_old;
         st->rz_old = rz;
-        if (!isfinite(st->beta)) { st->status = kNonFinite; st->iters = st->k + 1; }
+        if (!isfinite(st->beta)) { status = kNonFinite; st->iters = st->k + 1; }
         return;
     }
 }
@@ -333,6 +338,14 @@ __global__ void __launch_bounds__(256) k_xpay(int n, double beta_arg, const doub
                                               double* __restrict__ p, SolverState* st)
 {
     grid_dep_begin();
+    if (st) {
+        // a stop the persistent apply deferred: make it the solve's status
+        const int pd = *(volatile const int*)&st->pend;
+        if (pd != kRunning) {
+            if (blockIdx.x == 0 && threadIdx.x == 0 && st->status == kRunning) st->status = pd;
+            return;
+        }
+    }
     if (st_done(st)) return;
     const double beta = st ? st->beta : beta_arg;
     if ((((uintptr_t)z | (uintptr_t)p) & 15) != 0) {
@@ -372,6 +385,7 @@ __global__ void k_resume_true_check(SolverState* st)
     grid_dep_begin();
     if (st->status == kTrueCheck) {
         st->status = kRunning;
+        st->pend = kRunning;
         st->rr_flag = 1;
     }
 }
@@ -706,15 +720,24 @@ __device__ __forceinline__ double fold_ext_global(double a, int pb, int j0, int 
     return a;
 }
 
+// An earlier-level value.  COH: written by other CTAs of the running launch
+// (the persistent apply), so read through L2 (ld.global.cg); otherwise read
+// only, through the read-only path.
+template <bool COH>
+__device__ __forceinline__ double ld_prev(const double* p)
+{
+    return COH ? __ldcg(p) : __ldg(p);
+}
+
 // ... or at e + 32 j of the staged slot arrays in shared memory
-template <int KT, class T>
+template <int KT, class T, bool COH = false>
 __device__ __forceinline__ double fold_ext_staged(double a, int e, int j0, int j1, const int* s_col, const T* s_val,
-                                                  const double* __restrict__ prev)
+                                                  const double* prev)
 {
     for (int jc = j0; jc < j1; jc += KT) {
         double x[KT];
 #pragma unroll
-        for (int u = 0; u < KT; ++u) x[u] = jc + u < j1 ? __ldg(prev + s_col[e + 32 * (jc + u)]) : 0.0;
+        for (int u = 0; u < KT; ++u) x[u] = jc + u < j1 ? ld_prev<COH>(prev + s_col[e + 32 * (jc + u)]) : 0.0;
 #pragma unroll
         for (int u = 0; u < KT; ++u)
             if (jc + u < j1) a = fma(-(double)s_val[e + 32 * (jc + u)], x[u], a);
@@ -724,14 +747,14 @@ __device__ __forceinline__ double fold_ext_staged(double a, int e, int j0, int j
 
 // the gathered values of entries [j0, j1), parked beside the staged entries
 // (the exact backward order applies them after the in-unit entries)
-template <int KT>
+template <int KT, bool COH = false>
 __device__ __forceinline__ void park_ext_staged(int e, int j0, int j1, const int* s_col, double* s_pv,
-                                                const double* __restrict__ prev)
+                                                const double* prev)
 {
     for (int jc = j0; jc < j1; jc += KT) {
         double x[KT];
 #pragma unroll
-        for (int u = 0; u < KT; ++u) x[u] = jc + u < j1 ? __ldg(prev + s_col[e + 32 * (jc + u)]) : 0.0;
+        for (int u = 0; u < KT; ++u) x[u] = jc + u < j1 ? ld_prev<COH>(prev + s_col[e + 32 * (jc + u)]) : 0.0;
 #pragma unroll
         for (int u = 0; u < KT; ++u)
             if (jc + u < j1) s_pv[e + 32 * (jc + u)] = x[u];
@@ -1004,7 +1027,9 @@ __device__ __forceinline__ int stage_range(unsigned char* dst, const void* src, 
     return first - a0;
 }
 
-template <class T, bool FWD, bool WITH_R>
+// STAGE_IN = false leaves the inputs to the caller (the persistent apply's
+// fused update writes them into the tile itself).
+template <class T, bool FWD, bool WITH_R, bool STAGE_IN = true>
 __device__ __forceinline__ void stage_batch(unsigned char* base, const StageLayout& Ly, const BatchDesc& d,
                                             const SliceMeta* meta, const SellMat& M, const T* dg,
                                             const double* in, const double* rdot)
@@ -1012,13 +1037,363 @@ __device__ __forceinline__ void stage_batch(unsigned char* base, const StageLayo
     const int rows = d.qe - d.qb;
     const int p0 = FWD ? d.ps0 : d.pt0, p1 = FWD ? d.ps1 : d.pt1;
     stage_range(base + Ly.meta, meta, 16, d.sb, d.se - d.sb);
-    stage_range(base + Ly.in, in, 8, d.qb, rows);
+    if (STAGE_IN) stage_range(base + Ly.in, in, 8, d.qb, rows);
     if (WITH_R) stage_range(base + Ly.rd, rdot, 8, d.qb, rows);
     stage_range(base + Ly.piv, dg, (int)sizeof(T), d.qb, rows);
     stage_range(base + Ly.len, M.len, 4, d.qb, rows);
     stage_range(base + Ly.col, M.col, 4, p0, p1 - p0);
     stage_range(base + Ly.val, M.val, (int)sizeof(T), p0, p1 - p0);
     cp_async_commit();
+}
+
+// Phase G of a staged batch (all threads): the earlier-level values of each
+// row's entries are gathered and folded into the row's partial sum in the
+// tile, or, for the exact backward order, parked beside the entries; each
+// row's in-unit entries (count, first two steps and values) are packed for
+// phase C.  COH reads the earlier-level values through L2 (the persistent
+// apply, where other CTAs of the launch wrote them).
+template <class T, bool FWD, bool EXACT, bool COH>
+__device__ __forceinline__ void st_gather(const BatchDesc& cur, unsigned char* base, const StageLayout& Ly,
+                                          int rows_cap, const double* prev)
+{
+    constexpr bool ext_first = FWD || !EXACT;
+    constexpr int UG = 2;  // slices per warp in flight in G
+    constexpr int KG = 4;  // earlier-level entries per row gathered at once
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const SliceMeta* s_meta = reinterpret_cast<const SliceMeta*>(base + Ly.meta);
+    double* s_in = reinterpret_cast<double*>(base + Ly.in) + (cur.qb & 1);
+    const double* s_rd = reinterpret_cast<const double*>(base + Ly.rd) + (cur.qb & 1);
+    const T* s_piv = reinterpret_cast<const T*>(base + Ly.piv) + (cur.qb & (16 / (int)sizeof(T) - 1));
+    const int* s_len = reinterpret_cast<const int*>(base + Ly.len) + (cur.qb & 3);
+    const int* s_col = reinterpret_cast<const int*>(base + Ly.col);
+    const T* s_val = reinterpret_cast<const T*>(base + Ly.val);
+    double* s_pv = reinterpret_cast<double*>(base + Ly.pv);
+    int* s_iw = reinterpret_cast<int*>(base + Ly.iw);
+    T* s_iv = reinterpret_cast<T*>(base + Ly.iv);
+    const int p0 = FWD ? cur.ps0 : cur.pt0;
+    const int ns = cur.se - cur.sb;
+
+    // G, full batches (every slice 32 rows, so tile row rr is lane
+    // rr % 32 of slice rr / 32): rows tid + 256 k, straight-line code
+    // with predicated loads, RG rows of a thread in flight at once.
+    if (cur.flags & 4) {
+        constexpr int RG = 2;
+        const int nrows = ns * 32;
+        for (int rb = 0; rb < nrows; rb += 256 * RG) {
+            int rr[RG], e[RG], j0[RG], j1[RG], ni[RG];
+            bool act[RG];
+            double xg[RG][KG];
+#pragma unroll
+            for (int k = 0; k < RG; ++k) {
+                rr[k] = rb + (int)threadIdx.x + 256 * k;
+                act[k] = rr[k] < nrows;
+                const SliceMeta m = s_meta[act[k] ? rr[k] >> 5 : 0];
+                const int lw = act[k] ? s_len[rr[k]] : 0;
+                const int L = lw & 0xffff;
+                ni[k] = lw >> 16;
+                e[k] = (FWD ? m.pS : m.pT) - p0 + (rr[k] & 31);
+                j0[k] = FWD ? 0 : ni[k];
+                j1[k] = FWD ? L - ni[k] : L;
+            }
+#pragma unroll
+            for (int k = 0; k < RG; ++k)
+#pragma unroll
+                for (int j = 0; j < KG; ++j) {
+                    const bool pj = j0[k] + j < j1[k];
+                    const int cj = s_col[pj ? e[k] + 32 * (j0[k] + j) : e[k]];
+                    xg[k][j] = pj ? ld_prev<COH>(prev + cj) : 0.0;
+                }
+#pragma unroll
+            for (int k = 0; k < RG; ++k) {
+                if (!act[k]) continue;
+                const int jin = FWD ? j1[k] : 0;
+                const int ea = ni[k] > 0 ? e[k] + 32 * jin : e[k];
+                const int eb = ni[k] > 1 ? e[k] + 32 * (jin + 1) : e[k];
+                const int ca = s_col[ea], cb = s_col[eb];
+                const T va = s_val[ea], vb = s_val[eb];
+                int w = ni[k] << 16;
+                w |= ni[k] > 0 ? -ca - 1 : 0;
+                w |= ni[k] > 1 ? (-cb - 1) << 8 : 0;
+                s_iw[rr[k]] = w;
+                s_iv[rr[k]] = ni[k] > 0 ? va : (T)0;
+                s_iv[rows_cap + rr[k]] = ni[k] > 1 ? vb : (T)0;
+                if (ext_first) {
+                    double a = s_in[rr[k]];
+#pragma unroll
+                    for (int j = 0; j < KG; ++j) {
+                        const bool pj = j0[k] + j < j1[k];
+                        const double v = (double)s_val[pj ? e[k] + 32 * (j0[k] + j) : e[k]];
+                        a = pj ? fma(-v, xg[k][j], a) : a;
+                    }
+                    a = fold_ext_staged<8, T, COH>(a, e[k], j0[k] + KG, j1[k], s_col, s_val, prev);
+                    s_in[rr[k]] = a;
+                } else {
+#pragma unroll
+                    for (int j = 0; j < KG; ++j)
+                        if (j0[k] + j < j1[k]) s_pv[e[k] + 32 * (j0[k] + j)] = xg[k][j];
+                    park_ext_staged<8, COH>(e[k], j0[k] + KG, j1[k], s_col, s_pv, prev);
+                }
+            }
+        }
+    } else
+    // G: earlier-level entries
+    for (int t0 = warp; t0 < ns; t0 += 8 * UG) {
+        int rr[UG], e[UG], j0[UG], j1[UG];
+        bool act[UG];
+#pragma unroll
+        for (int u = 0; u < UG; ++u) {
+            const int t = t0 + 8 * u;
+            act[u] = false;
+            rr[u] = e[u] = j0[u] = j1[u] = 0;
+            if (t < ns) {
+                const SliceMeta m = s_meta[t];
+                if (lane < (m.w & 63)) {
+                    act[u] = true;
+                    rr[u] = m.q0 - cur.qb + lane;
+                    const int lw = s_len[rr[u]];
+                    const int L = lw & 0xffff, ni = lw >> 16;
+                    e[u] = (FWD ? m.pS : m.pT) - p0 + lane;
+                    j0[u] = FWD ? 0 : ni;
+                    j1[u] = FWD ? L - ni : L;
+                }
+            }
+        }
+        double x[UG][KG];
+#pragma unroll
+        for (int u = 0; u < UG; ++u)
+#pragma unroll
+            for (int j = 0; j < KG; ++j)
+                x[u][j] = (act[u] && j0[u] + j < j1[u]) ? ld_prev<COH>(prev + s_col[e[u] + 32 * (j0[u] + j)]) : 0.0;
+        // in-unit entries of the row, for the chain: count and first two (step, value)
+#pragma unroll
+        for (int u = 0; u < UG; ++u) {
+            if (!act[u]) continue;
+            const int ni = FWD ? s_len[rr[u]] >> 16 : j0[u];
+            const int jin = FWD ? j1[u] : 0;
+            int w = ni << 16;
+            T v0 = (T)0, v1 = (T)0;
+            if (ni > 0) {
+                w |= -s_col[e[u] + 32 * jin] - 1;
+                v0 = s_val[e[u] + 32 * jin];
+            }
+            if (ni > 1) {
+                w |= (-s_col[e[u] + 32 * (jin + 1)] - 1) << 8;
+                v1 = s_val[e[u] + 32 * (jin + 1)];
+            }
+            s_iw[rr[u]] = w;
+            s_iv[rr[u]] = v0;
+            s_iv[rows_cap + rr[u]] = v1;
+        }
+#pragma unroll
+        for (int u = 0; u < UG; ++u) {
+            if (!act[u]) continue;
+            if (ext_first) {
+                double a = s_in[rr[u]];
+#pragma unroll
+                for (int j = 0; j < KG; ++j)
+                    if (j0[u] + j < j1[u]) a = fma(-(double)s_val[e[u] + 32 * (j0[u] + j)], x[u][j], a);
+                a = fold_ext_staged<8, T, COH>(a, e[u], j0[u] + KG, j1[u], s_col, s_val, prev);
+                s_in[rr[u]] = a;
+            } else {
+#pragma unroll
+                for (int j = 0; j < KG; ++j)
+                    if (j0[u] + j < j1[u]) s_pv[e[u] + 32 * (j0[u] + j)] = x[u][j];
+                park_ext_staged<8, COH>(e[u], j0[u] + KG, j1[u], s_col, s_pv, prev);
+            }
+        }
+    }
+}
+
+// Phase C of a staged batch, one warp per group and one lane per unit: the
+// in-unit chains, from the tile only; each result goes to out and stays in
+// the tile for the unit's later steps; r.z (WITH_R) is accumulated.  gl / gs:
+// this warp's groups' unit lengths and first slices (groups warp, warp + 8).
+template <class T, bool FWD, bool EXACT, bool WITH_R>
+__device__ __forceinline__ void st_chain(const BatchDesc& cur, unsigned char* base, const StageLayout& Ly,
+                                         int rows_cap, const int (&gl)[2], const int (&gs)[2], double* out,
+                                         acc2& rz)
+{
+    constexpr bool ext_first = FWD || !EXACT;
+    constexpr bool with_r = WITH_R;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const SliceMeta* s_meta = reinterpret_cast<const SliceMeta*>(base + Ly.meta);
+    double* s_in = reinterpret_cast<double*>(base + Ly.in) + (cur.qb & 1);
+    const double* s_rd = reinterpret_cast<const double*>(base + Ly.rd) + (cur.qb & 1);
+    const T* s_piv = reinterpret_cast<const T*>(base + Ly.piv) + (cur.qb & (16 / (int)sizeof(T) - 1));
+    const int* s_len = reinterpret_cast<const int*>(base + Ly.len) + (cur.qb & 3);
+    const int* s_col = reinterpret_cast<const int*>(base + Ly.col);
+    const T* s_val = reinterpret_cast<const T*>(base + Ly.val);
+    double* s_pv = reinterpret_cast<double*>(base + Ly.pv);
+    int* s_iw = reinterpret_cast<int*>(base + Ly.iw);
+    T* s_iv = reinterpret_cast<T*>(base + Ly.iv);
+    const int p0 = FWD ? cur.ps0 : cur.pt0;
+    (void)s_len;
+    (void)s_col;
+    (void)s_val;
+    (void)s_pv;
+    (void)p0;
+    // C, regular batches: every group has 32 units of one length and
+    // every in-unit entry is the row one step earlier in the sweep, so
+    // step r of a group is tile row base + 32 r and the chain is one
+    // fused multiply-add (selected by the row's in-unit count) and one
+    // division / product per step, with no branches.  (The exact
+    // backward order applies earlier-level entries inside the chain
+    // and takes the general path.)
+    if (ext_first && (cur.flags & (FWD ? 1 : 2))) {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int gi = warp + 8 * k;
+            if (gi >= cur.ng) break;
+            const int len = gl[k];
+            const int base = s_meta[gs[k] - cur.sb].q0 - cur.qb + lane;
+            double last = 0.0;
+            if constexpr (EXACT) {
+                // FP64: one step's tile words are loaded a step ahead,
+                // so the shared-memory latency stays off a chain whose
+                // steps end in a division (it only carries `last`)
+                struct Row {
+                    double a, rd;
+                    T iv, piv;
+                    int iw;
+                };
+                auto row = [&](int t) {
+                    const int rr = base + 32 * (FWD ? t : len - 1 - t);
+                    Row q;
+                    q.a = s_in[rr];
+                    q.iv = s_iv[rr];
+                    q.iw = s_iw[rr];
+                    q.piv = s_piv[rr];
+                    q.rd = with_r ? s_rd[rr] : 0.0;
+                    return q;
+                };
+                Row R = len > 0 ? row(0) : Row{};
+#pragma unroll 4
+                for (int t = 0; t < len; ++t) {
+                    const Row N = t + 1 < len ? row(t + 1) : R;
+                    const int rr = base + 32 * (FWD ? t : len - 1 - t);
+                    double a = R.a;
+                    const double x = fma(-(double)R.iv, last, a);
+                    a = (R.iw >> 16) ? x : a;
+                    const double v = a / (double)R.piv;
+                    out[cur.qb + rr] = v;
+                    if (with_r) acc2_fma(rz, R.rd, v);
+                    last = v;
+                    R = N;
+                }
+            } else {
+#pragma unroll 8
+                for (int t = 0; t < len; ++t) {
+                    const int rr = base + 32 * (FWD ? t : len - 1 - t);
+                    double a = s_in[rr];
+                    const double x = fma(-(double)s_iv[rr], last, a);
+                    a = (s_iw[rr] >> 16) ? x : a;
+                    const double v = EXACT ? a / (double)s_piv[rr] : a * (double)s_piv[rr];
+                    s_in[rr] = v;
+                    out[cur.qb + rr] = v;
+                    if (with_r) acc2_fma(rz, s_rd[rr], v);
+                    last = v;
+                }
+            }
+        }
+    } else {
+    // C, general batches: in-unit chains of any shape.  The steps'
+    // first Q rows sit in two registers per lane (steps lane and
+    // lane + 32, shuffled out).
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int gi = warp + 8 * k;
+        if (gi >= cur.ng) break;
+        const int len = gl[k];
+        const int sbase = gs[k] - cur.sb;
+        const int maxlen = (int)__reduce_max_sync(0xffffffffu, (unsigned)len);
+        const int qlo = lane < maxlen ? s_meta[sbase + lane].q0 - cur.qb : 0;
+        const int qhi = lane + 32 < maxlen ? s_meta[sbase + lane + 32].q0 - cur.qb : 0;
+        // row of step r for this lane; the shuffle needs the whole
+        // warp, so only warp-uniform code (fetch) may call it
+        auto row_of = [&](int r) {
+            const int q = __shfl_sync(0xffffffffu, r < 32 ? qlo : qhi, r & 31);
+            return q + lane;
+        };
+        // the same from the staged metadata, for per-lane code
+        auto row_at = [&](int r) { return s_meta[sbase + r].q0 - cur.qb + lane; };
+        double last = 0.0;
+        int lastr = -1;
+        struct Step {
+            int rr, w;
+            double a, rd, p, v0, v1;
+        };
+        auto fetch = [&](int t, Step& S) {
+            const int r = FWD ? t : maxlen - 1 - t;
+            S.rr = t < maxlen ? row_of(r) : 0;
+            if (t < maxlen && r < len) {
+                S.a = s_in[S.rr];
+                S.p = (double)s_piv[S.rr];
+                S.w = s_iw[S.rr];
+                S.v0 = (double)s_iv[S.rr];
+                S.v1 = (double)s_iv[rows_cap + S.rr];
+                if (with_r) S.rd = s_rd[S.rr];
+            }
+        };
+        // value of the unit's row at step idx: the register for the
+        // step just done, else the tile (a volatile load, so that it
+        // is only issued on the lanes and steps that need it and
+        // never sits in front of the chain)
+        auto unit_value = [&](int idx) {
+            double x = last;
+            if (idx != lastr) x = *reinterpret_cast<volatile const double*>(s_in + row_at(idx));
+            return x;
+        };
+        auto step = [&](int t, const Step& S) {
+            const int r = FWD ? t : maxlen - 1 - t;
+            if (r >= len) return;
+            double a = S.a;
+            const int ni = S.w >> 16;
+            if (ni > 0) a = fma(-S.v0, unit_value(S.w & 0xff), a);
+            if (ni > 1) a = fma(-S.v1, unit_value((S.w >> 8) & 0xff), a);
+            if (ni > 2 || !ext_first) {
+                // more in-unit entries, and the exact backward order's
+                // earlier-level entries: from the staged row
+                const SliceMeta m = s_meta[sbase + r];
+                const int L = s_len[S.rr] & 0xffff;
+                const int e0 = (FWD ? m.pS : m.pT) - p0 + lane;
+                const int jin = FWD ? L - ni : 0;
+                for (int k2 = 2; k2 < ni; ++k2) {
+                    const int ek = e0 + 32 * (jin + k2);
+                    a = fma(-(double)s_val[ek], unit_value(-s_col[ek] - 1), a);
+                }
+                if (!ext_first)
+                    for (int j = ni; j < L; ++j) {
+                        const int ej = e0 + 32 * j;
+                        a = fma(-(double)s_val[ej], s_pv[ej], a);
+                    }
+            }
+            const double v = EXACT ? a / S.p : a * S.p;
+            s_in[S.rr] = v;
+            out[cur.qb + S.rr] = v;
+            if (with_r) acc2_fma(rz, S.rd, v);
+            last = v;
+            lastr = r;
+        };
+        if constexpr (EXACT) {
+            // FP64: each step's tile words are fetched a step ahead
+            // (they are the row's own, never written by the steps
+            // before it)
+            Step A{}, B{};
+            fetch(0, A);
+            for (int t = 0; t < maxlen; ++t) {
+                if (t + 1 < maxlen) fetch(t + 1, B);
+                step(t, A);
+                A = B;
+            }
+        } else {
+            for (int t = 0; t < maxlen; ++t) {
+                Step A{};
+                fetch(t, A);
+                step(t, A);
+            }
+        }
+    }
+    }
 }
 
 template <class T, bool FWD, int FIN, bool EXACT, int NB = 2>
@@ -1032,10 +1407,7 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
     grid_dep_begin();
     if (st_done(st)) return;
     constexpr bool with_r = FIN != FIN_NONE;
-    constexpr bool ext_first = FWD || !EXACT;
-    constexpr bool with_pv = !ext_first;
-    constexpr int UG = 2;  // slices per warp in flight in G
-    constexpr int KG = 4;  // earlier-level entries per row gathered at once
+    constexpr bool with_pv = !(FWD || !EXACT);
     extern __shared__ __align__(16) unsigned char smem_st[];
     const StageLayout Ly = stage_layout(rows_cap, slots_cap, slices_cap, (int)sizeof(T), with_r, with_pv);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1072,312 +1444,10 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
             else cp_async_wait<0>();
             __syncthreads();
 
-            const SliceMeta* s_meta = reinterpret_cast<const SliceMeta*>(base + Ly.meta);
-            double* s_in = reinterpret_cast<double*>(base + Ly.in) + (cur.qb & 1);
-            const double* s_rd = reinterpret_cast<const double*>(base + Ly.rd) + (cur.qb & 1);
-            const T* s_piv = reinterpret_cast<const T*>(base + Ly.piv) + (cur.qb & (16 / (int)sizeof(T) - 1));
-            const int* s_len = reinterpret_cast<const int*>(base + Ly.len) + (cur.qb & 3);
-            const int* s_col = reinterpret_cast<const int*>(base + Ly.col);
-            const T* s_val = reinterpret_cast<const T*>(base + Ly.val);
-            double* s_pv = reinterpret_cast<double*>(base + Ly.pv);
-            int* s_iw = reinterpret_cast<int*>(base + Ly.iw);
-            T* s_iv = reinterpret_cast<T*>(base + Ly.iv);
-            const int p0 = FWD ? cur.ps0 : cur.pt0;
-            const int ns = cur.se - cur.sb;
-
-            // G, full batches (every slice 32 rows, so tile row rr is lane
-            // rr % 32 of slice rr / 32): rows tid + 256 k, straight-line code
-            // with predicated loads, RG rows of a thread in flight at once.
-            if (cur.flags & 4) {
-                constexpr int RG = 2;
-                const int nrows = ns * 32;
-                for (int rb = 0; rb < nrows; rb += 256 * RG) {
-                    int rr[RG], e[RG], j0[RG], j1[RG], ni[RG];
-                    bool act[RG];
-                    double xg[RG][KG];
-#pragma unroll
-                    for (int k = 0; k < RG; ++k) {
-                        rr[k] = rb + (int)threadIdx.x + 256 * k;
-                        act[k] = rr[k] < nrows;
-                        const SliceMeta m = s_meta[act[k] ? rr[k] >> 5 : 0];
-                        const int lw = act[k] ? s_len[rr[k]] : 0;
-                        const int L = lw & 0xffff;
-                        ni[k] = lw >> 16;
-                        e[k] = (FWD ? m.pS : m.pT) - p0 + (rr[k] & 31);
-                        j0[k] = FWD ? 0 : ni[k];
-                        j1[k] = FWD ? L - ni[k] : L;
-                    }
-#pragma unroll
-                    for (int k = 0; k < RG; ++k)
-#pragma unroll
-                        for (int j = 0; j < KG; ++j) {
-                            const bool pj = j0[k] + j < j1[k];
-                            const int cj = s_col[pj ? e[k] + 32 * (j0[k] + j) : e[k]];
-                            xg[k][j] = pj ? __ldg(prev + cj) : 0.0;
-                        }
-#pragma unroll
-                    for (int k = 0; k < RG; ++k) {
-                        if (!act[k]) continue;
-                        const int jin = FWD ? j1[k] : 0;
-                        const int ea = ni[k] > 0 ? e[k] + 32 * jin : e[k];
-                        const int eb = ni[k] > 1 ? e[k] + 32 * (jin + 1) : e[k];
-                        const int ca = s_col[ea], cb = s_col[eb];
-                        const T va = s_val[ea], vb = s_val[eb];
-                        int w = ni[k] << 16;
-                        w |= ni[k] > 0 ? -ca - 1 : 0;
-                        w |= ni[k] > 1 ? (-cb - 1) << 8 : 0;
-                        s_iw[rr[k]] = w;
-                        s_iv[rr[k]] = ni[k] > 0 ? va : (T)0;
-                        s_iv[rows_cap + rr[k]] = ni[k] > 1 ? vb : (T)0;
-                        if (ext_first) {
-                            double a = s_in[rr[k]];
-#pragma unroll
-                            for (int j = 0; j < KG; ++j) {
-                                const bool pj = j0[k] + j < j1[k];
-                                const double v = (double)s_val[pj ? e[k] + 32 * (j0[k] + j) : e[k]];
-                                a = pj ? fma(-v, xg[k][j], a) : a;
-                            }
-                            a = fold_ext_staged<8>(a, e[k], j0[k] + KG, j1[k], s_col, s_val, prev);
-                            s_in[rr[k]] = a;
-                        } else {
-#pragma unroll
-                            for (int j = 0; j < KG; ++j)
-                                if (j0[k] + j < j1[k]) s_pv[e[k] + 32 * (j0[k] + j)] = xg[k][j];
-                            park_ext_staged<8>(e[k], j0[k] + KG, j1[k], s_col, s_pv, prev);
-                        }
-                    }
-                }
-            } else
-            // G: earlier-level entries
-            for (int t0 = warp; t0 < ns; t0 += 8 * UG) {
-                int rr[UG], e[UG], j0[UG], j1[UG];
-                bool act[UG];
-#pragma unroll
-                for (int u = 0; u < UG; ++u) {
-                    const int t = t0 + 8 * u;
-                    act[u] = false;
-                    rr[u] = e[u] = j0[u] = j1[u] = 0;
-                    if (t < ns) {
-                        const SliceMeta m = s_meta[t];
-                        if (lane < (m.w & 63)) {
-                            act[u] = true;
-                            rr[u] = m.q0 - cur.qb + lane;
-                            const int lw = s_len[rr[u]];
-                            const int L = lw & 0xffff, ni = lw >> 16;
-                            e[u] = (FWD ? m.pS : m.pT) - p0 + lane;
-                            j0[u] = FWD ? 0 : ni;
-                            j1[u] = FWD ? L - ni : L;
-                        }
-                    }
-                }
-                double x[UG][KG];
-#pragma unroll
-                for (int u = 0; u < UG; ++u)
-#pragma unroll
-                    for (int j = 0; j < KG; ++j)
-                        x[u][j] = (act[u] && j0[u] + j < j1[u]) ? __ldg(prev + s_col[e[u] + 32 * (j0[u] + j)]) : 0.0;
-                // in-unit entries of the row, for the chain: count and first two (step, value)
-#pragma unroll
-                for (int u = 0; u < UG; ++u) {
-                    if (!act[u]) continue;
-                    const int ni = FWD ? s_len[rr[u]] >> 16 : j0[u];
-                    const int jin = FWD ? j1[u] : 0;
-                    int w = ni << 16;
-                    T v0 = (T)0, v1 = (T)0;
-                    if (ni > 0) {
-                        w |= -s_col[e[u] + 32 * jin] - 1;
-                        v0 = s_val[e[u] + 32 * jin];
-                    }
-                    if (ni > 1) {
-                        w |= (-s_col[e[u] + 32 * (jin + 1)] - 1) << 8;
-                        v1 = s_val[e[u] + 32 * (jin + 1)];
-                    }
-                    s_iw[rr[u]] = w;
-                    s_iv[rr[u]] = v0;
-                    s_iv[rows_cap + rr[u]] = v1;
-                }
-#pragma unroll
-                for (int u = 0; u < UG; ++u) {
-                    if (!act[u]) continue;
-                    if (ext_first) {
-                        double a = s_in[rr[u]];
-#pragma unroll
-                        for (int j = 0; j < KG; ++j)
-                            if (j0[u] + j < j1[u]) a = fma(-(double)s_val[e[u] + 32 * (j0[u] + j)], x[u][j], a);
-                        a = fold_ext_staged<8>(a, e[u], j0[u] + KG, j1[u], s_col, s_val, prev);
-                        s_in[rr[u]] = a;
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < KG; ++j)
-                            if (j0[u] + j < j1[u]) s_pv[e[u] + 32 * (j0[u] + j)] = x[u][j];
-                        park_ext_staged<8>(e[u], j0[u] + KG, j1[u], s_col, s_pv, prev);
-                    }
-                }
-            }
+            st_gather<T, FWD, EXACT, false>(cur, base, Ly, rows_cap, prev);
             __syncthreads();
 
-            // C, regular batches: every group has 32 units of one length and
-            // every in-unit entry is the row one step earlier in the sweep, so
-            // step r of a group is tile row base + 32 r and the chain is one
-            // fused multiply-add (selected by the row's in-unit count) and one
-            // division / product per step, with no branches.  (The exact
-            // backward order applies earlier-level entries inside the chain
-            // and takes the general path.)
-            if (ext_first && (cur.flags & (FWD ? 1 : 2))) {
-#pragma unroll
-                for (int k = 0; k < 2; ++k) {
-                    const int gi = warp + 8 * k;
-                    if (gi >= cur.ng) break;
-                    const int len = gl[k];
-                    const int base = s_meta[gs[k] - cur.sb].q0 - cur.qb + lane;
-                    double last = 0.0;
-                    if constexpr (EXACT) {
-                        // FP64: one step's tile words are loaded a step ahead,
-                        // so the shared-memory latency stays off a chain whose
-                        // steps end in a division (it only carries `last`)
-                        struct Row {
-                            double a, rd;
-                            T iv, piv;
-                            int iw;
-                        };
-                        auto row = [&](int t) {
-                            const int rr = base + 32 * (FWD ? t : len - 1 - t);
-                            Row q;
-                            q.a = s_in[rr];
-                            q.iv = s_iv[rr];
-                            q.iw = s_iw[rr];
-                            q.piv = s_piv[rr];
-                            q.rd = with_r ? s_rd[rr] : 0.0;
-                            return q;
-                        };
-                        Row R = len > 0 ? row(0) : Row{};
-#pragma unroll 4
-                        for (int t = 0; t < len; ++t) {
-                            const Row N = t + 1 < len ? row(t + 1) : R;
-                            const int rr = base + 32 * (FWD ? t : len - 1 - t);
-                            double a = R.a;
-                            const double x = fma(-(double)R.iv, last, a);
-                            a = (R.iw >> 16) ? x : a;
-                            const double v = a / (double)R.piv;
-                            out[cur.qb + rr] = v;
-                            if (with_r) acc2_fma(rz[0], R.rd, v);
-                            last = v;
-                            R = N;
-                        }
-                    } else {
-#pragma unroll 8
-                        for (int t = 0; t < len; ++t) {
-                            const int rr = base + 32 * (FWD ? t : len - 1 - t);
-                            double a = s_in[rr];
-                            const double x = fma(-(double)s_iv[rr], last, a);
-                            a = (s_iw[rr] >> 16) ? x : a;
-                            const double v = EXACT ? a / (double)s_piv[rr] : a * (double)s_piv[rr];
-                            s_in[rr] = v;
-                            out[cur.qb + rr] = v;
-                            if (with_r) acc2_fma(rz[0], s_rd[rr], v);
-                            last = v;
-                        }
-                    }
-                }
-            } else {
-            // C, general batches: in-unit chains of any shape.  The steps'
-            // first Q rows sit in two registers per lane (steps lane and
-            // lane + 32, shuffled out).
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const int gi = warp + 8 * k;
-                if (gi >= cur.ng) break;
-                const int len = gl[k];
-                const int sbase = gs[k] - cur.sb;
-                const int maxlen = (int)__reduce_max_sync(0xffffffffu, (unsigned)len);
-                const int qlo = lane < maxlen ? s_meta[sbase + lane].q0 - cur.qb : 0;
-                const int qhi = lane + 32 < maxlen ? s_meta[sbase + lane + 32].q0 - cur.qb : 0;
-                // row of step r for this lane; the shuffle needs the whole
-                // warp, so only warp-uniform code (fetch) may call it
-                auto row_of = [&](int r) {
-                    const int q = __shfl_sync(0xffffffffu, r < 32 ? qlo : qhi, r & 31);
-                    return q + lane;
-                };
-                // the same from the staged metadata, for per-lane code
-                auto row_at = [&](int r) { return s_meta[sbase + r].q0 - cur.qb + lane; };
-                double last = 0.0;
-                int lastr = -1;
-                struct Step {
-                    int rr, w;
-                    double a, rd, p, v0, v1;
-                };
-                auto fetch = [&](int t, Step& S) {
-                    const int r = FWD ? t : maxlen - 1 - t;
-                    S.rr = t < maxlen ? row_of(r) : 0;
-                    if (t < maxlen && r < len) {
-                        S.a = s_in[S.rr];
-                        S.p = (double)s_piv[S.rr];
-                        S.w = s_iw[S.rr];
-                        S.v0 = (double)s_iv[S.rr];
-                        S.v1 = (double)s_iv[rows_cap + S.rr];
-                        if (with_r) S.rd = s_rd[S.rr];
-                    }
-                };
-                // value of the unit's row at step idx: the register for the
-                // step just done, else the tile (a volatile load, so that it
-                // is only issued on the lanes and steps that need it and
-                // never sits in front of the chain)
-                auto unit_value = [&](int idx) {
-                    double x = last;
-                    if (idx != lastr) x = *reinterpret_cast<volatile const double*>(s_in + row_at(idx));
-                    return x;
-                };
-                auto step = [&](int t, const Step& S) {
-                    const int r = FWD ? t : maxlen - 1 - t;
-                    if (r >= len) return;
-                    double a = S.a;
-                    const int ni = S.w >> 16;
-                    if (ni > 0) a = fma(-S.v0, unit_value(S.w & 0xff), a);
-                    if (ni > 1) a = fma(-S.v1, unit_value((S.w >> 8) & 0xff), a);
-                    if (ni > 2 || !ext_first) {
-                        // more in-unit entries, and the exact backward order's
-                        // earlier-level entries: from the staged row
-                        const SliceMeta m = s_meta[sbase + r];
-                        const int L = s_len[S.rr] & 0xffff;
-                        const int e0 = (FWD ? m.pS : m.pT) - p0 + lane;
-                        const int jin = FWD ? L - ni : 0;
-                        for (int k2 = 2; k2 < ni; ++k2) {
-                            const int ek = e0 + 32 * (jin + k2);
-                            a = fma(-(double)s_val[ek], unit_value(-s_col[ek] - 1), a);
-                        }
-                        if (!ext_first)
-                            for (int j = ni; j < L; ++j) {
-                                const int ej = e0 + 32 * j;
-                                a = fma(-(double)s_val[ej], s_pv[ej], a);
-                            }
-                    }
-                    const double v = EXACT ? a / S.p : a * S.p;
-                    s_in[S.rr] = v;
-                    out[cur.qb + S.rr] = v;
-                    if (with_r) acc2_fma(rz[0], S.rd, v);
-                    last = v;
-                    lastr = r;
-                };
-                if constexpr (EXACT) {
-                    // FP64: each step's tile words are fetched a step ahead
-                    // (they are the row's own, never written by the steps
-                    // before it)
-                    Step A{}, B{};
-                    fetch(0, A);
-                    for (int t = 0; t < maxlen; ++t) {
-                        if (t + 1 < maxlen) fetch(t + 1, B);
-                        step(t, A);
-                        A = B;
-                    }
-                } else {
-                    for (int t = 0; t < maxlen; ++t) {
-                        Step A{};
-                        fetch(t, A);
-                        step(t, A);
-                    }
-                }
-            }
-            }
+            st_chain<T, FWD, EXACT, with_r>(cur, base, Ly, rows_cap, gl, gs, out, rz[0]);
             __syncthreads();
             if (!has_next) break;
             if (NB == 1) stage_batch<T, FWD, with_r>(smem_st, Ly, nxt, meta, M, dg, in, rdot);

@@ -9,6 +9,8 @@
 // levels and steps reversed, which is a valid order because every backward
 // dependency is a forward dependency reversed.
 
+static void build_persist(iccg_ctx* c);  // persist.inl
+
 // encode: 0 plain columns; 1 forward rows, 2 backward rows -- in-unit entries
 // become -(step + 1) and each row's length word carries their count in its
 // high half; returns false (and leaves plain columns) when a row's in-unit
@@ -354,6 +356,7 @@ static void plan_staged(iccg_ctx* c)
     if (!plan_staged_type<double>(c, 0) || !plan_staged_type<float>(c, 1)) return;
     Q.bdesc.upload(bds.data(), bds.size(), &c->dev_bytes, c->stream);
     CK(cudaStreamSynchronize(c->stream));
+    Q.h_bdesc.swap(bds);
     Q.staged = true;
 }
 
@@ -431,6 +434,7 @@ static void build_q_factor(iccg_ctx* c)
         Q.b2nslots = s;
         ensure_partials(c, (size_t)std::max(s, 1));
         plan_staged(c);
+        build_persist(c);
     }
     std::vector<int> dsrc((size_t)c->n);
     for (int q = 0; q < c->n; ++q) dsrc[(size_t)q] = F.dpos[(size_t)Q.q2r[(size_t)q]];
@@ -484,7 +488,7 @@ static void ensure_q32(iccg_ctx* c)
             CK(cudaStreamSynchronize(c->stream));
             Q.d32_ok = true;
         }
-        if (Q.staged && !Q.r32_ok) {
+        if ((Q.staged || Q.pp.ok) && !Q.r32_ok) {
             Q.r32.alloc((size_t)c->n, &c->dev_bytes);
             launch(c, 3, k_recip_f32, grid_for(c, c->n), kThreads, (long long)c->n, (const double*)Q.d64.get(),
                    Q.r32.get());

@@ -143,6 +143,10 @@ template <class T, int FIN>
 static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, SolverState* st)
 {
     QSys& Q = c->Q;
+    if (use_persist(c, std::is_same<T, float>::value ? ICCG_STORE_FP32 : ICCG_STORE_FP64)) {
+        launch_persist<T, false, FIN>(c, const_cast<double*>(r), y, z, st);
+        return;
+    }
     for (int l = 0; l < Q.nlevels; ++l)
         launch_sweep_level<T, FIN_NONE, true>(c, l, sweep_level<T>(c, l, true), r, y, nullptr, 0, 0, st);
     std::vector<SweepLevel> bl((size_t)Q.nlevels);
@@ -221,6 +225,10 @@ static void prepare_path(iccg_ctx* c, int storage)
     if (c->use_q) {
         ensure_q(c);
         if (storage == ICCG_STORE_FP32) ensure_q32(c);
+        if (use_persist(c, storage)) {
+            if (storage == ICCG_STORE_FP32) prepare_persist_t<float>(c);
+            else prepare_persist_t<double>(c);
+        }
     } else if (storage == ICCG_STORE_FP32) {
         ensure_val32(c);
         if (c->pc_kind == ICCG_PRECOND_IC0) ensure_factor32(c);
@@ -307,6 +315,13 @@ static void fused_iteration(iccg_ctx* c, int storage, bool rr, const double* b, 
     SolverState* st = c->state.get();
     RedBuf red{c->partials.get(), c->scalars.get()};
     spmv_path<FIN_PAP>(c, storage, (const double*)c->vp.get(), c->vAp.get(), st);
+    if (!rr && use_persist(c, storage)) {
+        // update, both sweeps and the two reductions in one launch
+        if (storage == ICCG_STORE_FP32) launch_persist<float, true, FIN_RZ>(c, c->vr.get(), c->vy.get(), c->vz.get(), st, x);
+        else launch_persist<double, true, FIN_RZ>(c, c->vr.get(), c->vy.get(), c->vz.get(), st, x);
+        launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st);
+        return;
+    }
     launch_n(c, 3, k_update<FIN_UPD>, (long long)c->n, n, 0.0, (const double*)c->vp.get(), (const double*)c->vAp.get(), x,
            c->vr.get(), st, red, c->ticket.get());
     if (rr) residual_path<FIN_TRUE>(c, (const double*)x, b, c->vr.get(), st);
@@ -332,6 +347,7 @@ static void solve_fused(iccg_ctx* c, const double* b, double* x, int max_iter, d
     SolverState s0{};
     s0.tol = tol;
     s0.status = kRunning;
+    s0.pend = kRunning;
     s0.max_iter = max_iter;
     s0.rr_interval = rr ? o.rr_interval : 0;
     *c->h_state = s0;
@@ -503,6 +519,7 @@ static void solve_dev(iccg_ctx* c, const double* b, double* x, int max_iter, dou
     CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     res->solve_ms = ms;
     collect_profile(c);
+    check_persist(c);
     // A converged FP32-storage solve ends on a residual replacement, whose
     // convergence test is already ||b - A x|| / ||b|| with the FP64 matrix.
     if (o.mode == ICCG_MODE_FUSED && o.storage == ICCG_STORE_FP32 && o.rr_interval > 0 && res->converged)
@@ -528,6 +545,7 @@ static void apply_dev(iccg_ctx* c, int storage, const double* r, double* z)
     }
     CK(cudaStreamSynchronize(c->stream));
     collect_profile(c);
+    check_persist(c);
 }
 
 static void spmv_dev(iccg_ctx* c, int storage, const double* x, double* y)

@@ -210,12 +210,20 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
    batch into a second buffer while the current one is worked on.  One
    buffer halves a CTA's shared memory, so twice as many CTAs share an SM
    and overlap each other's copies; on the 128^3 system that was faster.
-   Every choice gives the same bits with FP64 storage. */
+   Every choice gives the same bits with FP64 storage.
+   ICCG_OPT_PERSIST (default 0): 1 runs each IC(0) apply -- both
+   substitution sweeps, every level -- as one persistent launch in which
+   CTAs take the staged batches from a ticket counter and wait only for the
+   batches whose rows they read; in a fused solve the same launch also does
+   the CG update x += alpha p, r -= alpha Ap and r.r.  0 launches one kernel
+   per level (ICCG_OPT_SWEEP chooses which).  It applies where every level
+   is staged.  FP64 results are the same bits either way. */
 #define ICCG_OPT_TILED 0
 #define ICCG_OPT_SWEEP 1
 #define ICCG_OPT_PDL 2
 #define ICCG_OPT_STAGE_KB 3
 #define ICCG_OPT_STAGE_BUFS 4
+#define ICCG_OPT_PERSIST 5
 int iccg_ctx_set_option(iccg_ctx* ctx, int option, long long value);
 
 /* Uploads A_run (the matrix conjugate_gradient runs on, cg_crs.cpp:442-447):
@@ -299,7 +307,8 @@ int iccg_solve_dev(iccg_ctx* ctx, const double* b, double* x, int max_iter, doub
 
 /* per-kernel-class device time of the last solve run with profiling on:
    class 0 SpMV, 1 forward sweep, 2 backward sweep, 3 vector/reduction
-   kernels, 4 residual replacement.  enable != 0 brackets every launch of
+   kernels, 4 residual replacement, 5 persistent IC(0) apply (both sweeps,
+   and in a fused solve the CG update).  enable != 0 brackets every launch of
    the following solves with CUDA events (launches are not graphed then). */
 int iccg_profile_enable(iccg_ctx* ctx, int enable);
 int iccg_profile_read(iccg_ctx* ctx, int cls, double* total_ms, long long* launches);
@@ -308,7 +317,8 @@ int iccg_profile_read(iccg_ctx* ctx, int cls, double* total_ms, long long* launc
    on, for storage ICCG_STORE_FP64 / ICCG_STORE_FP32 and the forward (fwd != 0)
    or backward sweep: kinds[l] = 0 chain-only, 1 staged, 2 per-slice
    two-phase, 3 one-phase (units of more than 64 rows), 4 CSR (untiled
-   path); grids[l] = CTAs launched.  *nlevels receives the level count and
+   path), 5 the persistent apply (all levels in one launch); grids[l] =
+   CTAs launched.  *nlevels receives the level count and
    at most cap entries are written.  Sets up the FP32 copies on first use,
    as a solve would.  No counterpart in the reference (its sweeps have one
    OpenMP form, ic0.cpp:194-339). */

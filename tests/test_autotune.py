@@ -55,20 +55,24 @@ class FakeCtx:
 
 def test_tune_kernels_coordinate_search_leaves_best_options_set():
     ctx = FakeCtx()
-    # cost: per-slice sweeps faster, 112 KB stages best, PDL on better
+    # cost: the persistent apply faster, per-slice sweeps faster, 112 KB
+    # stages best, PDL on better
     def timer():
         o = ctx.opts
         ms = 10.0
+        ms -= 2.0 if o[ib.OPT_PERSIST] == 1 else 0.0
         ms -= 1.0 if o[ib.OPT_SWEEP] == 1 else 0.0
         ms -= {0: 0.0, 160: 0.2, 112: 0.5, 80: 0.3}[o[ib.OPT_STAGE_KB]]
         ms -= 0.4 if o[ib.OPT_PDL] == 1 else 0.0
         return ms, 50, True
 
     res = at.tune_kernels(ctx, np.zeros(4), timer=timer)
-    assert ctx.opts == {ib.OPT_SWEEP: 1, ib.OPT_STAGE_BUFS: 1, ib.OPT_STAGE_KB: 112, ib.OPT_PDL: 1}
+    assert ctx.opts == {ib.OPT_PERSIST: 1, ib.OPT_SWEEP: 1, ib.OPT_STAGE_BUFS: 1, ib.OPT_STAGE_KB: 112,
+                        ib.OPT_PDL: 1}
+    assert res.choice["persist"] == 1
     assert res.choice["sweep"] == 1 and res.choice["stage_kb"] == 112 and res.choice["pdl"] == 1
-    assert abs(res.choice["ms"] - (10.0 - 1.0 - 0.5 - 0.4)) < 1e-12
-    assert len(res.trials) == 2 + 2 + 4 + 2
+    assert abs(res.choice["ms"] - (10.0 - 2.0 - 1.0 - 0.5 - 0.4)) < 1e-12
+    assert len(res.trials) == 2 + 2 + 2 + 4 + 2
 
 
 def test_tune_kernels_skips_unconverged_settings():

@@ -38,7 +38,7 @@ def test_gpu_tune_kernels_keeps_fp64_bits():
     r0 = ctx.solve(P.b_run, x0, 10000, 1e-8, storage=ib.STORE_FP64)
     res = at.tune_kernels(ctx, P.b_run, storage=ib.STORE_FP32, reps=1)
     assert res.choice["sweep"] in (0, 1) and res.choice["stage_kb"] in (0, 160, 112, 80)
-    assert res.choice["pdl"] in (0, 1) and res.choice["stage_bufs"] in (1, 2)
+    assert res.choice["pdl"] in (0, 1) and res.choice["stage_bufs"] in (1, 2) and res.choice["persist"] in (0, 1)
     assert len(res.trials) == sum(len(v) for _, v in at.KERNEL_OPTIONS)
     x1 = np.zeros(P.A_run.n)
     r1 = ctx.solve(P.b_run, x1, 10000, 1e-8, storage=ib.STORE_FP64)
