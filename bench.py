@@ -462,66 +462,142 @@ def main():
         run_gpu(args)
 
 
-def run_batched(args):
-    """Many independent SPD systems of uneven size, 4 right-hand sides each.
-
-    The systems are drawn 50/50 from two families. One is a 2D 5-point
-    Poisson problem with side U{32..256}. The other is a 3D 7-point
-    Laplacian with side U{16..48}. Each gets multicolor IC(0), FP32 storage
-    of A and L, and FP64 recurrences. Every system stays resident, and
-    `--threads` of them solve at once, each on its own stream. The
-    comparison is the same solves one at a time on the plain FP64 path.
-    """
-    import torch
-    import iccg_b200 as ib
-    import iccg_b200.batch as bt
+def _batched_problems(count: int, seed: int = 4):
+    """The batched workload's systems: 50/50 a 2D 5-point Poisson problem with
+    side U{32..256} and a 3D 7-point Laplacian with side U{16..48}, greedy
+    multicolor each."""
     import iccg_b200.problems as pb
-    rng = np.random.default_rng(4)
-    t0 = time.perf_counter()
+    rng = np.random.default_rng(seed)
     probs = []
-    for i in range(args.systems):
+    for i in range(count):
         if rng.random() < 0.5:
             probs.append(pb.make(pb.poisson2d(int(rng.integers(32, 257))), "piccg", seed=i))
         else:
             probs.append(pb.make(pb.laplace3d_aniso(int(rng.integers(16, 49)), 1.0), "piccg", seed=i))
-    rhs = [[pb.with_rhs(P, seed=1000 * i + k).b_run.copy() for k in range(4)] for i, P in enumerate(probs)]
-    host_setup_s = time.perf_counter() - t0
+    return probs
+
+
+def batched_case(count: int, nrhs: int = 4, steps: int = 3, warmup: int = 1, device: int = 0,
+                 compare_streams: bool = True, sample: int = 32):
+    """All count x nrhs solves of the batched workload through the batched
+    engine (ib.Batch: one launch per CG step for every solve), FP32 A and L,
+    FP64 vectors and reductions, tol 1e-8.  Reports solves/s from the device
+    time (CUDA events) and end to end (host arrays in and out, wall clock),
+    per-solve latency percentiles (batch start to the solve's stop, device
+    clock), the algorithmic GB/s of the iterations, and the same solves one
+    at a time (fused mixed path per system, and plain FP64) on a sample."""
+    import iccg_b200 as ib
     t0 = time.perf_counter()
-    systems = [bt.ResidentSystem(P, storage=ib.STORE_FP32) for P in probs]
+    probs = _batched_problems(count)
+    import iccg_b200.problems as pb
+    rhs = [[pb.with_rhs(P, seed=1000 * i + k).b_run.copy() for k in range(nrhs)] for i, P in enumerate(probs)]
+    host_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ctxs = []
+    for P in probs:
+        c = ib.Context(device)
+        c.upload(P.A_run)
+        c.set_schedule(P.sched)
+        c.build(ib.PRECOND_IC0, 0.0)
+        ctxs.append(c)
+    B = ib.Batch(device)
+    for c in ctxs:
+        B.add_system(c)
     upload_s = time.perf_counter() - t0
-    # warm-up: one solve per system (graph capture, first-touch)
-    bt.solve_batch(systems, [[r[0]] for r in rhs], threads=args.threads)
-    torch.cuda.synchronize()
+    systems = [i for i in range(count) for _ in range(nrhs)]
+    bs = [rhs[i][k] for i in range(count) for k in range(nrhs)]
     t0 = time.perf_counter()
-    recs = bt.solve_batch(systems, rhs, threads=args.threads)
-    torch.cuda.synchronize()
-    wall = time.perf_counter() - t0
-    ok = all(r.converged and r.true_rel_resid <= 1e-8 for r in recs)
-    # one at a time, plain FP64, on a sample of the systems
-    sample = list(range(0, len(systems), max(1, len(systems) // 32)))
-    plain_ms = []
-    for i in sample:
-        s = bt.ResidentSystem(probs[i], storage=ib.STORE_FP64)
-        s.solve(rhs[i][0], mode=ib.MODE_PLAIN)
-        x, res, wms = s.solve(rhs[i][0], mode=ib.MODE_PLAIN)
-        plain_ms.append(wms)
-        s.close()
-    for s in systems:
-        s.close()
-    plain_per_s = 1000.0 / statistics.mean(plain_ms)
-    line = {"workload": "batched", "systems": len(systems), "rhs_per_system": 4, "solves": len(recs),
-            "all_converged_1e-8": ok, "threads": args.threads,
-            "rows": {"min": min(P.A.n for P in probs), "max": max(P.A.n for P in probs),
-                     "mean": round(statistics.mean(P.A.n for P in probs))},
-            "solves_per_s": round(len(recs) / wall, 2), "wall_s": round(wall, 3),
-            "latency_ms": {"p50": round(bt.percentile([r.wall_ms for r in recs], 50), 3),
-                           "p99": round(bt.percentile([r.wall_ms for r in recs], 99), 3)},
-            "mean_iters": round(statistics.mean(r.iters for r in recs), 1),
-            "plain_fp64_one_at_a_time_solves_per_s": round(plain_per_s, 2),
-            "speedup_vs_plain_fp64_one_at_a_time": round(len(recs) / wall / plain_per_s, 2),
-            "setup_s": {"host": round(host_setup_s, 2), "upload_and_ic0": round(upload_s, 2)},
+    xs = [np.zeros(len(b)) for b in bs]
+    res = B.solve(systems, bs, xs, 10000, TOL, storage=ib.STORE_FP32, rr_interval=RR)
+    first_s = time.perf_counter() - t0
+    for _ in range(max(0, warmup - 1)):
+        xs = [np.zeros(len(b)) for b in bs]
+        B.solve(systems, bs, xs, 10000, TOL, storage=ib.STORE_FP32, rr_interval=RR)
+    dev_ms, wall_ms, lat, l0 = [], [], [], B.launches
+    for _ in range(steps):
+        xs = [np.zeros(len(b)) for b in bs]
+        t0 = time.perf_counter()
+        res = B.solve(systems, bs, xs, 10000, TOL, storage=ib.STORE_FP32, rr_interval=RR)
+        wall_ms.append((time.perf_counter() - t0) * 1e3)
+        dev_ms.append(B.device_ms)
+        lat.extend(r.solve_ms for r in res)
+    launches = (B.launches - l0) // max(1, steps)
+    ok = all(r.converged and r.true_rel_resid <= TOL for r in res)
+    nsolve = len(bs)
+    dms = statistics.median(dev_ms)
+    wms = statistics.median(wall_ms)
+    it_bytes = sum(bytes_model(probs[k], 4)["iteration"] * r.iters for k, r in zip(systems, res))
+    out = {"systems": count, "rhs_per_system": nrhs, "solves": nsolve, "all_converged_1e-8": ok,
+           "rows": {"min": min(P.A.n for P in probs), "max": max(P.A.n for P in probs),
+                    "mean": round(statistics.mean(P.A.n for P in probs))},
+           "solves_per_s": round(nsolve / (dms * 1e-3), 2),
+           "e2e_solves_per_s": round(nsolve / (wms * 1e-3), 2),
+           "batch_ms": {"device": round(dms, 3), "e2e": round(wms, 3)},
+           "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3),
+                          "p99": round(float(np.percentile(lat, 99)), 3)},
+           "mean_iters": round(statistics.mean(r.iters for r in res), 1),
+           "max_iters": max(r.iters for r in res),
+           "iteration_GBps": round(it_bytes / (dms * 1e-3) / 1e9, 1),
+           "launches_per_batch": int(launches),
+           "setup_s": {"host": round(host_s, 2), "upload_and_ic0": round(upload_s, 2),
+                       "first_batch_with_layouts": round(first_s, 2)},
+           "steps": steps}
+    # the same solves one at a time: the per-system fused mixed path (its
+    # own CUDA graphs) and the plain FP64 path, on a sample of the solves
+    pick = list(range(0, nsolve, max(1, nsolve // sample)))
+    one_mixed, one_plain = [], []
+    for s in pick:
+        c = ctxs[systems[s]]
+        x = np.zeros(len(bs[s]))
+        c.solve(bs[s], x, 10000, TOL, storage=ib.STORE_FP32, rr_interval=RR)
+        x[:] = 0.0
+        r = c.solve(bs[s], x, 10000, TOL, storage=ib.STORE_FP32, rr_interval=RR)
+        one_mixed.append(r.solve_ms)
+        x[:] = 0.0
+        r = c.solve(bs[s], x, 10000, TOL, storage=ib.STORE_FP64, mode=ib.MODE_PLAIN)
+        one_plain.append(r.solve_ms)
+    mixed_per_s = 1000.0 / statistics.mean(one_mixed)
+    plain_per_s = 1000.0 / statistics.mean(one_plain)
+    out["one_at_a_time_solves_per_s"] = {"fused_mixed": round(mixed_per_s, 2), "plain_fp64": round(plain_per_s, 2),
+                                         "sample": len(pick)}
+    out["speedup_vs_one_at_a_time_fused_mixed"] = round(out["solves_per_s"] / mixed_per_s, 2)
+    out["speedup_vs_one_at_a_time_plain_fp64"] = round(out["solves_per_s"] / plain_per_s, 2)
+    B.close()
+    if compare_streams:
+        # the earlier form: one context and stream per system, 16 host threads
+        import iccg_b200.batch as bt
+        for c in ctxs:
+            c.close()
+        ctxs = []
+        rs = [bt.ResidentSystem(P, device=device, storage=ib.STORE_FP32) for P in probs]
+        bt.solve_batch(rs, [[r[0]] for r in rhs], threads=16)
+        t0 = time.perf_counter()
+        recs = bt.solve_batch(rs, rhs, threads=16)
+        wall = time.perf_counter() - t0
+        out["streams_16_threads_solves_per_s"] = round(len(recs) / wall, 2)
+        for r in rs:
+            r.close()
+    for c in ctxs:
+        c.close()
+    return out
+
+
+def run_batched(args):
+    """Many independent SPD systems of uneven size, 4 right-hand sides each
+    (--systems, default 512: 2048 solves), through the batched engine: every
+    CG step of all solves is one kernel launch over a device work list, with
+    per-solve CG scalars and reductions.  The comparisons are the same solves
+    one at a time (the per-system fused path and the plain FP64 path) and the
+    earlier many-streams form (one context and stream per system, 16 host
+    threads)."""
+    import torch
+    torch.cuda.set_device(0)
+    out = batched_case(args.systems, 4, steps=max(1, args.steps), warmup=max(1, args.warmup))
+    line = {"workload": "batched", **out,
             "storage": "fp32 A and L, fp64 vectors", "preconditioner": "IC(0), greedy multicolor",
-            "data": "synthetic", "timing": "host wall clock around the batch (many streams)"}
+            "data": "synthetic",
+            "timing": "device: CUDA events around each batch on the batch's stream (median over steps); "
+                      "e2e: wall clock of Batch.solve with host arrays in and out"}
     print(json.dumps(line), flush=True)
 
 

@@ -22,7 +22,7 @@ import ctypes as C
 import os
 from dataclasses import dataclass, field
 from pathlib import Path
-from typing import Optional
+from typing import List, Optional, Sequence
 
 import numpy as np
 
@@ -38,7 +38,7 @@ __all__ = [
     "color_greedy", "block_partition", "color_blocks", "host_spmv",
     "Context", "Identity", "Jacobi", "IC0", "conjugate_gradient",
     "PRECOND_NONE", "PRECOND_JACOBI", "PRECOND_IC0", "STORE_FP64", "STORE_FP32",
-    "MODE_PLAIN", "MODE_FUSED",
+    "MODE_PLAIN", "MODE_FUSED", "Batch",
 ]
 
 _LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libiccg_b200.so"
@@ -55,6 +55,7 @@ OPT_PDL = 2
 OPT_STAGE_KB = 3
 OPT_STAGE_BUFS = 4
 OPT_PERSIST = 5
+OPT_FUSE_UPDATE = 6
 STATUS_NAMES = {0: "converged", 1: "breakdown", 2: "max_iter", 3: "nonfinite"}
 
 
@@ -144,6 +145,15 @@ def lib() -> C.CDLL:
         "iccg_profile_enable": (_I, [_P, _I]),
         "iccg_profile_read": (_I, [_P, _I, C.POINTER(_D), C.POINTER(C.c_longlong)]),
         "iccg_sweep_plan": (_I, [_P, _I, _I, _P, _P, _I, C.POINTER(_I)]),
+        "iccg_batch_create": (_I, [_I, C.POINTER(_P)]),
+        "iccg_batch_destroy": (_I, [_P]),
+        "iccg_batch_last_error": (C.c_char_p, [_P]),
+        "iccg_batch_launch_count": (C.c_longlong, [_P]),
+        "iccg_batch_device_bytes": (C.c_longlong, [_P]),
+        "iccg_batch_device_ms": (_D, [_P]),
+        "iccg_batch_add_system": (_I, [_P, _P, C.POINTER(_I)]),
+        "iccg_batch_clear": (_I, [_P]),
+        "iccg_batch_solve": (_I, [_P, _I, _P, _P, _P, _I, _D, C.POINTER(_Opts), _P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -590,6 +600,84 @@ class Context:
         grids = np.zeros(max(nl.value, 1), np.int32)
         self._ck(lib().iccg_sweep_plan(self.h, storage, int(fwd), _ptr(kinds), _ptr(grids), nl.value, C.byref(nl)))
         return [(self.SWEEP_KINDS[k], int(g)) for k, g in zip(kinds[:nl.value], grids[:nl.value])]
+
+
+class Batch:
+    """Many independent solves advanced together (iccg_batch): one kernel
+    launch per CG step for all of them.  Systems are Contexts with a matrix,
+    a schedule and a built IC(0) preconditioner; each solve gives the bits,
+    iterations and residuals of Context.solve on its system alone."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().iccg_batch_create(device, C.byref(h)))
+        self.h = h
+        self._systems: List[Context] = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().iccg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc):
+        if rc != OK:
+            raise IccgError(rc, lib().iccg_batch_last_error(self.h).decode(errors="replace"))
+
+    def add_system(self, ctx: Context) -> int:
+        """Adds a system (kept alive by the batch); returns its index."""
+        idx = C.c_int()
+        self._ck(lib().iccg_batch_add_system(self.h, ctx.h, C.byref(idx)))
+        self._systems.append(ctx)
+        return idx.value
+
+    def clear(self):
+        self._ck(lib().iccg_batch_clear(self.h))
+        self._systems = []
+
+    @property
+    def launches(self) -> int:
+        return int(lib().iccg_batch_launch_count(self.h))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(lib().iccg_batch_device_bytes(self.h))
+
+    @property
+    def device_ms(self) -> float:
+        """Device time of the last solve() (CUDA events)."""
+        return float(lib().iccg_batch_device_ms(self.h))
+
+    def solve(self, systems: Sequence[int], bs: Sequence[np.ndarray], xs: Sequence[np.ndarray],
+              max_iter: int = 10000, tol: float = 1e-8, storage: int = STORE_FP64, rr_interval: int = 50,
+              graph_iters: int = 8) -> List[CGResult]:
+        """Solve s: system systems[s], right-hand side bs[s], x0 / solution
+        xs[s] (contiguous float64, updated in place)."""
+        m = len(systems)
+        if len(bs) != m or len(xs) != m:
+            raise ValueError("systems, bs and xs differ in length")
+        sysv = _i32(systems)
+        bv = [_f64(b) for b in bs]
+        for s, (k, b, x) in enumerate(zip(sysv, bv, xs)):
+            if not 0 <= k < len(self._systems):
+                raise ValueError(f"solve {s}: no system {k}")
+            n = self._systems[k].n
+            if x.dtype != np.float64 or not x.flags.c_contiguous:
+                raise TypeError("x must be a contiguous float64 array (updated in place)")
+            if b.shape != (n,) or x.shape != (n,):
+                raise ValueError(f"solve {s}: vectors of system {k} have {n} entries")
+        bp = (C.c_void_p * m)(*[b.ctypes.data for b in bv])
+        xp = (C.c_void_p * m)(*[x.ctypes.data for x in xs])
+        res = (_Result * m)()
+        opts = _Opts(MODE_FUSED, storage, rr_interval, graph_iters)
+        self._ck(lib().iccg_batch_solve(self.h, m, _ptr(sysv), bp, xp, int(max_iter), float(tol), C.byref(opts),
+                                        res))
+        return [_cg_result(r) for r in res]
 
 
 def _cg_result(res: _Result) -> CGResult:

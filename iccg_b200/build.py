@@ -22,7 +22,7 @@ LIB = LIBDIR / "libiccg_b200.so"
 CUDA_SOURCES = ["ctx.cu", "noalloc.cu"]
 HOST_SOURCES = ["host_order.cpp", "host_gen.cpp", "host_layout.cpp", "host_capi.cpp"]
 HEADERS = ["dd.cuh", "kernels.cuh", "persist.cuh", "host.hpp", "devbuf.hpp", "context.hpp", "plan.inl", "factor.inl",
-           "qsys.inl", "persist.inl", "solver.inl"]
+           "qsys.inl", "persist.inl", "solver.inl", "batch.inl"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -271,6 +271,7 @@ struct iccg_ctx {
     int stage_bufs = 1;     // ICCG_OPT_STAGE_BUFS: staged-sweep buffers per CTA (1 or 2)
     int smem_optin = 0;     // largest dynamic shared memory per CTA
     bool persist = false;   // ICCG_OPT_PERSIST: the IC(0) apply as one persistent launch where planned
+    bool fuse_update = false; // ICCG_OPT_FUSE_UPDATE: the CG update inside the forward sweep's launches
     iccg::QSys Q;
     // preconditioner
     int pc_kind = -1;

@@ -28,6 +28,7 @@ extern thread_local std::string g_host_err;  // host_capi.cpp
 #include "qsys.inl"
 #include "persist.inl"
 #include "solver.inl"
+#include "batch.inl"
 
 template <class F>
 static int guard(iccg_ctx* c, F&& f)
@@ -49,6 +50,25 @@ static int guard(iccg_ctx* c, F&& f)
     }
 }
 
+template <class F>
+static int bguard(iccg_batch* B, F&& f)
+{
+    if (!B) return ICCG_ERR_ARG;
+    try {
+        CK(cudaSetDevice(B->device));
+        f();
+        return ICCG_OK;
+    } catch (const Error& e) {
+        B->err = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        B->err = "out of host memory";
+        return ICCG_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        B->err = e.what();
+        return ICCG_ERR_ARG;
+    }
+}
 
 }  // namespace iccg
 
@@ -132,6 +152,8 @@ int iccg_ctx_set_option(iccg_ctx* c, int option, long long value)
             c->pdl = value != 0;
         } else if (option == ICCG_OPT_PERSIST) {
             c->persist = value != 0;
+        } else if (option == ICCG_OPT_FUSE_UPDATE) {
+            c->fuse_update = value != 0;
         } else if (option == ICCG_OPT_STAGE_BUFS) {
             if (value != 1 && value != 2) throw Error(ICCG_ERR_ARG, "ICCG_OPT_STAGE_BUFS takes 1 or 2");
             c->stage_bufs = (int)value;
@@ -428,6 +450,99 @@ int iccg_sweep_plan(iccg_ctx* c, int storage, int fwd, int* kinds, int* grids, i
             kinds[l] = s.kind;
             grids[l] = s.grid;
         }
+    });
+}
+
+// ---------------------------------------------------------------------------
+// batched solves
+// ---------------------------------------------------------------------------
+static void batch_free(iccg_batch* B)
+{
+    if (B->ev0) cudaEventDestroy(B->ev0);
+    if (B->ev1) cudaEventDestroy(B->ev1);
+    for (auto e : B->evs)
+        if (e) cudaEventDestroy(e);
+    if (B->h_running) cudaFreeHost(B->h_running);
+    cudaStream_t s = B->stream;
+    delete B;  // device buffers free themselves
+    if (s) cudaStreamDestroy(s);
+}
+
+int iccg_batch_create(int device, iccg_batch** out)
+{
+    if (!out) return ICCG_ERR_ARG;
+    *out = nullptr;
+    auto* B = new iccg_batch;
+    B->device = device;
+    const int rc = bguard(B, [&] {
+        int ndev = 0;
+        CK(cudaGetDeviceCount(&ndev));
+        if (device < 0 || device >= ndev) throw Error(ICCG_ERR_ARG, "no such CUDA device");
+        CK(cudaDeviceGetAttribute(&B->nsm, cudaDevAttrMultiProcessorCount, device));
+        CK(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
+        CK(cudaEventCreate(&B->ev0));
+        CK(cudaEventCreate(&B->ev1));
+        CK(cudaEventCreateWithFlags(&B->evs[0], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&B->evs[1], cudaEventDisableTiming));
+        CK(cudaMallocHost(&B->h_running, 2 * sizeof(int)));
+    });
+    if (rc) {
+        iccg::g_host_err = B->err;
+        batch_free(B);
+        return rc;
+    }
+    *out = B;
+    return ICCG_OK;
+}
+
+int iccg_batch_destroy(iccg_batch* B)
+{
+    if (!B) return ICCG_OK;
+    cudaSetDevice(B->device);
+    if (B->stream) cudaStreamSynchronize(B->stream);
+    batch_free(B);
+    return ICCG_OK;
+}
+
+const char* iccg_batch_last_error(const iccg_batch* B) { return B ? B->err.c_str() : "null batch"; }
+long long iccg_batch_launch_count(const iccg_batch* B) { return B ? B->launches : 0; }
+long long iccg_batch_device_bytes(const iccg_batch* B) { return B ? B->dev_bytes : 0; }
+double iccg_batch_device_ms(const iccg_batch* B) { return B ? B->last_ms : 0.0; }
+
+int iccg_batch_add_system(iccg_batch* B, iccg_ctx* ctx, int* index)
+{
+    return bguard(B, [&] {
+        if (!ctx || !index) throw Error(ICCG_ERR_ARG, "null argument");
+        if (ctx->device != B->device) throw Error(ICCG_ERR_ARG, "context on another device");
+        require_precond(ctx);
+        *index = (int)B->sys.size();
+        B->sys.push_back(ctx);
+    });
+}
+
+int iccg_batch_clear(iccg_batch* B)
+{
+    return bguard(B, [&] {
+        CK(cudaStreamSynchronize(B->stream));
+        B->sys.clear();
+    });
+}
+
+int iccg_batch_solve(iccg_batch* B, int nsolve, const int* system, const double* const* b, double* const* x,
+                     int max_iter, double tol, const iccg_solve_opts* opts, iccg_result* res)
+{
+    return bguard(B, [&] {
+        if (nsolve <= 0 || !system || !b || !x || !res) throw Error(ICCG_ERR_ARG, "null argument or no solves");
+        for (int s = 0; s < nsolve; ++s)
+            if (!b[s] || !x[s]) throw Error(ICCG_ERR_ARG, "null right-hand side or solution");
+        if (B->sys.empty()) throw Error(ICCG_ERR_STATE, "the batch holds no system");
+        iccg_solve_opts o{ICCG_MODE_FUSED, ICCG_STORE_FP64, 50, 8};
+        if (opts) o = *opts;
+        if (o.graph_iters <= 0) o.graph_iters = 8;
+        if (o.mode != ICCG_MODE_FUSED) throw Error(ICCG_ERR_ARG, "batched solves run the fused form only");
+        if (o.storage == ICCG_STORE_FP32) bat::run<float>(B, nsolve, system, b, x, max_iter, tol, o, res);
+        else if (o.storage == ICCG_STORE_FP64) bat::run<double>(B, nsolve, system, b, x, max_iter, tol, o, res);
+        else throw Error(ICCG_ERR_ARG, "unknown storage");
     });
 }
 

@@ -46,8 +46,17 @@ struct SolverState {
     int pend;         // a stop decided by the persistent apply's own reductions (kRunning: none);
                       // the p update that follows the apply moves it into `status`
     unsigned int ticket;
-    unsigned int pad2;
+    int true_check;   // 1: a recurrence residual below tol asks for an FP64 residual check in the same
+                      // iteration (rr_flag) instead of stopping with kTrueCheck (the batched solves)
+    unsigned long long t_stop;  // %globaltimer (ns) when the solve stopped (0 while running)
 };
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
 
 enum Fin {
     FIN_NONE = 0,
@@ -134,7 +143,8 @@ __device__ void finish(const double* v, SolverState* st, double* out)
         if (st->rr_interval <= 0) {
             if (rel < st->tol) status = kConverged;
         } else if (rel < st->tol) {
-            status = kTrueCheck;
+            if (st->true_check) st->rr_flag = 1;
+            else status = kTrueCheck;
         } else if ((st->k + 1) % st->rr_interval == 0) {
             st->rr_flag = 1;
         }
@@ -510,6 +520,26 @@ __global__ void __launch_bounds__(256) k_sweep(SweepArgs a, int u0, int u1, int 
 // results keep its bits.  Vectors live in Q order; they are permuted only at
 // the API boundary.
 // ---------------------------------------------------------------------------
+// The CG update fused into the forward sweep (FIN_UPD): x += alpha p,
+// r -= alpha Ap (cg_crs.cpp:137-141) for each row as the sweep loads it;
+// the new r is the row's input and r.r is reduced by the sweep's launches
+// (the residual test of cg_crs.cpp:143).  The arithmetic is k_update's.
+struct UpdArgs {
+    double* r;
+    double* x;
+    const double* p;
+    const double* Ap;
+};
+
+__device__ __forceinline__ double cg_update_row(const UpdArgs& U, double alpha, int q)
+{
+    const double rq = U.r[q], apq = U.Ap[q], pq = U.p[q], xq = U.x[q];
+    U.x[q] = fma(alpha, pq, xq);
+    const double rn = fma(-alpha, apq, rq);
+    U.r[q] = rn;
+    return rn;
+}
+
 struct SellMat {
     const int* ptr;       // first slot of each slice
     const int* col;       // column (Q index) per slot
@@ -1072,6 +1102,7 @@ __device__ __forceinline__ void st_gather(const BatchDesc& cur, unsigned char* b
     T* s_iv = reinterpret_cast<T*>(base + Ly.iv);
     const int p0 = FWD ? cur.ps0 : cur.pt0;
     const int ns = cur.se - cur.sb;
+    (void)s_rd;
 
     // G, full batches (every slice 32 rows, so tile row rr is lane
     // rr % 32 of slice rr / 32): rows tid + 256 k, straight-line code
@@ -1400,24 +1431,40 @@ template <class T, bool FWD, int FIN, bool EXACT, int NB = 2>
 __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDesc* __restrict__ bd, int rows_cap,
                                                   int slots_cap, int slices_cap, const int* __restrict__ sl0,
                                                   const int* __restrict__ glen, const SliceMeta* __restrict__ meta,
-                                                  SellMat M, const T* __restrict__ dg, const double* __restrict__ in,
+                                                  SellMat M, const T* __restrict__ dg, const double* in,
                                                   double* out, const double* __restrict__ rdot, int slot0,
-                                                  int nslots, SolverState* st, RedBuf red, unsigned int* ticket)
+                                                  int nslots, SolverState* st, RedBuf red, unsigned int* ticket,
+                                                  UpdArgs U)
 {
     grid_dep_begin();
     if (st_done(st)) return;
-    constexpr bool with_r = FIN != FIN_NONE;
+    // FIN_UPD (forward, one buffer): the fused CG update writes each
+    // batch's inputs into its tile
+    constexpr bool UPD = FIN == FIN_UPD;
+    static_assert(!UPD || (FWD && NB == 1), "the fused update runs in single-buffered forward sweeps");
+    constexpr bool with_r = FIN == FIN_RZ || FIN == FIN_RZ0;
     constexpr bool with_pv = !(FWD || !EXACT);
+    const double alpha = UPD ? st->alpha : 0.0;
     extern __shared__ __align__(16) unsigned char smem_st[];
     const StageLayout Ly = stage_layout(rows_cap, slots_cap, slices_cap, (int)sizeof(T), with_r, with_pv);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const double* prev = out;  // earlier-level values: read-only in this launch
     acc2 rz[1] = {{0.0, 0.0}};
 
+    // the fused update of a just-staged batch's rows, into the tile
+    auto update = [&](unsigned char* base, const BatchDesc& d) {
+        double* s_in = reinterpret_cast<double*>(base + Ly.in) + (d.qb & 1);
+        for (int i = threadIdx.x; i < d.qe - d.qb; i += blockDim.x) {
+            const double rn = cg_update_row(U, alpha, d.qb + i);
+            s_in[i] = rn;
+            acc2_fma(rz[0], rn, rn);
+        }
+    };
     int b = b0 + blockIdx.x;
     if (b < b1) {
         BatchDesc cur = bd[b];
-        stage_batch<T, FWD, with_r>(smem_st, Ly, cur, meta, M, dg, in, rdot);
+        stage_batch<T, FWD, with_r, !UPD>(smem_st, Ly, cur, meta, M, dg, in, rdot);
+        if (UPD) update(smem_st, cur);
         bool has_next = b + (int)gridDim.x < b1;
         BatchDesc nxt = cur;
         if (has_next) nxt = bd[b + gridDim.x];
@@ -1426,7 +1473,7 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
             // is worked on; NB = 1: one buffer, refilled after each batch
             unsigned char* base = smem_st + (NB == 2 ? (i & 1) * Ly.bytes : 0);
             if (NB == 2 && has_next)
-                stage_batch<T, FWD, with_r>(smem_st + ((i + 1) & 1) * Ly.bytes, Ly, nxt, meta, M, dg, in, rdot);
+                stage_batch<T, FWD, with_r, !UPD>(smem_st + ((i + 1) & 1) * Ly.bytes, Ly, nxt, meta, M, dg, in, rdot);
             const bool has_nn = has_next && b + 2 * (int)gridDim.x < b1;
             BatchDesc nn = nxt;
             if (has_nn) nn = bd[b + 2 * gridDim.x];
@@ -1450,7 +1497,10 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
             st_chain<T, FWD, EXACT, with_r>(cur, base, Ly, rows_cap, gl, gs, out, rz[0]);
             __syncthreads();
             if (!has_next) break;
-            if (NB == 1) stage_batch<T, FWD, with_r>(smem_st, Ly, nxt, meta, M, dg, in, rdot);
+            if (NB == 1) {
+                stage_batch<T, FWD, with_r, !UPD>(smem_st, Ly, nxt, meta, M, dg, in, rdot);
+                if (UPD) update(smem_st, nxt);
+            }
             b += gridDim.x;
             cur = nxt;
             nxt = nn;
@@ -1475,14 +1525,16 @@ template <class T, bool FWD, int FIN, bool EXACT>
 __global__ void __launch_bounds__(256) k_sweep_chain(int g0, int g1, const int* __restrict__ glen,
                                                      const int* __restrict__ sl0, const SliceMeta* __restrict__ meta,
                                                      SellMat M, const T* __restrict__ dg,
-                                                     const double* __restrict__ in, double* __restrict__ out,
+                                                     const double* in, double* __restrict__ out,
                                                      const double* __restrict__ rdot, int slot0, int nslots,
-                                                     SolverState* st, RedBuf red, unsigned int* ticket)
+                                                     SolverState* st, RedBuf red, unsigned int* ticket, UpdArgs U)
 {
     grid_dep_begin();
     if (st_done(st)) return;
-    constexpr bool with_r = FIN != FIN_NONE;
+    constexpr bool UPD = FIN == FIN_UPD;  // forward: the fused CG update on load
+    constexpr bool with_r = FIN == FIN_RZ || FIN == FIN_RZ0;
     constexpr int CH = 4;
+    const double alpha = UPD ? st->alpha : 0.0;
     const T* __restrict__ val = (const T*)M.val;
     const int lane = threadIdx.x & 31;
     acc2 rz[1] = {{0.0, 0.0}};
@@ -1511,7 +1563,12 @@ __global__ void __launch_bounds__(256) k_sweep_chain(int g0, int g1, const int* 
                 const int p = __shfl_sync(0xffffffffu, my_p, rs) + lane;
                 const int w = __shfl_sync(0xffffffffu, my_w, rs);
                 C.q[u] = q;
-                C.a[u] = ok ? in[q] : 0.0;
+                if (UPD) {
+                    C.a[u] = ok ? cg_update_row(U, alpha, q) : 0.0;
+                    if (ok) acc2_fma(rz[0], C.a[u], C.a[u]);
+                } else {
+                    C.a[u] = ok ? in[q] : 0.0;
+                }
                 C.p[u] = ok ? dg[q] : (T)1;
                 C.L[u] = ok ? M.len[q] & 0xffff : 0;
                 C.v[u] = (ok && w > 0) ? val[p] : (T)0;

@@ -112,7 +112,6 @@ __device__ __forceinline__ void persist_wait_deps(const PArgs& A, int t, unsigne
         while (v != tag) {
             __nanosleep(32);
             v = ld_volatile_u32(f);
-            __nanosleep(32);
             // give up after the poll limit, or at once after another wait of
             // this launch gave up (no chain of timeouts)
             if (++it > kPersistSpin || ld_volatile_u32(A.err) != 0u) {

@@ -250,11 +250,13 @@ static bool plan_staged_type(iccg_ctx* c, int k)
         const int ng = Q.level_g[(size_t)l + 1] - Q.level_g[(size_t)l];
         Q.ch_grid[k][(size_t)l] = std::max(1, std::min((ng + 7) / 8, std::max(1, pc) * c->nsm));
     }
-    // reduction slots of a backward sweep, whichever kernels its levels use
+    // reduction slots of a sweep (the backward r.z, or the forward r.r of
+    // the fused update), whichever kernels its levels use
     long long s = 0;
     for (int l = 0; l < L; ++l)
-        s += std::max({Q.st_bgrid[k][(size_t)l], Q.st1_bgrid[k][(size_t)l], Q.ch_grid[k][(size_t)l],
-                       Q.two_phase ? Q.g2grid[(size_t)l] : 0, Q.fgrid.empty() ? 0 : Q.fgrid[(size_t)l]});
+        s += std::max({Q.st_bgrid[k][(size_t)l], Q.st1_bgrid[k][(size_t)l], Q.st_fgrid[k][(size_t)l],
+                       Q.st1_fgrid[k][(size_t)l], Q.ch_grid[k][(size_t)l], Q.two_phase ? Q.g2grid[(size_t)l] : 0,
+                       Q.fgrid.empty() ? 0 : Q.fgrid[(size_t)l]});
     ensure_partials(c, (size_t)std::max<long long>(s, 1));
     return true;
 }

@@ -94,7 +94,7 @@ static void launch_q2_level(iccg_ctx* c, int l, int grid, const double* in, doub
 
 template <class T, int FIN, bool FWD>
 static void launch_sweep_level(iccg_ctx* c, int l, const SweepLevel& sl, const double* in, double* out,
-                               const double* rdot, int slot0, int nslots, SolverState* st)
+                               const double* rdot, int slot0, int nslots, SolverState* st, UpdArgs U = UpdArgs{})
 {
     QSys& Q = c->Q;
     constexpr bool f32 = std::is_same<T, float>::value;
@@ -110,19 +110,31 @@ static void launch_sweep_level(iccg_ctx* c, int l, const SweepLevel& sl, const d
     case 0:
         launch(c, cls, k_sweep_chain<T, FWD, FIN, exact>, sl.grid, kThreads, Q.level_g[l_], Q.level_g[l_ + 1],
                (const int*)Q.glen.get(), (const int*)Q.sl0.get(), (const SliceMeta*)Q.meta.get(), M, dg, in, out,
-               rdot, slot0, nslots, st, red, c->ticket.get());
+               rdot, slot0, nslots, st, red, c->ticket.get(), U);
         break;
     case 1: {
         const int slots = FWD ? Q.st_slotsS[l_] : Q.st_slotsT[l_];
         const int nbuf = c->stage_bufs == 1 ? 1 : 2;
+        constexpr bool with_r = FIN == FIN_RZ || FIN == FIN_RZ0;
         const size_t smem = nbuf * (size_t)stage_layout(Q.st_rows[l_], slots, Q.st_slices[l_], (int)sizeof(T),
-                                                        FIN != FIN_NONE, !FWD && exact)
+                                                        with_r, !FWD && exact)
                                        .bytes;
-        auto kern = nbuf == 1 ? k_sweep_st<T, FWD, FIN, exact, 1> : k_sweep_st<T, FWD, FIN, exact, 2>;
-        allow_smem(c, kern);
-        launch_smem(c, cls, kern, sl.grid, kThreads, smem, Q.lb[l_], Q.lb[l_ + 1], (const BatchDesc*)Q.bdesc.get(),
-                    Q.st_rows[l_], slots, Q.st_slices[l_], (const int*)Q.sl0.get(), (const int*)Q.glen.get(),
-                    (const SliceMeta*)Q.meta.get(), M, dg, in, out, rdot, slot0, nslots, st, red, c->ticket.get());
+        if constexpr (FIN == FIN_UPD) {
+            // the fused update runs single-buffered only (fused_update_ok)
+            auto kern = k_sweep_st<T, FWD, FIN, exact, 1>;
+            allow_smem(c, kern);
+            launch_smem(c, cls, kern, sl.grid, kThreads, smem, Q.lb[l_], Q.lb[l_ + 1],
+                        (const BatchDesc*)Q.bdesc.get(), Q.st_rows[l_], slots, Q.st_slices[l_],
+                        (const int*)Q.sl0.get(), (const int*)Q.glen.get(), (const SliceMeta*)Q.meta.get(), M, dg, in,
+                        out, rdot, slot0, nslots, st, red, c->ticket.get(), U);
+        } else {
+            auto kern = nbuf == 1 ? k_sweep_st<T, FWD, FIN, exact, 1> : k_sweep_st<T, FWD, FIN, exact, 2>;
+            allow_smem(c, kern);
+            launch_smem(c, cls, kern, sl.grid, kThreads, smem, Q.lb[l_], Q.lb[l_ + 1],
+                        (const BatchDesc*)Q.bdesc.get(), Q.st_rows[l_], slots, Q.st_slices[l_],
+                        (const int*)Q.sl0.get(), (const int*)Q.glen.get(), (const SliceMeta*)Q.meta.get(), M, dg, in,
+                        out, rdot, slot0, nslots, st, red, c->ticket.get(), U);
+        }
         break;
     }
     case 2:
@@ -139,16 +151,47 @@ static void launch_sweep_level(iccg_ctx* c, int l, const SweepLevel& sl, const d
     }
 }
 
-template <class T, int FIN>
-static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, SolverState* st)
+// true if every forward level runs on a kernel with the fused CG update
+// (chain-only, or single-buffered staged)
+template <class T>
+static bool fused_update_ok(iccg_ctx* c)
+{
+    const QSys& Q = c->Q;
+    if (!c->use_q || c->pc_kind != ICCG_PRECOND_IC0 || c->stage_bufs != 1 || !c->fuse_update) return false;
+    for (int l = 0; l < Q.nlevels; ++l) {
+        const int k = sweep_level<T>(c, l, true).kind;
+        if (k != 0 && k != 1) return false;
+    }
+    return true;
+}
+
+// z = M^{-1} r.  UPD: the forward levels first do the CG update x += alpha
+// p, r -= alpha Ap of their rows (U) and reduce r.r over all their launches
+// (FIN_UPD at the last CTA of the last forward level).
+template <class T, int FIN, bool UPD = false>
+static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, SolverState* st, UpdArgs U = UpdArgs{})
 {
     QSys& Q = c->Q;
-    if (use_persist(c, std::is_same<T, float>::value ? ICCG_STORE_FP32 : ICCG_STORE_FP64)) {
+    if (!UPD && use_persist(c, std::is_same<T, float>::value ? ICCG_STORE_FP32 : ICCG_STORE_FP64)) {
         launch_persist<T, false, FIN>(c, const_cast<double*>(r), y, z, st);
         return;
     }
-    for (int l = 0; l < Q.nlevels; ++l)
-        launch_sweep_level<T, FIN_NONE, true>(c, l, sweep_level<T>(c, l, true), r, y, nullptr, 0, 0, st);
+    if (UPD) {
+        std::vector<SweepLevel> fl((size_t)Q.nlevels);
+        int fslots = 0;
+        for (int l = 0; l < Q.nlevels; ++l) {
+            fl[(size_t)l] = sweep_level<T>(c, l, true);
+            fslots += fl[(size_t)l].grid;
+        }
+        int s0 = 0;
+        for (int l = 0; l < Q.nlevels; ++l) {
+            launch_sweep_level<T, FIN_UPD, true>(c, l, fl[(size_t)l], r, y, nullptr, s0, fslots, st, U);
+            s0 += fl[(size_t)l].grid;
+        }
+    } else {
+        for (int l = 0; l < Q.nlevels; ++l)
+            launch_sweep_level<T, FIN_NONE, true>(c, l, sweep_level<T>(c, l, true), r, y, nullptr, 0, 0, st);
+    }
     std::vector<SweepLevel> bl((size_t)Q.nlevels);
     int nslots = 0;
     for (int l = Q.nlevels - 1; l >= 0; --l) {
@@ -319,6 +362,15 @@ static void fused_iteration(iccg_ctx* c, int storage, bool rr, const double* b, 
         // update, both sweeps and the two reductions in one launch
         if (storage == ICCG_STORE_FP32) launch_persist<float, true, FIN_RZ>(c, c->vr.get(), c->vy.get(), c->vz.get(), st, x);
         else launch_persist<double, true, FIN_RZ>(c, c->vr.get(), c->vy.get(), c->vz.get(), st, x);
+        launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st);
+        return;
+    }
+    const bool f32 = storage == ICCG_STORE_FP32;
+    if (!rr && (f32 ? fused_update_ok<float>(c) : fused_update_ok<double>(c))) {
+        // the update inside the forward sweep's launches
+        const UpdArgs U{c->vr.get(), x, c->vp.get(), c->vAp.get()};
+        if (f32) apply_ic0_q<float, FIN_RZ, true>(c, c->vr.get(), c->vy.get(), c->vz.get(), st, U);
+        else apply_ic0_q<double, FIN_RZ, true>(c, c->vr.get(), c->vy.get(), c->vz.get(), st, U);
         launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st);
         return;
     }

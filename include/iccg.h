@@ -217,13 +217,23 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
    batches whose rows they read; in a fused solve the same launch also does
    the CG update x += alpha p, r -= alpha Ap and r.r.  0 launches one kernel
    per level (ICCG_OPT_SWEEP chooses which).  It applies where every level
-   is staged.  FP64 results are the same bits either way. */
+   is staged.  FP64 results are the same bits either way.
+   ICCG_OPT_FUSE_UPDATE (default 0), lane-interleaved fused solves with the
+   per-level kernels: 1 does the CG update x += alpha p, r -= alpha Ap and
+   the r.r reduction inside the forward sweep's launches (where every
+   forward level runs the chain-only or single-buffered staged kernel), so
+   the update needs no launch and r is not read back; 0 launches the update
+   on its own.  Iterations with a residual replacement always update on
+   their own.  The fused form loads p, Ap, x and r of each batch's rows
+   synchronously before the batch's sweep, which costs more than the launch
+   it saves on the 128^3 ABMC system; it is kept as an option. */
 #define ICCG_OPT_TILED 0
 #define ICCG_OPT_SWEEP 1
 #define ICCG_OPT_PDL 2
 #define ICCG_OPT_STAGE_KB 3
 #define ICCG_OPT_STAGE_BUFS 4
 #define ICCG_OPT_PERSIST 5
+#define ICCG_OPT_FUSE_UPDATE 6
 int iccg_ctx_set_option(iccg_ctx* ctx, int option, long long value);
 
 /* Uploads A_run (the matrix conjugate_gradient runs on, cg_crs.cpp:442-447):
@@ -323,6 +333,43 @@ int iccg_profile_read(iccg_ctx* ctx, int cls, double* total_ms, long long* launc
    as a solve would.  No counterpart in the reference (its sweeps have one
    OpenMP form, ic0.cpp:194-339). */
 int iccg_sweep_plan(iccg_ctx* ctx, int storage, int fwd, int* kinds, int* grids, int cap, int* nlevels);
+
+/* ---------------------------------------------------------------------------
+   Batched solves: many independent conjugate_gradient runs (cg_crs.cpp:89-162)
+   advanced together, one kernel launch per CG step for all of them.  The
+   reference solves one system per call (main_abmc.cpp, main_piccg.cpp); a
+   caller with many systems loops over it.  No counterpart in the reference.
+
+   A batch holds systems: contexts with a matrix, a schedule and a built IC(0)
+   preconditioner (the caller keeps ownership; a context must stay alive and
+   unchanged while the batch solves with it, and is not used by other calls
+   meanwhile).  Every level of each system's sweeps must fit the staged
+   substitution kernel (iccg_sweep_plan kind 1 or 0), which holds for the
+   multicolor and ABMC schedules of the 7- and 27-point problems.
+
+   iccg_batch_solve runs nsolve solves: solve s is system system[s] (an index
+   returned by iccg_batch_add_system) with the right-hand side b[s] and the
+   initial guess / solution x[s] (host arrays of that system's n doubles, A_run
+   order).  Each solve gives the same iterations, status, residuals and the
+   same bits of x as iccg_solve on its context alone with the same opts, in
+   any batch (mode must be ICCG_MODE_FUSED).  res[s].solve_ms is the device
+   time from the start of the batch to the iteration at which solve s stopped;
+   iccg_batch_device_ms gives the whole batch's device time.  Solves of one
+   system are best placed next to each other: each level's matrix data is
+   then read from DRAM once for all of them.
+   --------------------------------------------------------------------------- */
+typedef struct iccg_batch iccg_batch;
+int iccg_batch_create(int device, iccg_batch** out);
+int iccg_batch_destroy(iccg_batch* batch);
+const char* iccg_batch_last_error(const iccg_batch* batch);
+long long iccg_batch_launch_count(const iccg_batch* batch);
+long long iccg_batch_device_bytes(const iccg_batch* batch);
+double iccg_batch_device_ms(const iccg_batch* batch);
+int iccg_batch_add_system(iccg_batch* batch, iccg_ctx* ctx, int* index);
+int iccg_batch_clear(iccg_batch* batch);
+int iccg_batch_solve(iccg_batch* batch, int nsolve, const int* system, const double* const* b,
+                     double* const* x, int max_iter, double tol, const iccg_solve_opts* opts,
+                     iccg_result* res);
 
 #ifdef __cplusplus
 }

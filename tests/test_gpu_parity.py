@@ -643,3 +643,34 @@ def test_gpu_solve_dev_on_alternating_buffer_pairs(tiled):
         other = pairs[1 - k][1].cpu().numpy()
         assert not other.any() or rel_err(other, want) > 1e-3
     ctx.close()
+
+
+@pytest.mark.parametrize("which", ["abmc_lin", "abmc_bfs", "d27_mc", "d27_abmc8", "mc2d", "knn_abmc"])
+def test_gpu_fused_update_gives_the_same_bits(which):
+    """The CG update done inside the forward sweep's launches
+    (ICCG_OPT_FUSE_UPDATE) against the update kernel on its own:
+    the same arithmetic per row, so FP64 solves keep their bits and
+    iteration counts; FP32 storage converges to the true residual."""
+    P = {"abmc_lin": lambda: pb.config_abmc_aniso(40, 16, "linear"),
+         "abmc_bfs": lambda: pb.config_abmc_aniso(40, 16, "bfs"),
+         "d27_mc": lambda: pb.config_diffusion27(24, "piccg"),
+         "d27_abmc8": lambda: pb.config_diffusion27(24, "abmc", 8),
+         "mc2d": lambda: pb.config_small_mc(100, seed=1),
+         "knn_abmc": lambda: pb.config_knn(8000, seed=5, block_size=16)}[which]()
+    ctx = _ctx_for(P.A_run, P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    out = {}
+    for fuse in (1, 0):
+        ctx.set_option(ib.OPT_FUSE_UPDATE, fuse)
+        res = []
+        for st in (ib.STORE_FP64, ib.STORE_FP32):
+            x = np.zeros(P.A_run.n)
+            rr = ctx.solve(P.b_run, x, 10000, 1e-8, storage=st)
+            res.append((x, rr))
+        out[fuse] = res
+    (xa, ra), (xb, rb) = out[1][0], out[0][0]
+    assert ra.converged and ra.iters == rb.iters and np.array_equal(xa, xb)
+    (xa, ra), (xb, rb) = out[1][1], out[0][1]
+    assert ra.converged and ra.true_rel_resid <= 1e-8 and abs(ra.iters - rb.iters) <= 1
+    assert rel_err(xa, xb) < 1e-6
+    ctx.close()
