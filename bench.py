@@ -142,6 +142,57 @@ def bytes_model(P, storage_bytes: int):
     }
 
 
+def _solve_case(P, device: int, with_plain: bool = True) -> dict:
+    """One system: the mixed form (FP32 A and L, FP64 vectors, replacement
+    every RR) and the FP64 fused and plain forms, each timed by CUDA events
+    (median of 3 after a warm-up solve), with iterations, the true residual
+    and the mixed solution's error against the FP64 one."""
+    import iccg_b200 as ib
+    ctx = ib.Context(device)
+    ctx.upload(P.A_run)
+    ctx.set_schedule(P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    out = {"n": P.A_run.n, "nnz": P.A_run.nnz, "colors": P.nc}
+    xs = {}
+    forms = [("mixed", ib.STORE_FP32, ib.MODE_FUSED), ("fp64_fused", ib.STORE_FP64, ib.MODE_FUSED)]
+    if with_plain:
+        forms.append(("fp64_plain", ib.STORE_FP64, ib.MODE_PLAIN))
+    for name, st, mode in forms:
+        ms = []
+        for _ in range(4):
+            x = np.zeros(P.A_run.n)
+            r = ctx.solve(P.b_run, x, 10000, TOL, mode=mode, storage=st, rr_interval=RR)
+            ms.append(r.solve_ms)
+        xs[name] = x
+        out[name] = {"ms": round(statistics.median(ms[1:]), 4), "iters": r.iters, "converged": r.converged,
+                     "true_rel_resid": r.true_rel_resid}
+    x64 = xs["fp64_fused"]
+    out["mixed"]["err_vs_fp64_solution"] = float(np.linalg.norm(xs["mixed"] - x64) / np.linalg.norm(x64))
+    out["speedup_mixed_vs_fp64_fused"] = round(out["fp64_fused"]["ms"] / out["mixed"]["ms"], 3)
+    ctx.close()
+    return out
+
+
+def sub_results(device: int) -> dict:
+    """Short results of the other workloads, carried on the headline line:
+    C1 the 2D 5-point 128^2 Poisson problem with greedy multicolor IC(0);
+    C3 the 27-point variable-coefficient 96^3 problem, multicolor and ABMC
+    B=8; the batched engine on 64 of the batched workload's systems x 4
+    right-hand sides."""
+    import iccg_b200.problems as pb
+    out = {}
+    t0 = time.perf_counter()
+    try:
+        out["c1_poisson2d_128_mc"] = _solve_case(pb.config_small_mc(128, seed=0), device)
+        for key, (v, B) in {"c3_diffusion27_96_mc": ("piccg", 16), "c3_diffusion27_96_abmc8": ("abmc", 8)}.items():
+            out[key] = _solve_case(pb.config_diffusion27(96, v, block_size=B, seed=0), device, with_plain=False)
+        out["batched_64x4"] = batched_case(64, 4, steps=2, warmup=1, device=device, compare_streams=False, sample=8)
+    except Exception as e:   # the headline number stands; the failure is shown, not hidden
+        out["error"] = repr(e)
+    out["wall_s"] = round(time.perf_counter() - t0, 1)
+    return out
+
+
 def run_gpu(args):
     import torch
     import iccg_b200 as ib
@@ -224,36 +275,46 @@ def run_gpu(args):
     plain = solve(ib.STORE_FP64, ib.MODE_PLAIN)
     fused64 = solve(ib.STORE_FP64, ib.MODE_FUSED)
 
-    # per-kernel device time: one more solve with every launch bracketed by
-    # CUDA events on the context's stream
+    # per-kernel device time.  The solve's kernels run back to back inside
+    # CUDA graphs (with programmatic dependent launch), so a kernel's time is
+    # its share of the graph-replayed solve -- from the committed ncu launch
+    # list of the same solve -- times the event-timed solve above.  One more
+    # solve with every launch bracketed by CUDA events (no graphs) is
+    # reported beside it; it runs about a fifth slower.
     ctx.profile(True)
     rp = solve(ib.STORE_FP32)
-    prof = {}
+    brk = {}
     names = {0: "spmv", 1: "fwd_sweep", 2: "bwd_sweep", 3: "vector", 4: "residual"}
     for cls, nm in names.items():
-        msum, cnt = ctx.profile_read(cls)
-        prof[nm] = (msum, cnt)
+        brk[nm] = ctx.profile_read(cls)
     ctx.profile(False)
-    iters = rp.iters
+    iters = r32.iters
     bm = bytes_model(P, 4)
     peak, peak_kind = _peaks()
+    shares = _launch_shares()
     kernels = {}
-    for nm, key in (("spmv", "spmv"), ("fwd_sweep", "fwd_sweep"), ("bwd_sweep", "bwd_sweep")):
-        msum, cnt = prof[nm]
+    for nm in ("spmv", "fwd_sweep", "bwd_sweep", "vector", "residual"):
+        b_ms, b_cnt = brk[nm]
+        per = "launch" if nm == "spmv" else "sweep" if nm.endswith("sweep") else "solve"
+        units = {"launch": iters + 1, "sweep": iters + 1, "solve": 1}[per]   # SpMV / sweeps: one per iteration + r0's
         if nm == "spmv":
-            per_launch_ms = msum / max(cnt, 1)
-            units = "launch"
+            units = iters
+        k = {"per": per, "bracketed_ms": round(b_ms / units, 5), "bracketed_launches": b_cnt}
+        if shares is not None and nm in shares:
+            k["share"] = round(shares[nm], 4)
+            k["ms"] = round(shares[nm] * ms_per / units, 5)
         else:
-            per_launch_ms = msum / max(iters + 1, 1)   # one sweep = nc color launches
-            units = "sweep"
-        gbs = bm[key] / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else 0.0
-        kernels[nm] = {"ms": round(per_launch_ms, 5), "per": units, "bytes": bm[key], "GB/s": round(gbs, 1),
-                       "frac": round(gbs / peak, 4), "launches": cnt}
-    kernels["vector"] = {"ms_total": round(prof["vector"][0], 4), "launches": prof["vector"][1]}
-    kernels["residual_replacement"] = {"ms_total": round(prof["residual"][0], 4), "launches": prof["residual"][1]}
+            k["ms"] = k["bracketed_ms"]
+        if nm in bm:
+            k["bytes"] = bm[nm]
+            gbs = bm[nm] / (k["ms"] * 1e-3) / 1e9 if k["ms"] > 0 else 0.0
+            k["GB/s"] = round(gbs, 1)
+            k["frac"] = round(gbs / peak, 4)
+        kernels[nm] = k
     # the dominant kernel: largest device time per solve; per-launch figures
     # (a sweep is one launch per color)
-    kernel_ms = {"spmv": prof["spmv"][0], "fwd_sweep": prof["fwd_sweep"][0], "bwd_sweep": prof["bwd_sweep"][0]}
+    kernel_ms = {nm: kernels[nm]["ms"] * (iters if nm == "spmv" else iters + 1)
+                 for nm in ("spmv", "fwd_sweep", "bwd_sweep")}
     dom_name = max(kernel_ms, key=kernel_ms.get)
     launches_per_unit = 1 if dom_name == "spmv" else max(1, P.nc)
     dom = dict(kernels[dom_name])
@@ -281,6 +342,11 @@ def run_gpu(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(P, samples=args.cpu_samples)
+    subs = None
+    if world == 1 and not args.no_sub_results:
+        ctx.close()
+        ctx = None
+        subs = sub_results(local)
 
     line = {
         "metric": METRIC,
@@ -296,13 +362,8 @@ def run_gpu(args):
         "dtype": "f64",
         "storage": "fp32 A and L, fp64 vectors and reductions",
         "data": "synthetic",
-        "config": {
-            "workload": WORKLOAD, "n": n, "nnz": P.A_run.nnz, "grid": f"{SIDE}^3", "coeffs": [1, 1, 0.01],
-            "block_size": BLOCK, "blocking": BLOCKING, "nb": P.nb, "colors": P.nc, "tol": TOL, "rr_interval": RR,
-            "x0": "zeros", "rhs": "b = A x*, x* ~ U(-1,1) splitmix64(0)",
-            "l2": "inputs larger than L2: ~0.5 GB streamed per iteration vs 126 MB L2",
-            "parallelism": f"replicas x{world}",
-        },
+        "config": headline_config(n, P.A_run.nnz, P.nb, P.nc),
+        "parallelism": f"replicas x{world}",
         "solves_per_s": round(tr.units_per_s, 3),
         "iters": r32.iters,
         "true_rel_resid": r32.true_rel_resid,
@@ -317,8 +378,12 @@ def run_gpu(args):
         "roofline": {"bound": "hbm", "kernel": dom_label, "achieved": dom["GB/s"],
                      "peak": peak, "unit": "GB/s", "frac": dom["frac"], "peak_source": peak_kind,
                      "traffic": traffic, "algorithmic_bytes_per_launch": dom["bytes"],
-                     "share_of_solve": round(kernel_ms[dom_name] / max(rp.solve_ms, 1e-9), 3)},
+                     "share_of_solve": round(kernel_ms[dom_name] / max(ms_per, 1e-9), 3)},
         "kernels": kernels,
+        "kernels_timing": ("ms = share of the solve in the committed ncu launch list (profiles/"
+                           "launches_solve_abmc128.md) x the event-timed solve; bracketed_ms: one extra solve "
+                           "with every launch bracketed by CUDA events, no graphs") if shares else
+                          "each launch bracketed by CUDA events in one extra solve (no graphs)",
         "iteration_bytes": bm["iteration"],
         "iteration_GBps": round(bm["iteration"] * iters / (rp.solve_ms * 1e-3) / 1e9, 1) if rp.solve_ms else None,
         "gpu_launches": int(launches),
@@ -328,12 +393,48 @@ def run_gpu(args):
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
-    ctx.close()
+    if subs is not None:
+        line["sub_results"] = subs
+    if ctx is not None:
+        ctx.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def _kernel_class(name: str):
+    """The solve part a kernel of the launch list belongs to (None: set-up)."""
+    import re
+    if name.startswith("iccg::k_spmv_q"):
+        return "spmv"
+    m = re.match(r"iccg::k_sweep_(?:st|chain|q2|q)<\w+, (\d)", name)
+    if m:
+        return "fwd_sweep" if m.group(1) == "1" else "bwd_sweep"
+    if name.startswith("iccg::k_persist"):
+        return "persistent"
+    if name.startswith(("iccg::k_update", "iccg::k_xpay", "iccg::k_copy", "iccg::k_resume")):
+        return "vector"
+    if name.startswith("iccg::k_residual_q"):
+        return "residual"
+    return None
+
+
+def _launch_shares(name: str = "launches_solve_abmc128.md"):
+    """Each solve part's share of the solve's device time, from the committed
+    ncu launch list (kernel, launches, total ms, share rows)."""
+    import re
+    p = ROOT / "profiles" / name
+    if not p.exists():
+        return None
+    tot = {}
+    for kname, _, ms, _ in re.findall(r"^\| `([^`]+)` \| (\d+) \| ([\d.]+) \| ([\d.]+)%", p.read_text(), re.M):
+        cls = _kernel_class(kname)
+        if cls is not None:
+            tot[cls] = tot.get(cls, 0.0) + float(ms)
+    s = sum(tot.values())
+    return {k: v / s for k, v in tot.items()} if s > 0 else None
 
 
 _PROFILE_OF = {"spmv": "ncu_spmv_abmc128.txt", "bwd_sweep": "ncu_sweep_st_abmc128.txt"}
@@ -381,6 +482,95 @@ def cpu_baseline(P, samples=3):
             "sample": f"1 full solve by the C restatement ({it} iterations)"}
 
 
+def headline_config(n: int, nnz: int, nb: int, nc: int) -> dict:
+    """The headline workload, the same in both arms' lines."""
+    return {"workload": WORKLOAD, "n": n, "nnz": nnz, "grid": f"{SIDE}^3", "coeffs": [1, 1, 0.01],
+            "block_size": BLOCK, "blocking": BLOCKING, "nb": nb, "colors": nc, "tol": TOL, "rr_interval": RR,
+            "x0": "zeros", "rhs": "b = A x*, x* ~ U(-1,1) splitmix64(0)",
+            "l2": "inputs larger than L2: ~0.5 GB streamed per iteration vs 126 MB L2"}
+
+
+def _splitmix_uniform(n: int, seed: int) -> np.ndarray:
+    """x_i ~ U(-1,1): the i-th splitmix64 output of `seed`, top 53 bits."""
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + (np.arange(1, n + 1, dtype=np.uint64) * np.uint64(0x9E3779B97F4A7C15))
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return (z >> np.uint64(11)).astype(np.float64) * 2.0 ** -53 * 2.0 - 1.0
+
+
+def reference_inputs(workdir: Path):
+    """The headline problem for the reference arm, made without this
+    package's library and read back through the reference's own readers
+    (read_matrix_market_crs, crs_io.cpp:73-159; ReadBlockFile_1Based /
+    ReadBlockColorFile_1Based, block.cpp:15-89), as its driver reads them.
+
+    The 3D 7-point stencil (x fastest; entries -0.01 (z-), -1 (y-), -1 (x-),
+    2 (1 + 1 + 0.01), -1 (x+), -1 (y+), -0.01 (z+)) is written as a
+    symmetric MatrixMarket file; blocks are 16 consecutive rows; the greedy
+    block coloring in block order of this bipartite block grid is the parity
+    of (block x + y + z), two colors.  b = A x* with x* the splitmix64(0)
+    U(-1,1) sequence, summed in row order."""
+    from oracle import bindings as ob
+    N = SIDE
+    n = N ** 3
+    idx = np.arange(n, dtype=np.int64)
+    x, y, z = idx % N, (idx // N) % N, idx // (N * N)
+    diag = 2.0 * (1.0 + 1.0 + 0.01)
+    # lower triangle, row by row: (z-), (y-), (x-), diagonal
+    parts = [(z > 0, -N * N, -0.01), (y > 0, -N, -1.0), (x > 0, -1, -1.0), (np.ones(n, bool), 0, diag)]
+    rows, cols, vals = [], [], []
+    for m, off, v in parts:
+        r = idx[m]
+        rows.append(r)
+        cols.append(r + off)
+        vals.append(np.full(r.size, v))
+    order = np.lexsort((np.concatenate(cols), np.concatenate(rows)))
+    I = np.concatenate(rows)[order] + 1
+    J = np.concatenate(cols)[order] + 1
+    V = np.concatenate(vals)[order]
+    u, inv = np.unique(V, return_inverse=True)
+    vs = np.array([repr(float(t)) for t in u])
+    lines = np.char.add(np.char.add(np.char.add(np.char.add(I.astype(str), " "), J.astype(str)), " "), vs[inv])
+    mtx = workdir / "laplace3d_aniso_128.mtx"
+    with open(mtx, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real symmetric\n")
+        f.write(f"{n} {n} {I.size}\n")
+        f.write("\n".join(lines.tolist()))
+        f.write("\n")
+    nb = n // BLOCK
+    blk = workdir / "laplace3d_aniso_128.blk"
+    with open(blk, "w") as f:
+        f.write(f"{nb}\n")
+        f.write("\n".join(f"{i + 1} {i // BLOCK + 1}" for i in range(n)))
+        f.write("\n")
+    b_idx = np.arange(nb)
+    bx, by, bz = b_idx % (N // BLOCK), (b_idx // (N // BLOCK)) % N, b_idx // ((N // BLOCK) * N)
+    bcolor = (bx + by + bz) % 2
+    bcol = workdir / "laplace3d_aniso_128.bcol"
+    with open(bcol, "w") as f:
+        f.write("2\n")
+        f.write("\n".join(f"{b + 1} {c + 1}" for b, c in enumerate(bcolor.tolist())))
+        f.write("\n")
+    # read back with the reference's readers
+    n_, rowptr, colind, val = ob.ref_read_mm(str(mtx))
+    block_of_old, nb_ = ob.ref_read_assignment(1, str(blk), n_)
+    block_color, nc = ob.ref_read_assignment(2, str(bcol), nb_)
+    R = ob.RefProblem(4, n_, rowptr, colind, val, block_of_old, nb_, block_color, nc)
+    # b = A x* in the original order (row order sums), then into the run order
+    xs = _splitmix_uniform(n_, 0)
+    b = np.zeros(n_)
+    cnt = np.diff(rowptr)
+    for j in range(int(cnt.max())):
+        has = cnt > j
+        pos = rowptr[:-1][has] + j
+        b[has] = b[has] + val[pos] * xs[colind[pos]]
+    b_run = np.empty_like(b)
+    b_run[R.perm()] = b
+    return R, b_run, headline_config(n_, int(rowptr[-1]), nb_, nc)
+
+
 def run_reference(args):
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
@@ -390,16 +580,17 @@ def run_reference(args):
     if ob.ref() is None:
         print(json.dumps({"impl": "reference", "unavailable": "compiled reference (oracle/_ref) not present"}))
         return
-    P, _ = build_problem()
-    n = P.A.n
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        R, b_run, config = reference_inputs(Path(td))
+    n = config["n"]
     cores = os.cpu_count() or 1
     ob.ref().ref_set_threads(cores)
-    R = ob.RefProblem(4, n, P.A.rowptr, P.A.colind, P.A.val, P.block_of_old, P.nb, P.block_color, P.nc)
     for _ in range(args.warmup):
-        R.cg(P.b_run, np.zeros(n), 10000, TOL)
+        R.cg(b_run, np.zeros(n), 10000, TOL)
     times, iters, rel = [], 0, 0.0
     for _ in range(args.steps):
-        x, it, rel, cv, us = R.cg(P.b_run, np.zeros(n), 10000, TOL)
+        x, it, rel, cv, us = R.cg(b_run, np.zeros(n), 10000, TOL)
         times.append(us / 1e3)
         iters = it
     ms = statistics.mean(times)
@@ -407,8 +598,8 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n": n, "nnz": P.A.nnz, "block_size": BLOCK, "tol": TOL,
-                   "parallelism": f"OpenMP x{cores} host threads"},
+        "config": config, "parallelism": f"OpenMP x{cores} host threads",
+        "inputs": "made with numpy, written as .mtx/.blk/.bcol and read by the reference's own readers",
         "iters": iters, "rel_resid": rel,
         "cpu_baseline": {"value": round(ms, 3), "unit": "ms", "cores": cores, "kind": "reference",
                          "sample": f"{args.steps} full solves (mean), conjugate_gradient only"},
@@ -425,6 +616,8 @@ def main():
     ap.add_argument("--impl", default="iccg_b200", choices=["iccg_b200", "reference"])
     ap.add_argument("--cpu-samples", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sub-results", action="store_true",
+                    help="headline only: leave out the C1 / C3 / batched sub-results")
     ap.add_argument("--kernel-only", choices=["spmv", "apply", "solve"], default=None,
                     help="set up the workload, then launch only this operation --reps times "
                          "(FP32 storage) and print its mean device time; for profilers")
@@ -443,8 +636,8 @@ def main():
                     help="diffusion27 with --kernel-only: the ordering of the system")
     ap.add_argument("--systems", type=int, default=512, help="batched: number of systems")
     ap.add_argument("--threads", type=int, default=16, help="batched / serving: concurrent solves")
-    ap.add_argument("--requests", type=int, default=200, help="serving: requests per arrival rate")
-    ap.add_argument("--max-points", type=int, default=100000, help="serving: largest kNN system")
+    ap.add_argument("--requests", type=int, default=400, help="serving: requests per arrival rate")
+    ap.add_argument("--max-points", type=int, default=1000000, help="serving: largest kNN system")
     args = ap.parse_args()
     if args.workload == "batched":
         run_batched(args)
@@ -606,11 +799,15 @@ def run_serving(args):
 
     Each request is a symmetrised 8-nearest-neighbour graph Laplacian plus
     1e-2 I, on N points with N log-uniform in [1e3, --max-points]. It gets a
-    seeded right-hand side and ABMC ICCG to 1e-8 with FP32 storage.
-    Requests are admitted under a 100 GB device-memory budget, and up to
-    `--threads` solves overlap. Each arrival rate reports p50 / p99 latency
-    (arrival to result, host set-up included) and solves/s. The comparison is
-    the same requests one at a time on the plain FP64 path.
+    seeded right-hand side and ABMC ICCG to 1e-8 with FP32 storage.  The
+    continuous-batching loop (iccg_b200.batch.ServingLoop) admits requests by
+    free device memory under a 100 GB budget, builds their systems on
+    --threads builder threads and steps every running solve together in one
+    batch session, retiring solves as they stop.  Each arrival rate reports
+    p50 / p99 latency (arrival to result, host set-up included) and solves/s.
+    The comparisons are the earlier thread-pool loop (one context and stream
+    per request) at the top rate and the same requests one at a time on the
+    plain FP64 path.
 
     Under torchrun (one process per GPU) every rank serves its share of the
     stream on its own GPU (iccg_b200.batch.serve_sharded), the arrival rates
@@ -633,6 +830,7 @@ def run_serving(args):
     rng = np.random.default_rng(5)
     lo, hi = np.log(1e3), np.log(float(args.max_points))
     sizes = [int(np.exp(rng.uniform(lo, hi))) for _ in range(args.requests * world)]
+    budget = 100 * 10**9
 
     def make_requests(rate):
         t, reqs = 0.0, []
@@ -643,20 +841,35 @@ def run_serving(args):
                                    bt.estimate_device_bytes(npts, 18 * npts)))
         return reqs
 
-    # service time one at a time (FP32 mixed and plain FP64) on a sample
+    # one request at a time, end to end (host set-up, upload, IC(0), mixed
+    # solve), and the plain FP64 solve alone, on a sample
     sample = sizes[:: max(1, len(sizes) // 16)]
-    alone_ms, plain_ms = [], []
+    alone_ms, plain_ms, bits_same = [], [], True
+    B = ib.Batch(local)
+    B.open(1, ib.STORE_FP32, rr_interval=RR, graph_iters=4)
     for i, npts in enumerate(sample):
         t0 = time.perf_counter()
         P = pb.config_knn(npts, seed=10_000 + i)
-        s = bt.ResidentSystem(P, device=local, storage=ib.STORE_FP32)
-        s.solve(P.b_run)
+        c = ib.Context(local)
+        bt.load_system(c, P, ib.STORE_FP32)
+        x = np.zeros(P.A_run.n)
+        r = c.solve(P.b_run, x, 10000, TOL, storage=ib.STORE_FP32, rr_interval=RR, graph_iters=4)
         alone_ms.append((time.perf_counter() - t0) * 1e3)
-        s.close()
-        s = bt.ResidentSystem(P, device=local, storage=ib.STORE_FP64)
-        _, _, wms = s.solve(P.b_run, mode=ib.MODE_PLAIN)
-        plain_ms.append(wms)
-        s.close()
+        # the same solve through a batch session: the same bits
+        k = B.add_system(c)
+        B.submit(k, P.b_run, None, 10000, TOL)
+        while True:
+            stopped, _ = B.step()
+            if stopped:
+                break
+        xb, rb = B.retire(stopped)
+        B.remove_system(k)
+        bits_same = bits_same and np.array_equal(xb[0], x) and rb[0].iters == r.iters
+        xp = np.zeros(P.A_run.n)
+        rp = c.solve(P.b_run, xp, 10000, TOL, storage=ib.STORE_FP64, mode=ib.MODE_PLAIN)
+        plain_ms.append(rp.solve_ms)
+        c.close()
+    B.close()
     sat = world * args.threads * 1000.0 / statistics.mean(alone_ms)
     if dist is not None:
         box = [sat]
@@ -664,23 +877,30 @@ def run_serving(args):
         sat = box[0]
     out = []
     for f in (0.25, 0.5, 1.0):
-        loop = bt.ServingLoop(budget_bytes=100 * 10**9, workers=args.threads, device=local)
+        loop = bt.ServingLoop(budget_bytes=budget, device=local, builders=args.threads, slots=1024,
+                              graph_iters=4, rr_interval=RR)
         st = bt.serve_sharded(make_requests(f * sat), loop, dist=dist)
         st["arrival_rate_per_s"] = round(f * sat, 2)
         out.append(st)
-    # the same top rate with a fresh context per request (no worker pool)
-    loop = bt.ServingLoop(budget_bytes=100 * 10**9, workers=args.threads, device=local, pool=False)
-    unpooled = bt.serve_sharded(make_requests(sat), loop, dist=dist)
-    unpooled["arrival_rate_per_s"] = round(sat, 2)
+    # the top rate on the thread-pool loop (one context and stream per request)
+    loop = bt.ThreadedServingLoop(budget_bytes=budget, workers=args.threads, device=local)
+    threaded = bt.serve_sharded(make_requests(sat), loop, dist=dist)
+    threaded["arrival_rate_per_s"] = round(sat, 2)
     line = {"workload": "serving", "n_gpus": world, "requests_per_rate": len(sizes),
-            "points": {"min": min(sizes), "max": max(sizes)},
-            "threads_per_gpu": args.threads, "budget_bytes_per_gpu": 100 * 10**9, "rates": out,
-            "context_per_request_at_top_rate": unpooled,
+            "points": {"min": min(sizes), "max": max(sizes), "distribution": "log-uniform",
+                       "max_points_arg": args.max_points},
+            "builders_per_gpu": args.threads, "budget_bytes_per_gpu": budget,
+            "admission": "free device memory (cudaMemGetInfo + idle pooled contexts - 2 GiB reserve) "
+                         "and the 100 GB budget",
+            "rates": out, "thread_pool_loop_at_top_rate": threaded,
             "one_at_a_time_ms": {"mixed_end_to_end_mean": round(statistics.mean(alone_ms), 3),
-                                 "plain_fp64_solve_mean": round(statistics.mean(plain_ms), 3)},
+                                 "plain_fp64_solve_mean": round(statistics.mean(plain_ms), 3),
+                                 "sample": len(sample)},
             "plain_fp64_one_at_a_time_solves_per_s": round(1000.0 / statistics.mean(plain_ms), 2),
+            "batch_session_same_bits_as_alone": bool(bits_same),
             "storage": "fp32 A and L, fp64 vectors", "preconditioner": "IC(0), ABMC B=16",
-            "data": "synthetic", "latency": "arrival to result, host set-up (kNN graph, blocking, PtAP) included"}
+            "data": "synthetic",
+            "latency": "arrival to result, host set-up (kNN graph, blocking, PtAP, upload, IC(0)) included"}
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

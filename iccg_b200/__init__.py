@@ -154,6 +154,12 @@ def lib() -> C.CDLL:
         "iccg_batch_add_system": (_I, [_P, _P, C.POINTER(_I)]),
         "iccg_batch_clear": (_I, [_P]),
         "iccg_batch_solve": (_I, [_P, _I, _P, _P, _P, _I, _D, C.POINTER(_Opts), _P]),
+        "iccg_batch_remove_system": (_I, [_P, _I]),
+        "iccg_batch_open": (_I, [_P, _I, C.POINTER(_Opts)]),
+        "iccg_batch_submit": (_I, [_P, _I, _P, _P, _I, _D, C.POINTER(_I)]),
+        "iccg_batch_step": (_I, [_P, _P, _I, C.POINTER(_I), C.POINTER(_I)]),
+        "iccg_batch_retire": (_I, [_P, _I, _P, _P, _P]),
+        "iccg_device_memory": (_I, [_I, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -602,6 +608,13 @@ class Context:
         return [(self.SWEEP_KINDS[k], int(g)) for k, g in zip(kinds[:nl.value], grids[:nl.value])]
 
 
+def device_memory(device: int = 0):
+    """(free, total) bytes of device memory (cudaMemGetInfo)."""
+    f, t = C.c_longlong(), C.c_longlong()
+    _check(lib().iccg_device_memory(int(device), C.byref(f), C.byref(t)))
+    return f.value, t.value
+
+
 class Batch:
     """Many independent solves advanced together (iccg_batch): one kernel
     launch per CG step for all of them.  Systems are Contexts with a matrix,
@@ -612,7 +625,9 @@ class Batch:
         h = C.c_void_p()
         _check(lib().iccg_batch_create(device, C.byref(h)))
         self.h = h
-        self._systems: List[Context] = []
+        self.device = device
+        self._systems: dict = {}      # index -> Context
+        self._slot_n: dict = {}       # slot -> rows of its system
 
     def close(self):
         if getattr(self, "h", None):
@@ -633,12 +648,65 @@ class Batch:
         """Adds a system (kept alive by the batch); returns its index."""
         idx = C.c_int()
         self._ck(lib().iccg_batch_add_system(self.h, ctx.h, C.byref(idx)))
-        self._systems.append(ctx)
+        self._systems[idx.value] = ctx
         return idx.value
+
+    def remove_system(self, index: int):
+        """Takes out a system none of whose solves is in flight."""
+        self._ck(lib().iccg_batch_remove_system(self.h, int(index)))
+        self._systems.pop(int(index), None)
 
     def clear(self):
         self._ck(lib().iccg_batch_clear(self.h))
-        self._systems = []
+        self._systems = {}
+
+    # -- continuous batching ------------------------------------------------
+    def open(self, slots: int, storage: int = STORE_FP64, rr_interval: int = 50, graph_iters: int = 8):
+        """Starts a session of `slots` solve slots (none may be in flight)."""
+        self._ck(lib().iccg_batch_open(self.h, int(slots), C.byref(_Opts(MODE_FUSED, storage, rr_interval,
+                                                                            graph_iters))))
+        self._slot_n = {}
+
+    def submit(self, system: int, b: np.ndarray, x0: Optional[np.ndarray] = None, max_iter: int = 10000,
+               tol: float = 1e-8) -> int:
+        """Admits a solve into a free slot (b and x0 are copied); returns the slot."""
+        ctx = self._systems.get(int(system))
+        if ctx is None:
+            raise ValueError(f"no system {system}")
+        b = _f64(b)
+        if b.shape != (ctx.n,):
+            raise ValueError(f"system {system} has {ctx.n} rows")
+        if x0 is not None:
+            x0 = _f64(x0)
+            if x0.shape != (ctx.n,):
+                raise ValueError(f"system {system} has {ctx.n} rows")
+        slot = C.c_int()
+        self._ck(lib().iccg_batch_submit(self.h, int(system), _ptr(b), _ptr(x0), int(max_iter), float(tol),
+                                         C.byref(slot)))
+        self._slot_n[slot.value] = ctx.n
+        return slot.value
+
+    def step(self, cap: int = 4096):
+        """Advances every running solve graph_iters iterations; returns (slots
+        that stopped, solves still running or waiting to start)."""
+        out = np.zeros(max(1, cap), np.int32)
+        ns, nr = C.c_int(), C.c_int()
+        self._ck(lib().iccg_batch_step(self.h, _ptr(out), int(cap), C.byref(ns), C.byref(nr)))
+        return [int(v) for v in out[:ns.value]], nr.value
+
+    def retire(self, slots: Sequence[int]):
+        """Solutions and results of stopped solves; frees their slots."""
+        slots = [int(s) for s in slots]
+        if not slots:
+            return [], []
+        xs = [np.zeros(self._slot_n[s]) for s in slots]
+        sv = _i32(slots)
+        xp = (C.c_void_p * len(slots))(*[x.ctypes.data for x in xs])
+        res = (_Result * len(slots))()
+        self._ck(lib().iccg_batch_retire(self.h, len(slots), _ptr(sv), xp, res))
+        for s in slots:
+            self._slot_n.pop(s, None)
+        return xs, [_cg_result(r) for r in res]
 
     @property
     def launches(self) -> int:
@@ -664,9 +732,9 @@ class Batch:
         sysv = _i32(systems)
         bv = [_f64(b) for b in bs]
         for s, (k, b, x) in enumerate(zip(sysv, bv, xs)):
-            if not 0 <= k < len(self._systems):
+            if int(k) not in self._systems:
                 raise ValueError(f"solve {s}: no system {k}")
-            n = self._systems[k].n
+            n = self._systems[int(k)].n
             if x.dtype != np.float64 or not x.flags.c_contiguous:
                 raise TypeError("x must be a contiguous float64 array (updated in place)")
             if b.shape != (n,) or x.shape != (n,):

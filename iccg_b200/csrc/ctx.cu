@@ -458,11 +458,13 @@ int iccg_sweep_plan(iccg_ctx* c, int storage, int fwd, int* kinds, int* grids, i
 // ---------------------------------------------------------------------------
 static void batch_free(iccg_batch* B)
 {
+    bat::drop_graph(B);
     if (B->ev0) cudaEventDestroy(B->ev0);
     if (B->ev1) cudaEventDestroy(B->ev1);
     for (auto e : B->evs)
         if (e) cudaEventDestroy(e);
     if (B->h_running) cudaFreeHost(B->h_running);
+    if (B->h_status) cudaFreeHost(B->h_status);
     cudaStream_t s = B->stream;
     delete B;  // device buffers free themselves
     if (s) cudaStreamDestroy(s);
@@ -479,6 +481,7 @@ int iccg_batch_create(int device, iccg_batch** out)
         CK(cudaGetDeviceCount(&ndev));
         if (device < 0 || device >= ndev) throw Error(ICCG_ERR_ARG, "no such CUDA device");
         CK(cudaDeviceGetAttribute(&B->nsm, cudaDevAttrMultiProcessorCount, device));
+        CK(cudaDeviceGetAttribute(&B->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
         CK(cudaStreamCreateWithFlags(&B->stream, cudaStreamNonBlocking));
         CK(cudaEventCreate(&B->ev0));
         CK(cudaEventCreate(&B->ev1));
@@ -515,16 +518,52 @@ int iccg_batch_add_system(iccg_batch* B, iccg_ctx* ctx, int* index)
         if (!ctx || !index) throw Error(ICCG_ERR_ARG, "null argument");
         if (ctx->device != B->device) throw Error(ICCG_ERR_ARG, "context on another device");
         require_precond(ctx);
-        *index = (int)B->sys.size();
-        B->sys.push_back(ctx);
+        for (const auto& h : B->sys)
+            if (h->c == ctx) throw Error(ICCG_ERR_ARG, "context already in the batch");
+        // a free entry (a removed system) is reused
+        int k = -1;
+        for (size_t i = 0; i < B->sys.size(); ++i)
+            if (!B->sys[i]->c) {
+                k = (int)i;
+                break;
+            }
+        if (k < 0) {
+            B->sys.push_back(std::make_unique<bat::SysHost>());
+            k = (int)B->sys.size() - 1;
+        }
+        bat::SysHost& H = *B->sys[(size_t)k];
+        H.c = ctx;
+        H.storage = -1;
+        H.active = 0;
+        B->sys_dirty = true;
+        *index = k;
+    });
+}
+
+int iccg_batch_remove_system(iccg_batch* B, int index)
+{
+    return bguard(B, [&] {
+        if (index < 0 || index >= (int)B->sys.size() || !B->sys[(size_t)index]->c)
+            throw Error(ICCG_ERR_ARG, "no such system in the batch");
+        bat::SysHost& H = *B->sys[(size_t)index];
+        if (H.active) throw Error(ICCG_ERR_STATE, "the system has solves in the batch");
+        CK(cudaStreamSynchronize(B->stream));
+        H.c = nullptr;
+        H.storage = -1;
+        H.bdb.release();
+        B->sys_dirty = true;
     });
 }
 
 int iccg_batch_clear(iccg_batch* B)
 {
     return bguard(B, [&] {
+        if (bat::in_flight(B)) throw Error(ICCG_ERR_STATE, "the batch has solves in flight");
         CK(cudaStreamSynchronize(B->stream));
+        bat::drop_graph(B);
         B->sys.clear();
+        B->sys_dirty = true;
+        B->lists_dirty = true;
     });
 }
 
@@ -538,12 +577,71 @@ int iccg_batch_solve(iccg_batch* B, int nsolve, const int* system, const double*
         if (B->sys.empty()) throw Error(ICCG_ERR_STATE, "the batch holds no system");
         iccg_solve_opts o{ICCG_MODE_FUSED, ICCG_STORE_FP64, 50, 8};
         if (opts) o = *opts;
-        if (o.graph_iters <= 0) o.graph_iters = 8;
-        if (o.mode != ICCG_MODE_FUSED) throw Error(ICCG_ERR_ARG, "batched solves run the fused form only");
         if (o.storage == ICCG_STORE_FP32) bat::run<float>(B, nsolve, system, b, x, max_iter, tol, o, res);
-        else if (o.storage == ICCG_STORE_FP64) bat::run<double>(B, nsolve, system, b, x, max_iter, tol, o, res);
-        else throw Error(ICCG_ERR_ARG, "unknown storage");
+        else bat::run<double>(B, nsolve, system, b, x, max_iter, tol, o, res);
     });
+}
+
+int iccg_batch_open(iccg_batch* B, int slots, const iccg_solve_opts* opts)
+{
+    return bguard(B, [&] {
+        iccg_solve_opts o{ICCG_MODE_FUSED, ICCG_STORE_FP64, 50, 8};
+        if (opts) o = *opts;
+        bat::open_session(B, slots, o);
+    });
+}
+
+int iccg_batch_submit(iccg_batch* B, int system, const double* b, const double* x0, int max_iter, double tol,
+                      int* slot)
+{
+    return bguard(B, [&] {
+        if (!slot) throw Error(ICCG_ERR_ARG, "null argument");
+        *slot = bat::submit(B, system, b, x0, max_iter, tol);
+    });
+}
+
+int iccg_batch_step(iccg_batch* B, int* stopped, int cap, int* nstopped, int* nrunning)
+{
+    return bguard(B, [&] {
+        if (!nstopped || (cap > 0 && !stopped)) throw Error(ICCG_ERR_ARG, "null argument");
+        if (B->storage < 0) throw Error(ICCG_ERR_STATE, "the batch is not open");
+        if (B->storage == ICCG_STORE_FP32) bat::step<float>(B, nrunning);
+        else bat::step<double>(B, nrunning);
+        const int k = std::min(cap, (int)B->report.size());
+        for (int i = 0; i < k; ++i) stopped[i] = B->report[(size_t)i];
+        B->report.erase(B->report.begin(), B->report.begin() + k);
+        *nstopped = k;
+    });
+}
+
+int iccg_batch_retire(iccg_batch* B, int n, const int* slots, double* const* x, iccg_result* res)
+{
+    return bguard(B, [&] {
+        if (n <= 0) return;
+        if (!slots || !x || !res) throw Error(ICCG_ERR_ARG, "null argument");
+        bat::retire(B, n, slots, x, res);
+    });
+}
+
+int iccg_device_memory(int device, long long* free_bytes, long long* total_bytes)
+{
+    if (!free_bytes || !total_bytes) return ICCG_ERR_ARG;
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess) return ICCG_ERR_CUDA;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return ICCG_ERR_ARG;
+    }
+    size_t f = 0, t = 0;
+    const cudaError_t e = cudaMemGetInfo(&f, &t);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return ICCG_ERR_CUDA;
+    }
+    *free_bytes = (long long)f;
+    *total_bytes = (long long)t;
+    return ICCG_OK;
 }
 
 }  // extern "C"

@@ -49,6 +49,7 @@ struct SolverState {
     int true_check;   // 1: a recurrence residual below tol asks for an FP64 residual check in the same
                       // iteration (rr_flag) instead of stopping with kTrueCheck (the batched solves)
     unsigned long long t_stop;  // %globaltimer (ns) when the solve stopped (0 while running)
+    unsigned long long t_start; // %globaltimer (ns) when a batched solve was admitted
 };
 
 __device__ __forceinline__ unsigned long long global_ns()

@@ -370,6 +370,35 @@ int iccg_batch_clear(iccg_batch* batch);
 int iccg_batch_solve(iccg_batch* batch, int nsolve, const int* system, const double* const* b,
                      double* const* x, int max_iter, double tol, const iccg_solve_opts* opts,
                      iccg_result* res);
+/* A system whose solves have all been retired leaves the batch; its index
+   may be given to a later iccg_batch_add_system. */
+int iccg_batch_remove_system(iccg_batch* batch, int index);
+
+/* Continuous batching (a serving loop): solves enter and leave while others
+   run.  iccg_batch_open starts a session of `slots` solve slots with the
+   given options (storage, rr_interval, graph_iters; mode must be FUSED); no
+   solve may be in flight.  iccg_batch_submit admits a solve of system
+   `system` into a free slot (*slot receives it): b and x0 (x0 NULL = zeros)
+   are copied before it returns; its start-up (r0, z0, p0) runs with the next
+   step.  iccg_batch_step advances every running solve graph_iters
+   iterations in one graph launch (each CG kernel one launch over all of
+   them), waits for it, and writes up to cap slots whose solves stopped and
+   were not reported before into stopped[] (*nstopped of them; the rest come
+   with the next calls); *nrunning (may be NULL) receives the solves still
+   running or waiting to start.  iccg_batch_retire copies the solutions of
+   n stopped solves into x[i] (host, n doubles of the solve's system, A_run
+   order), fills res[i] (solve_ms: device time from admission to the stop)
+   and frees their slots.  A solve gives the same bits, iterations and
+   residuals as iccg_solve on its context alone, whatever runs beside it. */
+int iccg_batch_open(iccg_batch* batch, int slots, const iccg_solve_opts* opts);
+int iccg_batch_submit(iccg_batch* batch, int system, const double* b, const double* x0, int max_iter,
+                      double tol, int* slot);
+int iccg_batch_step(iccg_batch* batch, int* stopped, int cap, int* nstopped, int* nrunning);
+int iccg_batch_retire(iccg_batch* batch, int n, const int* slots, double* const* x, iccg_result* res);
+
+/* free and total device memory of `device` (cudaMemGetInfo), for admission
+   by free device memory */
+int iccg_device_memory(int device, long long* free_bytes, long long* total_bytes);
 
 #ifdef __cplusplus
 }

@@ -146,3 +146,62 @@ def test_gpu_batch_rejects_bad_arguments():
     B.close()
     ctx.close()
     plain.close()
+
+
+@pytest.mark.parametrize("storage", [ib.STORE_FP64, ib.STORE_FP32])
+def test_gpu_continuous_batching_equals_solves_alone(storage):
+    """Solves admitted while others run (a new one every step, into slots
+    freed by retired ones), systems taken out and added again: every result
+    is the same bits as the solve alone."""
+    probs = [pb.make(pb.poisson2d(s), "piccg", seed=s) for s in (12, 30, 47)]
+    probs += [pb.config_abmc_aniso(s, 16, "bfs", seed=s) for s in (9, 14)]
+    probs += [pb.config_knn(2500, seed=3, block_size=16)]
+    ctxs = [_ctx(P) for P in probs]
+    alone = [_alone(c, P.b_run, storage, rr_interval=20) for c, P in zip(ctxs, probs)]
+    B = ib.Batch(0)
+    B.open(4, storage, rr_interval=20, graph_iters=2)          # fewer slots than requests
+    order = [0, 1, 2, 3, 4, 5, 2, 0, 5, 3, 1, 4]
+    queue = list(order)
+    live = {}                                                    # slot -> (problem index, system index)
+    held = {}                                                    # problem index -> [system index, solves]
+    done = []
+    steps = 0
+    while queue or live:
+        if queue and len(live) < 4:
+            i = queue.pop(0)
+            if i not in held:
+                held[i] = [B.add_system(ctxs[i]), 0]
+            held[i][1] += 1
+            live[B.submit(held[i][0], probs[i].b_run, None, 10000, 1e-8)] = (i, held[i][0])
+        stopped, running = B.step()
+        steps += 1
+        assert running <= len(live)
+        if stopped:
+            xs, res = B.retire(stopped)
+            for s, x, r in zip(stopped, xs, res):
+                i, k = live.pop(s)
+                held[i][1] -= 1
+                if held[i][1] == 0:
+                    B.remove_system(k)
+                    del held[i]
+                done.append(i)
+                _same((x, r), alone[i])
+                assert r.solve_ms > 0
+    assert sorted(done) == sorted(order)
+    assert steps > len(order)
+    # retiring a running or free slot is refused
+    k = B.add_system(ctxs[2])
+    s = B.submit(k, probs[2].b_run)
+    with pytest.raises(ib.IccgError):
+        B.retire([s])
+    with pytest.raises(ib.IccgError):
+        B.remove_system(k)
+    while True:
+        stopped, _ = B.step()
+        if stopped:
+            break
+    xs, res = B.retire(stopped)
+    _same((xs[0], res[0]), alone[2])
+    B.close()
+    for c in ctxs:
+        c.close()

@@ -136,7 +136,7 @@ def _serve_rank(rank, world, port, out):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
     try:
         import iccg_b200.batch as bt
-        loop = bt.ServingLoop(budget_bytes=1 << 30, workers=2, make_system=_FakeSystem, make_context=_FakeCtx)
+        loop = bt.ThreadedServingLoop(budget_bytes=1 << 30, workers=2, make_system=_FakeSystem, make_context=_FakeCtx)
         out[rank] = bt.serve_sharded(_requests(11), loop, dist=dist)
     finally:
         dist.destroy_process_group()
@@ -167,6 +167,6 @@ def test_serving_sharded_over_two_ranks_gloo():
 
 def test_serving_sharded_single_process():
     import iccg_b200.batch as bt
-    loop = bt.ServingLoop(budget_bytes=1 << 30, workers=3, make_system=_FakeSystem, make_context=_FakeCtx)
+    loop = bt.ThreadedServingLoop(budget_bytes=1 << 30, workers=3, make_system=_FakeSystem, make_context=_FakeCtx)
     s = bt.serve_sharded(_requests(7), loop)
     assert s["ranks"] == 1 and s["solves"] == 7 and s["solves_per_rank"] == [7] and s["failed"] == 0
