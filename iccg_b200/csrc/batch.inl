@@ -675,6 +675,7 @@ static int submit(iccg_batch* B, int k, const double* b, const double* x0, int m
     q.max_iter = max_iter;
     q.rr_interval = B->storage == ICCG_STORE_FP32 ? B->opts.rr_interval : 0;
     q.true_check = 1;
+    q.xdefer_k = -1;
     const size_t nb = sizeof(double) * (size_t)n;
     CK(cudaMemcpyAsync(B->dsol.get() + s, &v, sizeof(BSolve), cudaMemcpyHostToDevice, B->stream));
     CK(cudaMemcpyAsync(B->dstate.get() + s, &q, sizeof(SolverState), cudaMemcpyHostToDevice, B->stream));

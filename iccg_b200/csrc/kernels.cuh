@@ -50,6 +50,8 @@ struct SolverState {
                       // iteration (rr_flag) instead of stopping with kTrueCheck (the batched solves)
     unsigned long long t_stop;  // %globaltimer (ns) when the solve stopped (0 while running)
     unsigned long long t_start; // %globaltimer (ns) when a batched solve was admitted
+    int xdefer_k;     // the last iteration whose x += alpha p waits for the p update (FIN_UPDX); -1: none
+    int xp;           // 1: the solve stopped before that x update (applied by k_apply_xp)
 };
 
 __device__ __forceinline__ unsigned long long global_ns()
@@ -68,6 +70,8 @@ enum Fin {
     FIN_UPD,    // (r.r): rel, convergence / replacement trigger
     FIN_TRUE,   // (r.r) of the replaced residual: convergence
     FIN_RZ,     // (r.z): beta, rz_old
+    FIN_UPDX,   // FIN_UPD where x += alpha p waits for the p update (the update fused into the
+                // forward sweep): a stop here, or at this iteration's beta, leaves it pending (xp)
 };
 
 struct RedBuf {
@@ -136,11 +140,16 @@ __device__ void finish(const double* v, SolverState* st, double* out)
         st->alpha = st->rz_old / pAp;
         return;
     }
-    if (FIN == FIN_UPD) {
+    if (FIN == FIN_UPD || FIN == FIN_UPDX) {
+        if (FIN == FIN_UPDX) st->xdefer_k = st->k;
         const double rel = sqrt(v[0]) / st->normb;
         st->iters = st->k + 1;
         st->rel_resid = rel;
-        if (!isfinite(rel)) { status = kNonFinite; return; }
+        if (!isfinite(rel)) {
+            status = kNonFinite;
+            if (FIN == FIN_UPDX) st->xp = 1;
+            return;
+        }
         if (st->rr_interval <= 0) {
             if (rel < st->tol) status = kConverged;
         } else if (rel < st->tol) {
@@ -149,6 +158,7 @@ __device__ void finish(const double* v, SolverState* st, double* out)
         } else if ((st->k + 1) % st->rr_interval == 0) {
             st->rr_flag = 1;
         }
+        if (FIN == FIN_UPDX && status != kRunning) st->xp = 1;
         return;
     }
     if (FIN == FIN_TRUE) {
@@ -163,7 +173,11 @@ __device__ void finish(const double* v, SolverState* st, double* out)
         const double rz = v[0];
         st->beta = rz / st->rz_old;
         st->rz_old = rz;
-        if (!isfinite(st->beta)) { status = kNonFinite; st->iters = st->k + 1; }
+        if (!isfinite(st->beta)) {
+            status = kNonFinite;
+            st->iters = st->k + 1;
+            if (st->xdefer_k == st->k) st->xp = 1;
+        }
         return;
     }
 }
@@ -344,9 +358,11 @@ __global__ void __launch_bounds__(256) k_update(int n, double alpha_arg, const d
 }
 
 // p = z + beta p (cg_crs.cpp:155-157); the fused form then advances k and
-// stops the solve after max_iter iterations (cg_crs.cpp:125).
+// stops the solve after max_iter iterations (cg_crs.cpp:125).  With x
+// (the update fused into the forward sweep) x += alpha p comes first, with
+// the p of this iteration (cg_crs.cpp:137-138).
 __global__ void __launch_bounds__(256) k_xpay(int n, double beta_arg, const double* __restrict__ z,
-                                              double* __restrict__ p, SolverState* st)
+                                              double* __restrict__ p, SolverState* st, double* __restrict__ x)
 {
     grid_dep_begin();
     if (st) {
@@ -359,17 +375,27 @@ __global__ void __launch_bounds__(256) k_xpay(int n, double beta_arg, const doub
     }
     if (st_done(st)) return;
     const double beta = st ? st->beta : beta_arg;
-    if ((((uintptr_t)z | (uintptr_t)p) & 15) != 0) {
-        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    const double alpha = (st && x) ? st->alpha : 0.0;
+    if ((((uintptr_t)z | (uintptr_t)p | (uintptr_t)x) & 15) != 0) {
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+            if (x) x[k] = fma(alpha, p[k], x[k]);
             p[k] = fma(beta, p[k], z[k]);
+        }
     } else {
         const int n2 = n >> 1;
         const int stride = gridDim.x * blockDim.x;
         const double2* __restrict__ z2 = reinterpret_cast<const double2*>(z);
         double2* __restrict__ p2 = reinterpret_cast<double2*>(p);
+        double2* __restrict__ x2 = reinterpret_cast<double2*>(x);
         auto pair = [&](int i) {
             const double2 zv = z2[i];
             double2 pv = p2[i];
+            if (x) {
+                double2 xv = x2[i];
+                xv.x = fma(alpha, pv.x, xv.x);
+                xv.y = fma(alpha, pv.y, xv.y);
+                x2[i] = xv;
+            }
             pv.x = fma(beta, pv.x, zv.x);
             pv.y = fma(beta, pv.y, zv.y);
             p2[i] = pv;
@@ -380,7 +406,10 @@ __global__ void __launch_bounds__(256) k_xpay(int n, double beta_arg, const doub
             pair(i + stride);
         }
         if (i < n2) pair(i);
-        if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) p[n - 1] = fma(beta, p[n - 1], z[n - 1]);
+        if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+            if (x) x[n - 1] = fma(alpha, p[n - 1], x[n - 1]);
+            p[n - 1] = fma(beta, p[n - 1], z[n - 1]);
+        }
     }
     grid_dep_trigger();
     if (st && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -388,6 +417,24 @@ __global__ void __launch_bounds__(256) k_xpay(int n, double beta_arg, const doub
         st->k = k1;
         if (k1 >= st->max_iter) st->status = kMaxIter;
     }
+}
+
+// x += alpha p of a solve that stopped between the fused update and the p
+// update (xp set by FIN_UPDX / FIN_RZ); k_clear_xp clears the mark after it
+__global__ void __launch_bounds__(256) k_apply_xp(int n, const double* __restrict__ p, double* __restrict__ x,
+                                                  const SolverState* st)
+{
+    grid_dep_begin();
+    if (!st->xp) return;
+    const double alpha = st->alpha;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        x[k] = fma(alpha, p[k], x[k]);
+}
+
+__global__ void k_clear_xp(SolverState* st)
+{
+    grid_dep_begin();
+    st->xp = 0;
 }
 
 // resumes a solve stopped at kTrueCheck with the replacement requested
@@ -521,25 +568,18 @@ __global__ void __launch_bounds__(256) k_sweep(SweepArgs a, int u0, int u1, int 
 // results keep its bits.  Vectors live in Q order; they are permuted only at
 // the API boundary.
 // ---------------------------------------------------------------------------
-// The CG update fused into the forward sweep (FIN_UPD): x += alpha p,
-// r -= alpha Ap (cg_crs.cpp:137-141) for each row as the sweep loads it;
-// the new r is the row's input and r.r is reduced by the sweep's launches
-// (the residual test of cg_crs.cpp:143).  The arithmetic is k_update's.
+// The CG update fused into the forward sweep (FIN_UPDX): r -= alpha Ap
+// (cg_crs.cpp:139-141) for each row as the sweep stages it -- r and Ap come
+// into the tile with the batch's other arrays -- and the new r is written
+// back, is the row's input, and r.r is reduced by the sweep's launches (the
+// residual test of cg_crs.cpp:143).  x += alpha p (cg_crs.cpp:137-138) waits
+// for the p update, which reads p anyway (k_xpay with x); a stop in between
+// leaves it pending in the state (xp) for k_apply_xp.  The arithmetic of
+// each element is k_update's.
 struct UpdArgs {
     double* r;
-    double* x;
-    const double* p;
     const double* Ap;
 };
-
-__device__ __forceinline__ double cg_update_row(const UpdArgs& U, double alpha, int q)
-{
-    const double rq = U.r[q], apq = U.Ap[q], pq = U.p[q], xq = U.x[q];
-    U.x[q] = fma(alpha, pq, xq);
-    const double rn = fma(-alpha, apq, rq);
-    U.r[q] = rn;
-    return rn;
-}
 
 struct SellMat {
     const int* ptr;       // first slot of each slice
@@ -1439,33 +1479,36 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
 {
     grid_dep_begin();
     if (st_done(st)) return;
-    // FIN_UPD (forward, one buffer): the fused CG update writes each
-    // batch's inputs into its tile
-    constexpr bool UPD = FIN == FIN_UPD;
+    // FIN_UPDX (forward, one buffer): the fused CG update; each batch's r
+    // and Ap are staged (Ap in the area of the backward sweep's r)
+    constexpr bool UPD = FIN == FIN_UPDX;
     static_assert(!UPD || (FWD && NB == 1), "the fused update runs in single-buffered forward sweeps");
     constexpr bool with_r = FIN == FIN_RZ || FIN == FIN_RZ0;
     constexpr bool with_pv = !(FWD || !EXACT);
     const double alpha = UPD ? st->alpha : 0.0;
     extern __shared__ __align__(16) unsigned char smem_st[];
-    const StageLayout Ly = stage_layout(rows_cap, slots_cap, slices_cap, (int)sizeof(T), with_r, with_pv);
+    const StageLayout Ly = stage_layout(rows_cap, slots_cap, slices_cap, (int)sizeof(T), with_r || UPD, with_pv);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const double* prev = out;  // earlier-level values: read-only in this launch
     acc2 rz[1] = {{0.0, 0.0}};
+    const double* stage2 = UPD ? U.Ap : rdot;
 
-    // the fused update of a just-staged batch's rows, into the tile
+    // the fused update of a staged batch's rows (after its copy landed):
+    // r -= alpha Ap in the tile and back to r
     auto update = [&](unsigned char* base, const BatchDesc& d) {
         double* s_in = reinterpret_cast<double*>(base + Ly.in) + (d.qb & 1);
+        const double* s_ap = reinterpret_cast<const double*>(base + Ly.rd) + (d.qb & 1);
         for (int i = threadIdx.x; i < d.qe - d.qb; i += blockDim.x) {
-            const double rn = cg_update_row(U, alpha, d.qb + i);
+            const double rn = fma(-alpha, s_ap[i], s_in[i]);
             s_in[i] = rn;
+            U.r[d.qb + i] = rn;
             acc2_fma(rz[0], rn, rn);
         }
     };
     int b = b0 + blockIdx.x;
     if (b < b1) {
         BatchDesc cur = bd[b];
-        stage_batch<T, FWD, with_r, !UPD>(smem_st, Ly, cur, meta, M, dg, in, rdot);
-        if (UPD) update(smem_st, cur);
+        stage_batch<T, FWD, with_r || UPD>(smem_st, Ly, cur, meta, M, dg, in, stage2);
         bool has_next = b + (int)gridDim.x < b1;
         BatchDesc nxt = cur;
         if (has_next) nxt = bd[b + gridDim.x];
@@ -1474,7 +1517,8 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
             // is worked on; NB = 1: one buffer, refilled after each batch
             unsigned char* base = smem_st + (NB == 2 ? (i & 1) * Ly.bytes : 0);
             if (NB == 2 && has_next)
-                stage_batch<T, FWD, with_r, !UPD>(smem_st + ((i + 1) & 1) * Ly.bytes, Ly, nxt, meta, M, dg, in, rdot);
+                stage_batch<T, FWD, with_r || UPD>(smem_st + ((i + 1) & 1) * Ly.bytes, Ly, nxt, meta, M, dg, in,
+                                                   stage2);
             const bool has_nn = has_next && b + 2 * (int)gridDim.x < b1;
             BatchDesc nn = nxt;
             if (has_nn) nn = bd[b + 2 * gridDim.x];
@@ -1491,6 +1535,10 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
             if (NB == 2 && has_next) cp_async_wait<1>();
             else cp_async_wait<0>();
             __syncthreads();
+            if (UPD) {
+                update(base, cur);
+                __syncthreads();
+            }
 
             st_gather<T, FWD, EXACT, false>(cur, base, Ly, rows_cap, prev);
             __syncthreads();
@@ -1498,10 +1546,7 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
             st_chain<T, FWD, EXACT, with_r>(cur, base, Ly, rows_cap, gl, gs, out, rz[0]);
             __syncthreads();
             if (!has_next) break;
-            if (NB == 1) {
-                stage_batch<T, FWD, with_r, !UPD>(smem_st, Ly, nxt, meta, M, dg, in, rdot);
-                if (UPD) update(smem_st, nxt);
-            }
+            if (NB == 1) stage_batch<T, FWD, with_r || UPD>(smem_st, Ly, nxt, meta, M, dg, in, stage2);
             b += gridDim.x;
             cur = nxt;
             nxt = nn;
@@ -1532,7 +1577,7 @@ __global__ void __launch_bounds__(256) k_sweep_chain(int g0, int g1, const int* 
 {
     grid_dep_begin();
     if (st_done(st)) return;
-    constexpr bool UPD = FIN == FIN_UPD;  // forward: the fused CG update on load
+    constexpr bool UPD = FIN == FIN_UPDX;  // forward: the fused CG update (r -= alpha Ap) on load
     constexpr bool with_r = FIN == FIN_RZ || FIN == FIN_RZ0;
     constexpr int CH = 4;
     const double alpha = UPD ? st->alpha : 0.0;
@@ -1540,7 +1585,7 @@ __global__ void __launch_bounds__(256) k_sweep_chain(int g0, int g1, const int* 
     const int lane = threadIdx.x & 31;
     acc2 rz[1] = {{0.0, 0.0}};
     struct Chunk {
-        double a[CH], rd[CH];
+        double a[CH], rd[CH];  // rd: r (backward r.z) or Ap (the fused update)
         T v[CH], p[CH];
         int L[CH], q[CH];
     };
@@ -1564,16 +1609,11 @@ __global__ void __launch_bounds__(256) k_sweep_chain(int g0, int g1, const int* 
                 const int p = __shfl_sync(0xffffffffu, my_p, rs) + lane;
                 const int w = __shfl_sync(0xffffffffu, my_w, rs);
                 C.q[u] = q;
-                if (UPD) {
-                    C.a[u] = ok ? cg_update_row(U, alpha, q) : 0.0;
-                    if (ok) acc2_fma(rz[0], C.a[u], C.a[u]);
-                } else {
-                    C.a[u] = ok ? in[q] : 0.0;
-                }
+                C.a[u] = ok ? in[q] : 0.0;
                 C.p[u] = ok ? dg[q] : (T)1;
                 C.L[u] = ok ? M.len[q] & 0xffff : 0;
                 C.v[u] = (ok && w > 0) ? val[p] : (T)0;
-                C.rd[u] = (with_r && ok) ? rdot[q] : 0.0;
+                C.rd[u] = ok ? (with_r ? rdot[q] : UPD ? U.Ap[q] : 0.0) : 0.0;
             }
         };
         double last = 0.0;
@@ -1585,6 +1625,11 @@ __global__ void __launch_bounds__(256) k_sweep_chain(int g0, int g1, const int* 
             for (int u = 0; u < CH; ++u) {
                 if (t0 + u < len) {
                     double a = A.a[u];
+                    if (UPD) {
+                        a = fma(-alpha, A.rd[u], a);
+                        U.r[A.q[u]] = a;
+                        acc2_fma(rz[0], a, a);
+                    }
                     const double x = fma(-(double)A.v[u], last, a);
                     a = A.L[u] ? x : a;
                     const double v = EXACT ? a / (double)A.p[u] : a * (double)A.p[u];

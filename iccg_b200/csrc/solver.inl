@@ -115,11 +115,12 @@ static void launch_sweep_level(iccg_ctx* c, int l, const SweepLevel& sl, const d
     case 1: {
         const int slots = FWD ? Q.st_slotsS[l_] : Q.st_slotsT[l_];
         const int nbuf = c->stage_bufs == 1 ? 1 : 2;
-        constexpr bool with_r = FIN == FIN_RZ || FIN == FIN_RZ0;
+        // the fused update stages Ap in the area of the backward sweep's r
+        constexpr bool with_r = FIN == FIN_RZ || FIN == FIN_RZ0 || FIN == FIN_UPDX;
         const size_t smem = nbuf * (size_t)stage_layout(Q.st_rows[l_], slots, Q.st_slices[l_], (int)sizeof(T),
                                                         with_r, !FWD && exact)
                                        .bytes;
-        if constexpr (FIN == FIN_UPD) {
+        if constexpr (FIN == FIN_UPDX) {
             // the fused update runs single-buffered only (fused_update_ok)
             auto kern = k_sweep_st<T, FWD, FIN, exact, 1>;
             allow_smem(c, kern);
@@ -165,9 +166,10 @@ static bool fused_update_ok(iccg_ctx* c)
     return true;
 }
 
-// z = M^{-1} r.  UPD: the forward levels first do the CG update x += alpha
-// p, r -= alpha Ap of their rows (U) and reduce r.r over all their launches
-// (FIN_UPD at the last CTA of the last forward level).
+// z = M^{-1} r.  UPD: the forward levels first do the CG update r -= alpha
+// Ap of their rows (U; x += alpha p waits for the p update) and reduce r.r
+// over all their launches (FIN_UPDX at the last CTA of the last forward
+// level).
 template <class T, int FIN, bool UPD = false>
 static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, SolverState* st, UpdArgs U = UpdArgs{})
 {
@@ -185,7 +187,7 @@ static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, Solv
         }
         int s0 = 0;
         for (int l = 0; l < Q.nlevels; ++l) {
-            launch_sweep_level<T, FIN_UPD, true>(c, l, fl[(size_t)l], r, y, nullptr, s0, fslots, st, U);
+            launch_sweep_level<T, FIN_UPDX, true>(c, l, fl[(size_t)l], r, y, nullptr, s0, fslots, st, U);
             s0 += fl[(size_t)l].grid;
         }
     } else {
@@ -342,7 +344,7 @@ static void solve_plain(iccg_ctx* c, const double* b, double* x, int max_iter, d
         apply_path<FIN_NONE>(c, ICCG_STORE_FP64, r, z, nullptr);
         const double rz_new = dot_dev(c, n, r, z);
         const double beta = rz_new / rz_old;
-        launch_n(c, 3, k_xpay, (long long)c->n, n, beta, (const double*)z, p, (SolverState*)nullptr);
+        launch_n(c, 3, k_xpay, (long long)c->n, n, beta, (const double*)z, p, (SolverState*)nullptr, (double*)nullptr);
         rz_old = rz_new;
     }
     res->status = kMaxIter;
@@ -362,23 +364,24 @@ static void fused_iteration(iccg_ctx* c, int storage, bool rr, const double* b, 
         // update, both sweeps and the two reductions in one launch
         if (storage == ICCG_STORE_FP32) launch_persist<float, true, FIN_RZ>(c, c->vr.get(), c->vy.get(), c->vz.get(), st, x);
         else launch_persist<double, true, FIN_RZ>(c, c->vr.get(), c->vy.get(), c->vz.get(), st, x);
-        launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st);
+        launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st, (double*)nullptr);
         return;
     }
     const bool f32 = storage == ICCG_STORE_FP32;
     if (!rr && (f32 ? fused_update_ok<float>(c) : fused_update_ok<double>(c))) {
         // the update inside the forward sweep's launches
-        const UpdArgs U{c->vr.get(), x, c->vp.get(), c->vAp.get()};
+        const UpdArgs U{c->vr.get(), c->vAp.get()};
         if (f32) apply_ic0_q<float, FIN_RZ, true>(c, c->vr.get(), c->vy.get(), c->vz.get(), st, U);
         else apply_ic0_q<double, FIN_RZ, true>(c, c->vr.get(), c->vy.get(), c->vz.get(), st, U);
-        launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st);
+        // x += alpha p, then p = z + beta p
+        launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st, x);
         return;
     }
     launch_n(c, 3, k_update<FIN_UPD>, (long long)c->n, n, 0.0, (const double*)c->vp.get(), (const double*)c->vAp.get(), x,
            c->vr.get(), st, red, c->ticket.get());
     if (rr) residual_path<FIN_TRUE>(c, (const double*)x, b, c->vr.get(), st);
     apply_path<FIN_RZ>(c, storage, c->vr.get(), c->vz.get(), st);
-    launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st);
+    launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st, (double*)nullptr);
 }
 
 // releases every captured iteration graph of the context
@@ -402,6 +405,7 @@ static void solve_fused(iccg_ctx* c, const double* b, double* x, int max_iter, d
     s0.pend = kRunning;
     s0.max_iter = max_iter;
     s0.rr_interval = rr ? o.rr_interval : 0;
+    s0.xdefer_k = -1;
     *c->h_state = s0;
     CK(cudaMemcpyAsync(c->state.get(), c->h_state, sizeof(SolverState), cudaMemcpyHostToDevice, c->stream));
     unsigned int zero = 0;
@@ -510,15 +514,21 @@ static void solve_fused(iccg_ctx* c, const double* b, double* x, int max_iter, d
         // and, if it is not below the tolerance, finish this iteration
         // (z = M^-1 r, beta, p) and go on.
         CK(cudaStreamSynchronize(c->stream));
+        // x += alpha p where the fused update left it to the p update
+        launch_n(c, 3, k_apply_xp, (long long)c->n, n, (const double*)c->vp.get(), x, (const SolverState*)st);
+        launch(c, 3, k_clear_xp, 1, 1, st);
         launch(c, 3, k_resume_true_check, 1, 1, st);
         residual_path<FIN_TRUE>(c, (const double*)x, b, c->vr.get(), st);
         apply_path<FIN_RZ>(c, storage, c->vr.get(), c->vz.get(), st);
-        launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st);
+        launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st, (double*)nullptr);
         CK(cudaMemcpyAsync(c->h_state, st, sizeof(SolverState), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
         if (c->h_state->status != kRunning) break;
         k_base = c->h_state->k;
     }
+    // a stop between the fused update and the p update leaves x += alpha p
+    launch_n(c, 3, k_apply_xp, (long long)c->n, n, (const double*)c->vp.get(), x, (const SolverState*)st);
+    launch(c, 3, k_clear_xp, 1, 1, st);
     CK(cudaEventRecord(c->ev1, c->stream));
     CK(cudaMemcpyAsync(c->h_state, st, sizeof(SolverState), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));

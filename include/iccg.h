@@ -224,9 +224,12 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
    forward level runs the chain-only or single-buffered staged kernel), so
    the update needs no launch and r is not read back; 0 launches the update
    on its own.  Iterations with a residual replacement always update on
-   their own.  The fused form loads p, Ap, x and r of each batch's rows
-   synchronously before the batch's sweep, which costs more than the launch
-   it saves on the 128^3 ABMC system; it is kept as an option. */
+   their own.  The fused form stages r and Ap with each batch, writes the new
+   r back, and leaves x += alpha p to the p update (k_xpay); the same bits
+   as the update on its own.  On the 128^3 ABMC system it is slower
+   (22.50 against 21.78 ms mixed, 34.85 against 32.66 ms FP64): the
+   chain-only forward level, latency-bound, loses more than the launch and
+   the bytes saved; it is kept as an option. */
 #define ICCG_OPT_TILED 0
 #define ICCG_OPT_SWEEP 1
 #define ICCG_OPT_PDL 2
