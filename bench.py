@@ -622,6 +622,8 @@ def main():
                     help="set up the workload, then launch only this operation --reps times "
                          "(FP32 storage) and print its mean device time; for profilers")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--kernel-storage", choices=["fp32", "fp64"], default="fp32",
+                    help="--kernel-only: storage of A and L (fp32: the headline's mixed form)")
     ap.add_argument("--persist", type=int, choices=[0, 1], default=0,
                     help="--kernel-only: 1 runs each IC(0) apply as one persistent launch; 0 (the default, "
                          "as the headline solve) one launch per level")
@@ -1117,10 +1119,11 @@ def run_kernel_only(args):
     if args.kernel_only == "solve":
         # the headline solve: b = A x*, x0 = 0, mixed form
         rhs = torch.from_numpy(P.b_run).to(dev)
+        storage = ib.STORE_FP32 if args.kernel_storage == "fp32" else ib.STORE_FP64
         for _ in range(args.reps):
             b.zero_()
             torch.cuda.synchronize()
-            res = ctx.solve_dev(rhs.data_ptr(), b.data_ptr(), 10000, TOL, storage=ib.STORE_FP32, rr_interval=RR)
+            res = ctx.solve_dev(rhs.data_ptr(), b.data_ptr(), 10000, TOL, storage=storage, rr_interval=RR)
             ms.append(res.solve_ms)
         print(json.dumps({"kernel_only": "solve", "reps": args.reps, "solve_ms": ms, "iters": res.iters}))
         ctx.close()

@@ -151,6 +151,7 @@ struct QSys {
     std::vector<int> lb;                                  // first batch of each level (nlevels + 1)
     std::vector<int> st_rows, st_slotsS, st_slotsT, st_slices;
     std::vector<int> st_fit;                              // 1: the level's batches fit the stage budget
+    std::vector<int> st_one;                              // 1: ... in one stage buffer only (single-buffered kernel)
     // levels whose rows have in-unit entries only, one per row, the previous
     // step, in full groups of at most 16 steps: the chain-only kernel
     std::vector<int> chainS, chainT;
@@ -202,7 +203,7 @@ struct QSys {
         bdesc.free();
         h_bdesc.clear();
         lb.clear();
-        for (auto* v : {&st_rows, &st_slotsS, &st_slotsT, &st_slices, &st_fit, &chainS, &chainT}) v->clear();
+        for (auto* v : {&st_rows, &st_slotsS, &st_slotsT, &st_slices, &st_fit, &st_one, &chainS, &chainT}) v->clear();
         for (int k = 0; k < 2; ++k) {
             st_fgrid[k].clear();
             st_bgrid[k].clear();
@@ -272,6 +273,7 @@ struct iccg_ctx {
     int smem_optin = 0;     // largest dynamic shared memory per CTA
     bool persist = false;   // ICCG_OPT_PERSIST: the IC(0) apply as one persistent launch where planned
     bool fuse_update = false; // ICCG_OPT_FUSE_UPDATE: the CG update inside the forward sweep's launches
+    bool defer_x = false;     // ICCG_OPT_DEFER_X: x += alpha p with the p update instead of the r update
     iccg::QSys Q;
     // preconditioner
     int pc_kind = -1;
@@ -289,12 +291,14 @@ struct iccg_ctx {
     iccg::SolverState* h_state = nullptr;  // pinned
     double* h_scalars = nullptr;           // pinned
     int* h_status = nullptr;               // pinned, 2 slots
+    iccg::SolverState* h_obs = nullptr;    // pinned, 2 slots: the state after each graph launch
     size_t partial_slots = 0;
     // graph of the fused iteration
     // graphs of the fused iterations: one per pattern of residual-replacement
     // positions within a batch, all for the same system / vectors (gkey)
     struct GraphEntry {
-        unsigned mask;
+        unsigned mask;   // iterations with the FP64 residual replacement
+        int size;        // iterations in the graph
         cudaGraphExec_t exec;
         int kernels;
     };

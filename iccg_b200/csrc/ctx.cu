@@ -96,6 +96,7 @@ int iccg_ctx_create(int device, iccg_ctx** out)
         CK(cudaMallocHost(&c->h_state, sizeof(SolverState)));
         CK(cudaMallocHost(&c->h_scalars, 8 * sizeof(double)));
         CK(cudaMallocHost(&c->h_status, 2 * sizeof(int)));
+        CK(cudaMallocHost(&c->h_obs, 2 * sizeof(SolverState)));
         c->ticket.alloc(4, &c->dev_bytes);
         c->scalars.alloc(8, &c->dev_bytes);
         c->state.alloc(1, &c->dev_bytes);
@@ -129,6 +130,7 @@ int iccg_ctx_destroy(iccg_ctx* c)
     if (c->h_state) cudaFreeHost(c->h_state);
     if (c->h_scalars) cudaFreeHost(c->h_scalars);
     if (c->h_status) cudaFreeHost(c->h_status);
+    if (c->h_obs) cudaFreeHost(c->h_obs);
     cudaStream_t s = c->stream;
     delete c;  // device buffers free themselves
     if (s) cudaStreamDestroy(s);
@@ -154,6 +156,8 @@ int iccg_ctx_set_option(iccg_ctx* c, int option, long long value)
             c->persist = value != 0;
         } else if (option == ICCG_OPT_FUSE_UPDATE) {
             c->fuse_update = value != 0;
+        } else if (option == ICCG_OPT_DEFER_X) {
+            c->defer_x = value != 0;
         } else if (option == ICCG_OPT_STAGE_BUFS) {
             if (value != 1 && value != 2) throw Error(ICCG_ERR_ARG, "ICCG_OPT_STAGE_BUFS takes 1 or 2");
             c->stage_bufs = (int)value;

@@ -296,6 +296,8 @@ __global__ void __launch_bounds__(256) k_residual(int n, const int* __restrict__
 
 // x += alpha p; r -= alpha Ap (cg_crs.cpp:137-141), then r.r (cg_crs.cpp:143).
 // alpha comes from the state (fused) or from the argument (st == nullptr).
+// FIN_UPDX leaves x += alpha p to the p update (k_xpay with x), which reads
+// p anyway: 8 bytes per row less, a stop in between marks it pending.
 template <int FIN>
 __global__ void __launch_bounds__(256) k_update(int n, double alpha_arg, const double* __restrict__ p,
                                                 const double* __restrict__ Ap, double* __restrict__ x,
@@ -304,14 +306,15 @@ __global__ void __launch_bounds__(256) k_update(int n, double alpha_arg, const d
 {
     grid_dep_begin();
     if (st_done(st)) return;
+    constexpr bool DOX = FIN != FIN_UPDX;
     const double alpha = st ? st->alpha : alpha_arg;
     acc2 a[1] = {{0.0, 0.0}};
     // pairs of elements as 16-byte accesses, two pairs in flight per thread
-    // (all four vectors 16-byte aligned; otherwise one element at a time)
-    const bool vec = (((uintptr_t)p | (uintptr_t)Ap | (uintptr_t)x | (uintptr_t)r) & 15) == 0;
+    // (all vectors 16-byte aligned; otherwise one element at a time)
+    const bool vec = (((uintptr_t)Ap | (uintptr_t)r | (DOX ? ((uintptr_t)p | (uintptr_t)x) : 0)) & 15) == 0;
     if (!vec) {
         for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-            x[k] = fma(alpha, p[k], x[k]);
+            if (DOX) x[k] = fma(alpha, p[k], x[k]);
             const double rk = fma(-alpha, Ap[k], r[k]);
             r[k] = rk;
             if (FIN != FIN_NONE) acc2_fma(a[0], rk, rk);
@@ -327,13 +330,17 @@ __global__ void __launch_bounds__(256) k_update(int n, double alpha_arg, const d
     double2* __restrict__ x2 = reinterpret_cast<double2*>(x);
     double2* __restrict__ r2 = reinterpret_cast<double2*>(r);
     auto pair = [&](int i) {
-        const double2 pv = p2[i], qv = q2[i];
-        double2 xv = x2[i], rv = r2[i];
-        xv.x = fma(alpha, pv.x, xv.x);
-        xv.y = fma(alpha, pv.y, xv.y);
+        const double2 qv = q2[i];
+        double2 rv = r2[i];
+        if (DOX) {
+            const double2 pv = p2[i];
+            double2 xv = x2[i];
+            xv.x = fma(alpha, pv.x, xv.x);
+            xv.y = fma(alpha, pv.y, xv.y);
+            x2[i] = xv;
+        }
         rv.x = fma(-alpha, qv.x, rv.x);
         rv.y = fma(-alpha, qv.y, rv.y);
-        x2[i] = xv;
         r2[i] = rv;
         if (FIN != FIN_NONE) {
             acc2_fma(a[0], rv.x, rv.x);
@@ -348,7 +355,7 @@ __global__ void __launch_bounds__(256) k_update(int n, double alpha_arg, const d
     if (i < n2) pair(i);
     if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
         const int k = n - 1;
-        x[k] = fma(alpha, p[k], x[k]);
+        if (DOX) x[k] = fma(alpha, p[k], x[k]);
         const double rk = fma(-alpha, Ap[k], r[k]);
         r[k] = rk;
         if (FIN != FIN_NONE) acc2_fma(a[0], rk, rk);

@@ -221,25 +221,27 @@ static bool plan_staged_type(iccg_ctx* c, int k)
     for (int l = 0; l < L; ++l) {
         if (!Q.st_fit[(size_t)l]) continue;
         const int nb = Q.lb[(size_t)l + 1] - Q.lb[(size_t)l];
-        const size_t fs = 2 * (size_t)stage_layout(Q.st_rows[(size_t)l], Q.st_slotsS[(size_t)l],
-                                                   Q.st_slices[(size_t)l], (int)sizeof(T), false, false).bytes;
-        if (fs > lim) return false;
+        // levels marked st_one run single-buffered only
+        const bool two = !Q.st_one[(size_t)l];
+        const size_t fs = (size_t)stage_layout(Q.st_rows[(size_t)l], Q.st_slotsS[(size_t)l],
+                                               Q.st_slices[(size_t)l], (int)sizeof(T), false, false).bytes;
+        if ((two ? 2 : 1) * fs > lim) return false;
         int pf = 0, pf1 = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf, kf, kThreads, fs));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf1, kf1, kThreads, fs / 2));
-        if (pf < 1 || pf1 < 1) return false;
-        Q.st_fgrid[k][(size_t)l] = std::max(1, std::min(nb, pf * c->nsm));
+        if (two) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf, kf, kThreads, 2 * fs));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pf1, kf1, kThreads, fs));
+        if ((two && pf < 1) || pf1 < 1) return false;
         Q.st1_fgrid[k][(size_t)l] = std::max(1, std::min(nb, pf1 * c->nsm));
+        Q.st_fgrid[k][(size_t)l] = two ? std::max(1, std::min(nb, pf * c->nsm)) : Q.st1_fgrid[k][(size_t)l];
         if (!exact) {
-            const size_t bs = 2 * (size_t)stage_layout(Q.st_rows[(size_t)l], Q.st_slotsT[(size_t)l],
-                                                       Q.st_slices[(size_t)l], (int)sizeof(T), true, false).bytes;
-            if (bs > lim) return false;
+            const size_t bs = (size_t)stage_layout(Q.st_rows[(size_t)l], Q.st_slotsT[(size_t)l],
+                                                   Q.st_slices[(size_t)l], (int)sizeof(T), true, false).bytes;
+            if ((two ? 2 : 1) * bs > lim) return false;
             int pb = 0, pb1 = 0;
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pb, kb, kThreads, bs));
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pb1, kb1, kThreads, bs / 2));
-            if (pb < 1 || pb1 < 1) return false;
-            Q.st_bgrid[k][(size_t)l] = std::max(1, std::min(nb, pb * c->nsm));
+            if (two) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pb, kb, kThreads, 2 * bs));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pb1, kb1, kThreads, bs));
+            if ((two && pb < 1) || pb1 < 1) return false;
             Q.st1_bgrid[k][(size_t)l] = std::max(1, std::min(nb, pb1 * c->nsm));
+            Q.st_bgrid[k][(size_t)l] = two ? std::max(1, std::min(nb, pb * c->nsm)) : Q.st1_bgrid[k][(size_t)l];
         }
     }
     // chain-only levels: one warp per group
@@ -281,6 +283,7 @@ static void plan_staged(iccg_ctx* c)
     Q.st_slotsT.assign((size_t)Q.nlevels, 0);
     Q.st_slices.assign((size_t)Q.nlevels, 0);
     Q.st_fit.assign((size_t)Q.nlevels, 1);
+    Q.st_one.assign((size_t)Q.nlevels, 0);
     Q.chainS.assign((size_t)Q.nlevels, 1);
     Q.chainT.assign((size_t)Q.nlevels, 1);
     // groups [g, g + ng) of a level as one batch (se <= sb: not a batch)
@@ -300,15 +303,20 @@ static void plan_staged(iccg_ctx* c)
         return d;
     };
     // the level's buffer holds its largest batch in every dimension: the
-    // stage bytes of the level's capacities grown by batch d
-    auto stage_bytes = [&](int l, const BatchDesc& d) {
+    // stage bytes of one buffer at the level's capacities grown by batch d
+    auto stage_bytes1 = [&](int l, const BatchDesc& d) {
         const int rows = std::max(Q.st_rows[(size_t)l], d.qe - d.qb);
         const int slS = std::max(Q.st_slotsS[(size_t)l], d.ps1 - d.ps0);
         const int slT = std::max(Q.st_slotsT[(size_t)l], d.pt1 - d.pt0);
         const int slices = std::max(Q.st_slices[(size_t)l], d.se - d.sb);
-        return 2 * (size_t)std::max({stage_layout(rows, slS, slices, 8, false, false).bytes,
-                                     stage_layout(rows, slS, slices, 4, false, false).bytes,
-                                     stage_layout(rows, slT, slices, 4, true, false).bytes});
+        return (size_t)std::max({stage_layout(rows, slS, slices, 8, false, false).bytes,
+                                 stage_layout(rows, slS, slices, 4, false, false).bytes,
+                                 stage_layout(rows, slT, slices, 4, true, false).bytes});
+    };
+    // two buffers (the double-buffered kernel), or one at levels whose
+    // single groups need it (st_one)
+    auto stage_bytes = [&](int l, const BatchDesc& d) {
+        return (Q.st_one[(size_t)l] ? 1 : 2) * stage_bytes1(l, d);
     };
     for (int l = 0; l < Q.nlevels; ++l) {
         const int g1 = Q.level_g[(size_t)l + 1];
@@ -317,7 +325,11 @@ static void plan_staged(iccg_ctx* c)
         for (int g = Q.level_g[(size_t)l]; g < g1;) {
             BatchDesc d = describe(g, 1);
             if (d.se <= d.sb) return;
-            if (stage_bytes(l, d) > budget) Q.st_fit[(size_t)l] = 0;
+            if (stage_bytes(l, d) > budget) {
+                // a group too large for two buffers: the level runs single-buffered
+                if (!Q.st_one[(size_t)l] && stage_bytes1(l, d) <= budget) Q.st_one[(size_t)l] = 1;
+                else Q.st_fit[(size_t)l] = 0;
+            }
             while (d.ng < gmax && g + d.ng < g1 && Q.st_fit[(size_t)l]) {
                 const BatchDesc e = describe(g, d.ng + 1);
                 if (e.qe - e.qb > 512 || stage_bytes(l, e) > budget) break;

@@ -69,7 +69,7 @@ static SweepLevel sweep_level(iccg_ctx* c, int l, bool fwd)
     const bool st_ok = Q.staged && c->sweep_kernel == 0 && (!f32 || Q.r32_ok);
     if (st_ok && (fwd ? Q.chainS[l_] : Q.chainT[l_])) return {0, Q.ch_grid[k][l_]};
     if (st_ok && Q.st_fit[l_] && (fwd || f32)) {
-        if (c->stage_bufs == 1) return {1, fwd ? Q.st1_fgrid[k][l_] : Q.st1_bgrid[k][l_]};
+        if (c->stage_bufs == 1 || Q.st_one[l_]) return {1, fwd ? Q.st1_fgrid[k][l_] : Q.st1_bgrid[k][l_]};
         return {1, fwd ? Q.st_fgrid[k][l_] : Q.st_bgrid[k][l_]};
     }
     if (Q.two_phase) return {2, Q.g2grid[l_]};
@@ -114,7 +114,7 @@ static void launch_sweep_level(iccg_ctx* c, int l, const SweepLevel& sl, const d
         break;
     case 1: {
         const int slots = FWD ? Q.st_slotsS[l_] : Q.st_slotsT[l_];
-        const int nbuf = c->stage_bufs == 1 ? 1 : 2;
+        const int nbuf = (c->stage_bufs == 1 || Q.st_one[l_]) ? 1 : 2;
         // the fused update stages Ap in the area of the backward sweep's r
         constexpr bool with_r = FIN == FIN_RZ || FIN == FIN_RZ0 || FIN == FIN_UPDX;
         const size_t smem = nbuf * (size_t)stage_layout(Q.st_rows[l_], slots, Q.st_slices[l_], (int)sizeof(T),
@@ -162,6 +162,10 @@ static bool fused_update_ok(iccg_ctx* c)
     for (int l = 0; l < Q.nlevels; ++l) {
         const int k = sweep_level<T>(c, l, true).kind;
         if (k != 0 && k != 1) return false;
+        // the staged form also stages Ap: its buffer must still fit
+        if (k == 1 && stage_layout(Q.st_rows[(size_t)l], Q.st_slotsS[(size_t)l], Q.st_slices[(size_t)l],
+                                   (int)sizeof(T), true, false).bytes > c->smem_optin - 2048)
+            return false;
     }
     return true;
 }
@@ -377,11 +381,19 @@ static void fused_iteration(iccg_ctx* c, int storage, bool rr, const double* b, 
         launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st, x);
         return;
     }
-    launch_n(c, 3, k_update<FIN_UPD>, (long long)c->n, n, 0.0, (const double*)c->vp.get(), (const double*)c->vAp.get(), x,
-           c->vr.get(), st, red, c->ticket.get());
+    // x += alpha p with the p update (defer_x), except where the FP64
+    // residual of this iteration needs the new x
+    const bool dx = c->defer_x && !rr;
+    if (dx)
+        launch_n(c, 3, k_update<FIN_UPDX>, (long long)c->n, n, 0.0, (const double*)c->vp.get(),
+                 (const double*)c->vAp.get(), x, c->vr.get(), st, red, c->ticket.get());
+    else
+        launch_n(c, 3, k_update<FIN_UPD>, (long long)c->n, n, 0.0, (const double*)c->vp.get(),
+                 (const double*)c->vAp.get(), x, c->vr.get(), st, red, c->ticket.get());
     if (rr) residual_path<FIN_TRUE>(c, (const double*)x, b, c->vr.get(), st);
     apply_path<FIN_RZ>(c, storage, c->vr.get(), c->vz.get(), st);
-    launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st, (double*)nullptr);
+    launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st,
+             dx ? x : (double*)nullptr);
 }
 
 // releases every captured iteration graph of the context
@@ -424,15 +436,15 @@ static void solve_fused(iccg_ctx* c, const double* b, double* x, int max_iter, d
     // the host can name: a batch of m iterations starting at iteration k0
     // carries the replacement kernel only where (k + 1) % rr_interval == 0
     const int rri = rr ? o.rr_interval : 0;
-    auto rr_mask = [&](long long k0) {
+    auto rr_mask = [&](long long k0, int sz) {
         unsigned mk = 0;
         if (rri > 0)
-            for (int it = 0; it < m && it < 32; ++it)
+            for (int it = 0; it < sz && it < 32; ++it)
                 if ((k0 + it + 1) % rri == 0) mk |= 1u << it;
         return mk;
     };
-    auto one_batch = [&](unsigned mk) {
-        for (int it = 0; it < m; ++it) fused_iteration(c, storage, it < 32 && ((mk >> it) & 1u), b, x);
+    auto one_batch = [&](unsigned mk, int sz) {
+        for (int it = 0; it < sz; ++it) fused_iteration(c, storage, it < 32 && ((mk >> it) & 1u), b, x);
     };
     GraphKey key;
     key.sched_version = c->sched_version;
@@ -450,22 +462,22 @@ static void solve_fused(iccg_ctx* c, const double* b, double* x, int max_iter, d
         c->gkey = key;
         c->gkey_valid = true;
     }
-    auto graph_for = [&](unsigned mk) -> iccg_ctx::GraphEntry& {
+    auto graph_for = [&](unsigned mk, int sz) -> iccg_ctx::GraphEntry& {
         for (auto& g : c->graphs)
-            if (g.mask == mk) return g;
+            if (g.mask == mk && g.size == sz) return g;
         cudaGraph_t graph = nullptr;
         const long long before = c->launches;
         SetupPhase tg("solve.graph_capture");
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         try {
-            one_batch(mk);
+            one_batch(mk, sz);
         } catch (...) {
             cudaStreamEndCapture(c->stream, &graph);
             if (graph) cudaGraphDestroy(graph);
             throw;
         }
         CK(cudaStreamEndCapture(c->stream, &graph));
-        iccg_ctx::GraphEntry e{mk, nullptr, 0};
+        iccg_ctx::GraphEntry e{mk, sz, nullptr, 0};
         const cudaError_t ie = cudaGraphInstantiate(&e.exec, graph, 0);
         cudaGraphDestroy(graph);
         CK(ie);
@@ -474,41 +486,67 @@ static void solve_fused(iccg_ctx* c, const double* b, double* x, int max_iter, d
         c->graphs.push_back(e);
         return c->graphs.back();
     };
-    auto run_batch = [&](long long k0) {
-        const unsigned mk = rr_mask(k0);
+    auto run_batch = [&](long long k0, int sz) {
+        const unsigned mk = rr_mask(k0, sz);
         if (use_graph) {
-            auto& g = graph_for(mk);
+            auto& g = graph_for(mk, sz);
             CK(cudaGraphLaunch(g.exec, c->stream));
             c->launches += g.kernels;
         } else {
-            one_batch(mk);
+            one_batch(mk, sz);
         }
     };
-    // Batches are launched ahead: the status of batch i - 1 is read while
-    // batch i runs.  A batch that finds the solve stopped does nothing.
+    // Batches of iterations are launched ahead: the state after batch i - 1
+    // is read while batch i runs, and a batch that finds the solve stopped
+    // does nothing.  Near the end the recurrence residual's decay per
+    // iteration, from the last two reads, predicts the stop: no batch is
+    // queued past the predicted iteration, and the last batches shrink to
+    // 4, 2 or 1 iterations, so few iterations run on after the stop.  A wrong
+    // prediction costs one more read, never an iteration.
+    const double ltol = std::log(tol);
     long long k_base = 0;  // iterations completed before the current run of batches
     for (;;) {
-        int stopped = kRunning;
-        int batch = 0;
-        for (;; ++batch) {
-            run_batch(k_base + (long long)batch * m);
-            CK(cudaMemcpyAsync(&c->h_status[batch & 1], &st->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-            CK(cudaEventRecord(c->evs[batch & 1], c->stream));
-            if (batch > 0) {
-                CK(cudaEventSynchronize(c->evs[(batch - 1) & 1]));
-                stopped = c->h_status[(batch - 1) & 1];
-                if (stopped != kRunning) break;
+        long long k_next = k_base;  // first iteration of the next batch
+        int nl = 0, nr = 0;         // batches launched / read
+        bool have1 = false, have2 = false;
+        long long k_last = 0, k_prev = 0;
+        double lr_last = 0.0, lr_prev = 0.0;
+        for (;;) {
+            int sz = m;
+            if (have2 && lr_last < lr_prev && k_last > k_prev) {
+                const double slope = (lr_last - lr_prev) / (double)(k_last - k_prev);
+                const double left = (ltol - lr_last) / slope - (double)(k_next - k_last);
+                if (left <= 0.0) sz = 0;
+                else if (left < (double)m) sz = left > 4.0 ? std::min(m, 4) : left > 2.0 ? std::min(m, 2) : 1;
             }
-            if (k_base + (long long)(batch + 1) * m > (long long)max_iter + m) {
-                CK(cudaEventSynchronize(c->evs[batch & 1]));
-                stopped = c->h_status[batch & 1];
-                break;
+            if (sz == 0 && nl == nr) sz = 1;
+            if (k_next >= (long long)max_iter + m) sz = 0;
+            if (sz > 0 && nl - nr < 2) {
+                run_batch(k_next, sz);
+                k_next += sz;
+                CK(cudaMemcpyAsync(&c->h_obs[nl & 1], st, sizeof(SolverState), cudaMemcpyDeviceToHost, c->stream));
+                CK(cudaEventRecord(c->evs[nl & 1], c->stream));
+                ++nl;
+                if (nl - nr < 2) continue;  // keep one batch queued behind the one running
+            }
+            if (nl == nr) break;  // nothing to read: past max_iter
+            CK(cudaEventSynchronize(c->evs[nr & 1]));
+            const SolverState& ob = c->h_obs[nr & 1];
+            ++nr;
+            if (ob.status != kRunning) break;
+            if (ob.k > k_last || !have1) {
+                k_prev = k_last;
+                lr_prev = lr_last;
+                have2 = have1;
+                k_last = ob.k;
+                lr_last = std::log(std::max(ob.rel_resid, 1e-300));
+                have1 = true;
             }
         }
-        if (stopped != kTrueCheck) {
-            CK(cudaStreamSynchronize(c->stream));
-            if (c->h_status[batch & 1] != kTrueCheck) break;
-        }
+        CK(cudaStreamSynchronize(c->stream));
+        CK(cudaMemcpyAsync(c->h_state, st, sizeof(SolverState), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (c->h_state->status != kTrueCheck) break;
         // The recurrence residual passed the tolerance: replace it by the
         // FP64 residual b - A x (cg_crs.cpp:518-528 semantics), test that,
         // and, if it is not below the tolerance, finish this iteration

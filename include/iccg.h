@@ -229,7 +229,14 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
    as the update on its own.  On the 128^3 ABMC system it is slower
    (22.50 against 21.78 ms mixed, 34.85 against 32.66 ms FP64): the
    chain-only forward level, latency-bound, loses more than the launch and
-   the bytes saved; it is kept as an option. */
+   the bytes saved; it is kept as an option.
+   ICCG_OPT_DEFER_X (default 0), fused solves: x += alpha p is done by the p
+   update (p = z + beta p), which reads p anyway, instead of by the r update:
+   8 bytes per row less per iteration.  A solve that stops between the two
+   gets the pending x update before its true residual.  Iterations with an
+   FP64 residual replacement update x with r.  The same bits either way;
+   measured slightly slower on the 128^3 ABMC system (21.26 against 21.15 ms
+   mixed, 32.39 against 32.00 ms FP64), so it is kept as an option. */
 #define ICCG_OPT_TILED 0
 #define ICCG_OPT_SWEEP 1
 #define ICCG_OPT_PDL 2
@@ -237,6 +244,7 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
 #define ICCG_OPT_STAGE_BUFS 4
 #define ICCG_OPT_PERSIST 5
 #define ICCG_OPT_FUSE_UPDATE 6
+#define ICCG_OPT_DEFER_X 7
 int iccg_ctx_set_option(iccg_ctx* ctx, int option, long long value);
 
 /* Uploads A_run (the matrix conjugate_gradient runs on, cg_crs.cpp:442-447):

@@ -381,8 +381,8 @@ def test_gpu_tiled_kernels_equal_simple_kernels(which):
     ctx.close()
 
 
-@pytest.mark.parametrize("which", ["mc2d", "abmc_lin", "abmc_bfs", "d27_abmc8", "d27_abmc32", "abmc_b32", "p2d_abmc64",
-                                   "d27_mc", "knn_abmc"])
+@pytest.mark.parametrize("which", ["mc2d", "abmc_lin", "abmc_bfs", "d27_abmc8", "d27_abmc16", "d27_abmc32", "abmc_b32",
+                                   "p2d_abmc64", "d27_mc", "knn_abmc"])
 def test_gpu_staged_sweeps_equal_per_slice_sweeps(which):
     """The staged substitution kernel (double-buffered shared-memory batches)
     against the per-slice two-phase kernel (ICCG_OPT_SWEEP = 1): the same
@@ -393,6 +393,7 @@ def test_gpu_staged_sweeps_equal_per_slice_sweeps(which):
          "abmc_lin": lambda: pb.config_abmc_aniso(40, 16, "linear"),
          "abmc_bfs": lambda: pb.config_abmc_aniso(40, 16, "bfs"),
          "d27_abmc8": lambda: pb.config_diffusion27(24, "abmc", 8),
+         "d27_abmc16": lambda: pb.config_diffusion27(24, "abmc", 16),
          "d27_abmc32": lambda: pb.config_diffusion27(24, "abmc", 32),
          "abmc_b32": lambda: pb.config_abmc_aniso(40, 32, "linear"),
          "p2d_abmc64": lambda: pb.make(pb.poisson2d(96), "abmc", block_size=64, blocking="bfs", seed=4),
@@ -673,4 +674,36 @@ def test_gpu_fused_update_gives_the_same_bits(which):
     (xa, ra), (xb, rb) = out[1][1], out[0][1]
     assert ra.converged and ra.true_rel_resid <= 1e-8 and abs(ra.iters - rb.iters) <= 1
     assert rel_err(xa, xb) < 1e-6
+    ctx.close()
+
+
+@pytest.mark.parametrize("which", ["abmc_lin", "d27_mc", "mc2d"])
+def test_gpu_deferred_x_update_gives_the_same_bits(which):
+    """x += alpha p done by the p update (ICCG_OPT_DEFER_X) against the r
+    update doing it (the default): the same bits for converged solves (the
+    last x update left pending and applied before the true residual), for
+    iteration caps (stops at the p update), in FP64 and in the mixed form
+    (whose FP64 confirmation resumes a stopped solve)."""
+    P = {"abmc_lin": lambda: pb.config_abmc_aniso(40, 16, "linear"),
+         "d27_mc": lambda: pb.config_diffusion27(24, "piccg"),
+         "mc2d": lambda: pb.config_small_mc(100, seed=1)}[which]()
+    ctx = _ctx_for(P.A_run, P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    out = {}
+    for dx in (1, 0):
+        ctx.set_option(ib.OPT_DEFER_X, dx)
+        res = []
+        for st, cap, tol, rri, gi in ((ib.STORE_FP64, 10000, 1e-8, 50, 8), (ib.STORE_FP64, 7, 1e-8, 50, 8),
+                                      (ib.STORE_FP64, 10000, 1e-3, 50, 3), (ib.STORE_FP32, 10000, 1e-8, 50, 8),
+                                      (ib.STORE_FP32, 10000, 1e-8, 7, 5), (ib.STORE_FP32, 9, 1e-8, 4, 8)):
+            x = np.zeros(P.A_run.n)
+            r = ctx.solve(P.b_run, x, cap, tol, storage=st, rr_interval=rri, graph_iters=gi)
+            res.append((x, r))
+        out[dx] = res
+    ctx.set_option(ib.OPT_DEFER_X, 0)
+    for (xa, ra), (xb, rb) in zip(out[1], out[0]):
+        assert ra.iters == rb.iters and ra.status == rb.status and ra.n_replacements == rb.n_replacements
+        assert np.array_equal(xa, xb)
+        assert ra.true_rel_resid == rb.true_rel_resid
+    assert out[1][1][1].status == "max_iter" and out[1][0][1].converged
     ctx.close()
