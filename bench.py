@@ -414,7 +414,8 @@ def _kernel_class(name: str):
         return "fwd_sweep" if m.group(1) == "1" else "bwd_sweep"
     if name.startswith("iccg::k_persist"):
         return "persistent"
-    if name.startswith(("iccg::k_update", "iccg::k_xpay", "iccg::k_copy", "iccg::k_resume")):
+    if name.startswith(("iccg::k_update", "iccg::k_xpay", "iccg::k_copy", "iccg::k_resume", "iccg::k_apply_xp",
+                        "iccg::k_clear_xp")):
         return "vector"
     if name.startswith("iccg::k_residual_q"):
         return "residual"
