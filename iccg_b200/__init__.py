@@ -57,6 +57,7 @@ OPT_STAGE_BUFS = 4
 OPT_PERSIST = 5
 OPT_FUSE_UPDATE = 6
 OPT_DEFER_X = 7
+OPT_SPMV_PACK = 8
 STATUS_NAMES = {0: "converged", 1: "breakdown", 2: "max_iter", 3: "nonfinite"}
 
 

@@ -60,17 +60,22 @@ struct SellDev : SellLayout {
     Buf<int> ptr, col, len;
     Buf<double> v64;
     Buf<float> v32;
+    Buf<int2> pk;          // FP32 values packed with their columns (the SpMV's matrix)
     bool has32 = false;
+    bool haspk = false;
     SellMat view(bool fp32) const
     {
-        return SellMat{ptr.get(), col.get(), fp32 ? (const void*)v32.get() : (const void*)v64.get(), len.get()};
+        return SellMat{ptr.get(), col.get(), fp32 ? (const void*)v32.get() : (const void*)v64.get(), len.get(),
+                       fp32 && haspk ? pk.get() : nullptr};
     }
     void reset()
     {
         for (auto* b : {&ptr, &col, &len}) b->free();
         v64.free();
         v32.free();
+        pk.free();
         has32 = false;
+        haspk = false;
         slots = 0;
         max_nin = 0;
         src.clear();
@@ -274,6 +279,7 @@ struct iccg_ctx {
     bool persist = false;   // ICCG_OPT_PERSIST: the IC(0) apply as one persistent launch where planned
     bool fuse_update = false; // ICCG_OPT_FUSE_UPDATE: the CG update inside the forward sweep's launches
     bool defer_x = false;     // ICCG_OPT_DEFER_X: x += alpha p with the p update instead of the r update
+    bool spmv_pack = true;    // ICCG_OPT_SPMV_PACK: FP32 SpMV reads (value, column) words
     iccg::QSys Q;
     // preconditioner
     int pc_kind = -1;

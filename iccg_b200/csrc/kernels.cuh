@@ -593,7 +593,17 @@ struct SellMat {
     const int* col;       // column (Q index) per slot
     const void* val;      // value per slot (float or double)
     const int* len;       // entries of each Q row
+    const int2* pk;       // FP32 values with their columns, one 8-byte word per slot (or null)
 };
+
+// pk[s] = (value bits, column) of slot s: one load per entry in the SpMV
+__global__ void __launch_bounds__(256) k_pack_sell(long long m, const float* __restrict__ v,
+                                                   const int* __restrict__ col, int2* __restrict__ pk)
+{
+    grid_dep_begin();
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
+        pk[i] = make_int2(__float_as_int(v[i]), col[i]);
+}
 
 // y = A x over regular 32-row slices (slice s = Q rows [32 s, 32 s + 32)),
 // product and sum rounded separately as in spmv (cg_crs.cpp:73-75).
@@ -617,14 +627,25 @@ __global__ void __launch_bounds__(256) k_spmv_q(int n, SellMat A, const double* 
     constexpr int K = 8;
     int L = 0, c[K];
     T v[K];
+    // FP32 values packed with their columns: one 8-byte load per entry
+    const int2* __restrict__ pk = sizeof(T) == 4 ? A.pk : nullptr;
     auto load = [&](int s) {
         const int i = (s << 5) + lane;
         L = i < n ? A.len[i] : 0;
         const int p0 = A.ptr[s] + lane;
+        if (pk) {
 #pragma unroll
-        for (int j = 0; j < K; ++j) {
-            c[j] = j < L ? __ldcs(col + p0 + 32 * j) : 0;
-            v[j] = j < L ? __ldcs(val + p0 + 32 * j) : (T)0;
+            for (int j = 0; j < K; ++j) {
+                const int2 e = j < L ? __ldcs(pk + p0 + 32 * j) : make_int2(0, 0);
+                c[j] = e.y;
+                v[j] = (T)__int_as_float(e.x);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < K; ++j) {
+                c[j] = j < L ? __ldcs(col + p0 + 32 * j) : 0;
+                v[j] = j < L ? __ldcs(val + p0 + 32 * j) : (T)0;
+            }
         }
     };
     int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;

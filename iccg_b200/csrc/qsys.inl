@@ -492,6 +492,14 @@ static void ensure_q32(iccg_ctx* c)
     SetupPhase t("q.fp32_copies");
     QSys& Q = c->Q;
     sell_f32(c, Q.A);
+    if (c->spmv_pack && !Q.A.haspk) {
+        Q.A.pk.alloc((size_t)Q.A.slots, &c->dev_bytes);
+        if (Q.A.slots)
+            launch(c, 3, k_pack_sell, grid_for(c, Q.A.slots), kThreads, (long long)Q.A.slots,
+                   (const float*)Q.A.v32.get(), (const int*)Q.A.col.get(), Q.A.pk.get());
+        CK(cudaStreamSynchronize(c->stream));
+        Q.A.haspk = true;
+    }
     if (c->pc_kind == ICCG_PRECOND_IC0 && c->F.built) {
         sell_f32(c, Q.S);
         sell_f32(c, Q.T);

@@ -236,7 +236,11 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
    gets the pending x update before its true residual.  Iterations with an
    FP64 residual replacement update x with r.  The same bits either way;
    measured slightly slower on the 128^3 ABMC system (21.26 against 21.15 ms
-   mixed, 32.39 against 32.00 ms FP64), so it is kept as an option. */
+   mixed, 32.39 against 32.00 ms FP64), so it is kept as an option.
+   ICCG_OPT_SPMV_PACK (default 1), lane-interleaved FP32 SpMV: the matrix
+   entries are read as one 8-byte word of value and column instead of two
+   4-byte loads (an extra packed copy of A's FP32 values and columns).  The
+   same bits either way. */
 #define ICCG_OPT_TILED 0
 #define ICCG_OPT_SWEEP 1
 #define ICCG_OPT_PDL 2
@@ -245,6 +249,7 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
 #define ICCG_OPT_PERSIST 5
 #define ICCG_OPT_FUSE_UPDATE 6
 #define ICCG_OPT_DEFER_X 7
+#define ICCG_OPT_SPMV_PACK 8
 int iccg_ctx_set_option(iccg_ctx* ctx, int option, long long value);
 
 /* Uploads A_run (the matrix conjugate_gradient runs on, cg_crs.cpp:442-447):

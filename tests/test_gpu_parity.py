@@ -707,3 +707,26 @@ def test_gpu_deferred_x_update_gives_the_same_bits(which):
         assert ra.true_rel_resid == rb.true_rel_resid
     assert out[1][1][1].status == "max_iter" and out[1][0][1].converged
     ctx.close()
+
+
+@pytest.mark.parametrize("which", ["abmc_lin", "d27_abmc8", "knn_abmc"])
+def test_gpu_packed_spmv_gives_the_same_bits(which):
+    """The FP32 SpMV reading (value, column) words (ICCG_OPT_SPMV_PACK, the
+    default) against two separate loads: the same bits for the product and
+    for a mixed-precision solve."""
+    P = {"abmc_lin": lambda: pb.config_abmc_aniso(40, 16, "linear"),
+         "d27_abmc8": lambda: pb.config_diffusion27(24, "abmc", 8),
+         "knn_abmc": lambda: pb.config_knn(8000, seed=5, block_size=16)}[which]()
+    ctx = _ctx_for(P.A_run, P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    v = ib.gen_uniform(P.A_run.n, 41)
+    out = {}
+    for pk in (1, 0):
+        ctx.set_option(ib.OPT_SPMV_PACK, pk)
+        x = np.zeros(P.A_run.n)
+        r = ctx.solve(P.b_run, x, 10000, 1e-8, storage=ib.STORE_FP32)
+        out[pk] = (ctx.spmv(v, ib.STORE_FP32), x, r)
+    ctx.set_option(ib.OPT_SPMV_PACK, 1)
+    assert np.array_equal(out[1][0], out[0][0])
+    assert np.array_equal(out[1][1], out[0][1]) and out[1][2].iters == out[0][2].iters
+    ctx.close()
