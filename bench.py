@@ -124,6 +124,7 @@ def build_problem():
     t0 = time.perf_counter()
     P = pb.config_abmc_aniso(SIDE, BLOCK, BLOCKING, seed=0)
     return P, time.perf_counter() - t0
+    P, setup_s = build_problem()
 
 
 def bytes_model(P, storage_bytes: int):

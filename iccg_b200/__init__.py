@@ -32,7 +32,7 @@ __all__ = [
     "ReadColorFile_1Based", "ReadBlockFile_1Based", "ReadBlockColorFile_1Based",
     "write_assignment_1based",
     "BuildPermutationByColor", "BuildPermutationByBlockColor",
-    "Permute_PtAP_LowerCRS_to_LowerCRS", "BuildColorPtrRows_FromPermutationAndColor",
+    "Permute_PtAP_LowerCRS_to_LowerCRS", "Permute_PtAP_full_gpu", "BuildColorPtrRows_FromPermutationAndColor",
     "BuildABMCSchedule", "check_interblock_same_color", "check_schedule_hazards",
     "gen_stencil_2d5", "gen_stencil_3d7", "gen_diffusion27", "gen_knn_laplacian", "gen_uniform",
     "color_greedy", "block_partition", "color_blocks", "host_spmv",
@@ -109,6 +109,7 @@ def lib() -> C.CDLL:
         "iccg_ptap_lower": (_I, [_I, _P, _P, _P, _P, _I, _P, _P, _P, C.POINTER(_I)]),
         "iccg_expand_lower_nnz": (_I, [_I, _P, _P, C.POINTER(_I)]),
         "iccg_expand_lower_to_full": (_I, [_I, _P, _P, _P, _P, _P, _P]),
+        "iccg_ptap_full_gpu": (_I, [_I, _I, _P, _P, _P, _P, _I, _P, _P, _P, C.POINTER(_I), C.POINTER(_I)]),
         "iccg_color_schedule": (_I, [_I, _P, _I, _P, _P, _P]),
         "iccg_abmc_schedule": (_I, [_I, _P, _P, _P, _I, _I, _P, _P, _P, _P]),
         "iccg_check_interblock_same_color": (C.c_longlong, [_I, _P, _P, _P, _P, _I, _I, _P]),
@@ -318,6 +319,21 @@ def Permute_PtAP_LowerCRS_to_LowerCRS(A: CRS, new_of_old) -> CRS:
     # views of the leading entries: the result is short-lived (expanded to
     # the full matrix next), so the unused tail is kept rather than copied
     return CRS(A.n, rp, ci[: nnz.value], v[: nnz.value])
+
+
+def Permute_PtAP_full_gpu(A: CRS, new_of_old, device: int = 0):
+    """expand_lower_to_full(Permute_PtAP_LowerCRS_to_LowerCRS(A, new_of_old))
+    computed on the GPU (iccg_ptap_full_gpu): the caller's A_run, the same
+    bits as the host routines.  Returns (CRS, computed_on_device)."""
+    p = _i32(new_of_old)
+    cap = max(2 * int(A.nnz), 1)
+    rp = np.zeros(A.n + 1, np.int32)
+    ci = np.zeros(cap, np.int32)
+    v = np.zeros(cap, np.float64)
+    nnz, dev = C.c_int(), C.c_int()
+    _check(lib().iccg_ptap_full_gpu(int(device), A.n, _ptr(A.rowptr), _ptr(A.colind), _ptr(A.val), _ptr(p), cap,
+                                    _ptr(rp), _ptr(ci), _ptr(v), C.byref(nnz), C.byref(dev)))
+    return CRS(A.n, rp, ci[: nnz.value].copy(), v[: nnz.value].copy()), bool(dev.value)
 
 
 def BuildColorPtrRows_FromPermutationAndColor(color, nc: int, new_of_old):

@@ -19,7 +19,7 @@ CSRC = PKG / "csrc"
 LIBDIR = PKG / "_lib"
 LIB = LIBDIR / "libiccg_b200.so"
 
-CUDA_SOURCES = ["ctx.cu", "noalloc.cu"]
+CUDA_SOURCES = ["ctx.cu", "noalloc.cu", "setup_dev.cu"]
 HOST_SOURCES = ["host_order.cpp", "host_gen.cpp", "host_layout.cpp", "host_capi.cpp"]
 HEADERS = ["dd.cuh", "kernels.cuh", "persist.cuh", "host.hpp", "devbuf.hpp", "context.hpp", "plan.inl", "factor.inl",
            "qsys.inl", "persist.inl", "solver.inl", "batch.inl"]

@@ -512,7 +512,7 @@ static void sys_tables(iccg_batch* B, int k)
     CK(cudaStreamSynchronize(c->stream));
     QSys& Q = c->Q;
     bool fit = Q.staged && Q.two_phase && (!f32 || Q.r32_ok);
-    for (int l = 0; fit && l < Q.nlevels; ++l) fit = Q.st_fit[(size_t)l] != 0;
+    for (int l = 0; fit && l < Q.nlevels; ++l) fit = Q.st_fit[(size_t)l] != 0 && (f32 || Q.st_fit64[(size_t)l] != 0);
     if (!fit) throw Error(ICCG_ERR_STATE, "system " + std::to_string(k) + ": a level does not fit the staged sweep");
     const int lim = std::max(0, B->smem_optin - 2048);  // the reduction scratch comes on top
     auto fwd_bytes = [&](const BatchDesc& d) {

@@ -157,6 +157,7 @@ struct QSys {
     std::vector<int> st_rows, st_slotsS, st_slotsT, st_slices;
     std::vector<int> st_fit;                              // 1: the level's batches fit the stage budget
     std::vector<int> st_one;                              // 1: ... in one stage buffer only (single-buffered kernel)
+    std::vector<int> st_fit64;                            // 1: ... with FP64 values too (forward sweep)
     // levels whose rows have in-unit entries only, one per row, the previous
     // step, in full groups of at most 16 steps: the chain-only kernel
     std::vector<int> chainS, chainT;
@@ -208,7 +209,8 @@ struct QSys {
         bdesc.free();
         h_bdesc.clear();
         lb.clear();
-        for (auto* v : {&st_rows, &st_slotsS, &st_slotsT, &st_slices, &st_fit, &st_one, &chainS, &chainT}) v->clear();
+        for (auto* v : {&st_rows, &st_slotsS, &st_slotsT, &st_slices, &st_fit, &st_one, &st_fit64, &chainS, &chainT})
+            v->clear();
         for (int k = 0; k < 2; ++k) {
             st_fgrid[k].clear();
             st_bgrid[k].clear();

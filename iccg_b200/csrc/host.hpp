@@ -60,6 +60,10 @@ CRS permute_ptap_lower(const CRS& A, const std::vector<int>& new_of_old);
 CRS permute_ptap_lower(int n, const int* rowptr, const int* colind, const double* val, const int* new_of_old);
 CRS expand_lower_to_full(const CRS& L);
 CRS expand_lower_to_full(int n, const int* rowptr, const int* colind, const double* val);
+// C ABI argument checks of a CRS (rowptr nondecreasing, inside [0, nnz]) and
+// the copy of a result into caller arrays (host_capi.cpp)
+void check_crs(int n, const int* rowptr, const int* colind, const double* val, bool need_val = true);
+void copy_out(const CRS& B, int* rowptr, int* colind, double* val);
 void build_color_schedule(const std::vector<int>& color, int nc,
                           const std::vector<int>& new_of_old, std::vector<int>& color_ptr,
                           std::vector<int>& rows_of_color);

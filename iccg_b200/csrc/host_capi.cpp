@@ -33,7 +33,7 @@ int guarded(F&& f)
 }
 
 // the argument checks of wrap() without its copy
-static void check_crs(int n, const int* rowptr, const int* colind, const double* val, bool need_val = true)
+void check_crs(int n, const int* rowptr, const int* colind, const double* val, bool need_val)
 {
     if (n < 0 || !rowptr) throw Error(ICCG_ERR_ARG, "bad CRS arguments");
     const int nnz = rowptr[n];
@@ -47,7 +47,7 @@ static void check_crs(int n, const int* rowptr, const int* colind, const double*
 }
 
 // a result matrix into the caller's arrays, on host threads
-static void copy_out(const CRS& B, int* rowptr, int* colind, double* val)
+void copy_out(const CRS& B, int* rowptr, int* colind, double* val)
 {
     const int T = host_threads(B.nnz());
     parallel_copy(rowptr, B.rowptr.data(), sizeof(int) * B.rowptr.size(), T);

@@ -219,7 +219,7 @@ static bool plan_staged_type(iccg_ctx* c, int k)
     // the kernel's static shared memory (reduction scratch) comes on top
     const size_t lim = (size_t)std::max(0, c->smem_optin - 2048);
     for (int l = 0; l < L; ++l) {
-        if (!Q.st_fit[(size_t)l]) continue;
+        if (!Q.st_fit[(size_t)l] || (exact && !Q.st_fit64[(size_t)l])) continue;
         const int nb = Q.lb[(size_t)l + 1] - Q.lb[(size_t)l];
         // levels marked st_one run single-buffered only
         const bool two = !Q.st_one[(size_t)l];
@@ -284,6 +284,7 @@ static void plan_staged(iccg_ctx* c)
     Q.st_slices.assign((size_t)Q.nlevels, 0);
     Q.st_fit.assign((size_t)Q.nlevels, 1);
     Q.st_one.assign((size_t)Q.nlevels, 0);
+    Q.st_fit64.assign((size_t)Q.nlevels, 1);
     Q.chainS.assign((size_t)Q.nlevels, 1);
     Q.chainT.assign((size_t)Q.nlevels, 1);
     // groups [g, g + ng) of a level as one batch (se <= sb: not a batch)
@@ -304,12 +305,13 @@ static void plan_staged(iccg_ctx* c)
     };
     // the level's buffer holds its largest batch in every dimension: the
     // stage bytes of one buffer at the level's capacities grown by batch d
+    // (FP32 forward and backward, and FP64 forward unless the level dropped it)
     auto stage_bytes1 = [&](int l, const BatchDesc& d) {
         const int rows = std::max(Q.st_rows[(size_t)l], d.qe - d.qb);
         const int slS = std::max(Q.st_slotsS[(size_t)l], d.ps1 - d.ps0);
         const int slT = std::max(Q.st_slotsT[(size_t)l], d.pt1 - d.pt0);
         const int slices = std::max(Q.st_slices[(size_t)l], d.se - d.sb);
-        return (size_t)std::max({stage_layout(rows, slS, slices, 8, false, false).bytes,
+        return (size_t)std::max({Q.st_fit64[(size_t)l] ? stage_layout(rows, slS, slices, 8, false, false).bytes : 0,
                                  stage_layout(rows, slS, slices, 4, false, false).bytes,
                                  stage_layout(rows, slT, slices, 4, true, false).bytes});
     };
@@ -326,9 +328,13 @@ static void plan_staged(iccg_ctx* c)
             BatchDesc d = describe(g, 1);
             if (d.se <= d.sb) return;
             if (stage_bytes(l, d) > budget) {
-                // a group too large for two buffers: the level runs single-buffered
-                if (!Q.st_one[(size_t)l] && stage_bytes1(l, d) <= budget) Q.st_one[(size_t)l] = 1;
-                else Q.st_fit[(size_t)l] = 0;
+                // a group too large for two buffers: the level runs single-buffered;
+                // too large for one with FP64 values: FP64 leaves the staged kernel
+                // there (the per-slice kernel, the same bits); too large still: the
+                // level is not staged
+                Q.st_one[(size_t)l] = 1;
+                if (stage_bytes(l, d) > budget) Q.st_fit64[(size_t)l] = 0;
+                if (stage_bytes(l, d) > budget) Q.st_fit[(size_t)l] = 0;
             }
             while (d.ng < gmax && g + d.ng < g1 && Q.st_fit[(size_t)l]) {
                 const BatchDesc e = describe(g, d.ng + 1);

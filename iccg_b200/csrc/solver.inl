@@ -68,7 +68,7 @@ static SweepLevel sweep_level(iccg_ctx* c, int l, bool fwd)
     const size_t l_ = (size_t)l;
     const bool st_ok = Q.staged && c->sweep_kernel == 0 && (!f32 || Q.r32_ok);
     if (st_ok && (fwd ? Q.chainS[l_] : Q.chainT[l_])) return {0, Q.ch_grid[k][l_]};
-    if (st_ok && Q.st_fit[l_] && (fwd || f32)) {
+    if (st_ok && Q.st_fit[l_] && (f32 || (fwd && Q.st_fit64[l_]))) {
         if (c->stage_bufs == 1 || Q.st_one[l_]) return {1, fwd ? Q.st1_fgrid[k][l_] : Q.st1_bgrid[k][l_]};
         return {1, fwd ? Q.st_fgrid[k][l_] : Q.st_bgrid[k][l_]};
     }

@@ -22,10 +22,15 @@ import numpy as np
 
 from . import (CRS, ColorSchedule, BuildABMCSchedule, BuildColorPtrRows_FromPermutationAndColor,
                BuildPermutationByBlockColor, BuildPermutationByColor, Permute_PtAP_LowerCRS_to_LowerCRS,
+               Permute_PtAP_full_gpu,
                block_partition, color_blocks, color_greedy, expand_lower_to_full, gen_diffusion27,
                gen_knn_laplacian, gen_stencil_2d5, gen_stencil_3d7, gen_uniform, host_spmv)
 
 VARIANTS = ("cg", "dcg", "iccg", "piccg", "abmc")
+
+# device on which setup() forms A_run (iccg_ptap_full_gpu: the same bits as
+# the host routines), or None for the host routines
+PTAP_DEVICE: Optional[int] = None
 
 
 @dataclass
@@ -76,8 +81,11 @@ def setup(A: CRS, variant: str, color=None, nc: int = 0, block_of_old=None, nb: 
     else:
         return P
     P.new_of_old = new_of_old
-    Ap = Permute_PtAP_LowerCRS_to_LowerCRS(A, new_of_old)
-    P.A_run = expand_lower_to_full(Ap)                         # cg_crs.cpp:420-421
+    if PTAP_DEVICE is not None:
+        P.A_run, _ = Permute_PtAP_full_gpu(A, new_of_old, PTAP_DEVICE)   # cg_crs.cpp:419-421 on the GPU
+    else:
+        Ap = Permute_PtAP_LowerCRS_to_LowerCRS(A, new_of_old)
+        P.A_run = expand_lower_to_full(Ap)                     # cg_crs.cpp:420-421
     if variant == "abmc":
         cpb, boc, bp, rob = BuildABMCSchedule(new_of_old, block_of_old, block_color, nb, nbc)
         P.sched = ColorSchedule(nc=nbc, mode=ColorSchedule.ABMC_BLOCK, nb=nb, color_ptr_blk=cpb,

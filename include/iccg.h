@@ -118,6 +118,20 @@ int iccg_ptap_lower(int n, const int* rowptr, const int* colind, const double* v
 int iccg_expand_lower_nnz(int n, const int* rowptr, const int* colind, int* out_nnz);
 int iccg_expand_lower_to_full(int n, const int* rowptr, const int* colind, const double* val,
                               int* out_rowptr, int* out_colind, double* out_val);
+/* Permute_PtAP_LowerCRS_to_LowerCRS (color.cpp:66-141) followed by
+   expand_lower_to_full (crs_io.cpp:163-227), the caller's A_run
+   (cg_crs.cpp:419-421), computed on CUDA device `device`: host arrays in,
+   the full permuted matrix into out_rowptr[n+1], out_colind[cap],
+   out_val[cap]; *out_nnz receives its size (also when cap is too small, with
+   ICCG_ERR_ARG).  The same bits as iccg_ptap_lower + iccg_expand_lower_to_full:
+   each output entry is one input value when no (i, j) pair repeats; inputs
+   that repeat a pair (whose sums depend on the order) or give output rows of
+   more than 256 entries are computed by those host routines instead, and
+   *on_device (may be NULL) receives 0.  2 * nnz of the input bounds the
+   output size. */
+int iccg_ptap_full_gpu(int device, int n, const int* rowptr, const int* colind, const double* val,
+                       const int* new_of_old, int cap, int* out_rowptr, int* out_colind, double* out_val,
+                       int* out_nnz, int* on_device);
 /* BuildColorPtrRows_FromPermutationAndColor (color.cpp:164-197) */
 int iccg_color_schedule(int n, const int* color, int nc, const int* new_of_old,
                         int* color_ptr, int* rows_of_color);

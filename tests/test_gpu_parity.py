@@ -516,9 +516,12 @@ def test_gpu_stage_budget_keeps_fp64_bits(which):
 
 
 def test_gpu_sweep_plan_reports_kernels():
-    """Units of 32 rows on the 27-point operator: one group's stage exceeds
-    the shared memory, so every level runs the per-slice two-phase kernel;
-    the untiled path reports the CSR kernels."""
+    """Units of 32 rows on the 27-point operator: one group's stage needs
+    more than half the shared memory, so the levels where it fits one buffer
+    run the staged kernel single-buffered (FP32, and the FP64 forward sweep
+    where FP64 values fit too) and the others the per-slice two-phase kernel;
+    the exact-order FP64 backward sweep stays per-slice; the untiled path
+    reports the CSR kernels."""
     P = pb.config_diffusion27(24, "abmc", 32)
     ctx = _ctx_for(P.A_run, P.sched)
     ctx.build(ib.PRECOND_IC0, 0.0)
@@ -526,7 +529,10 @@ def test_gpu_sweep_plan_reports_kernels():
         for fwd in (True, False):
             plan = ctx.sweep_plan(st, fwd)
             assert len(plan) == P.nc
-            assert all(k == "two_phase" and g >= 1 for k, g in plan), plan
+            assert all(k in ("two_phase", "staged", "chain") and g >= 1 for k, g in plan), plan
+            if st == ib.STORE_FP64 and not fwd:
+                assert all(k != "staged" for k, _ in plan), plan
+    assert any(k == "staged" for k, _ in ctx.sweep_plan(ib.STORE_FP32, True))
     ctx.use_tiled(False)
     assert all(k == "csr" for k, _ in ctx.sweep_plan(ib.STORE_FP64, True))
     ctx.use_tiled(True)
