@@ -272,9 +272,14 @@ def run_gpu(args):
     err = float(np.linalg.norm(x32 - x64) / np.linalg.norm(x64))
     per_solve = [r.solve_ms for r in results]
 
-    # plain FP64 path (one kernel per reference op, host-checked) and fused FP64, untimed by the contract
-    plain = solve(ib.STORE_FP64, ib.MODE_PLAIN)
-    fused64 = solve(ib.STORE_FP64, ib.MODE_FUSED)
+    # plain FP64 path (one kernel per reference op, host-checked) and fused
+    # FP64, outside the timed region: the median of 3 solves each
+    def median_solve(storage, mode):
+        rs = sorted((solve(storage, mode) for _ in range(3)), key=lambda r: r.solve_ms)
+        return rs[1]
+
+    plain = median_solve(ib.STORE_FP64, ib.MODE_PLAIN)
+    fused64 = median_solve(ib.STORE_FP64, ib.MODE_FUSED)
 
     # per-kernel device time.  The solve's kernels run back to back inside
     # CUDA graphs (with programmatic dependent launch), so a kernel's time is

@@ -163,6 +163,14 @@ int iccg_ctx_set_option(iccg_ctx* c, int option, long long value)
         } else if (option == ICCG_OPT_STAGE_BUFS) {
             if (value != 1 && value != 2) throw Error(ICCG_ERR_ARG, "ICCG_OPT_STAGE_BUFS takes 1 or 2");
             c->stage_bufs = (int)value;
+        } else if (option == ICCG_OPT_STAGE_ROWS) {
+            if (value < 32 || value > 8192) throw Error(ICCG_ERR_ARG, "ICCG_OPT_STAGE_ROWS takes 32 to 8192");
+            c->stage_rows = (int)value;
+            if (c->Q.two_phase && !c->Q.steps.empty()) {
+                CK(cudaStreamSynchronize(c->stream));
+                plan_staged(c);
+                build_persist(c);
+            }
         } else if (option == ICCG_OPT_STAGE_KB) {
             if (value < 0 || value > 1024) throw Error(ICCG_ERR_ARG, "ICCG_OPT_STAGE_KB takes 0 to 1024");
             c->stage_kb = (int)value;

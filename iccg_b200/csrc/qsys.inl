@@ -264,7 +264,7 @@ static bool plan_staged_type(iccg_ctx* c, int k)
 }
 
 // Batches of the staged sweeps: consecutive groups of one level, at most 16
-// groups and 512 rows, and as many groups as keep two stage buffers of every
+// groups and ICCG_OPT_STAGE_ROWS rows (512), and as many groups as keep two stage buffers of every
 // type the staged kernel runs with (FP64 and FP32 forward, FP32 backward)
 // within the budget (ICCG_OPT_STAGE_KB, default the opt-in shared memory);
 // the default single buffer per CTA then takes half of it.  A level with a group that alone exceeds the budget runs on the
@@ -273,7 +273,8 @@ static void plan_staged(iccg_ctx* c)
 {
     QSys& Q = c->Q;
     Q.staged = false;
-    const int gmax = std::max(1, std::min(16, 512 / (32 * std::max(1, Q.maxu))));
+    const int cap_rows = c->stage_rows;
+    const int gmax = std::max(1, std::min(16, cap_rows / (32 * std::max(1, Q.maxu))));
     const size_t lim = (size_t)std::max(0, c->smem_optin - 2048);
     const size_t budget = c->stage_kb > 0 ? std::min(lim, (size_t)c->stage_kb * 1024) : lim;
     std::vector<BatchDesc> bds;
@@ -338,7 +339,7 @@ static void plan_staged(iccg_ctx* c)
             }
             while (d.ng < gmax && g + d.ng < g1 && Q.st_fit[(size_t)l]) {
                 const BatchDesc e = describe(g, d.ng + 1);
-                if (e.qe - e.qb > 512 || stage_bytes(l, e) > budget) break;
+                if (e.qe - e.qb > cap_rows || stage_bytes(l, e) > budget) break;
                 d = e;
             }
             for (int s = d.sb + 1; s < d.se; ++s)

@@ -254,7 +254,11 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
    ICCG_OPT_SPMV_PACK (default 1), lane-interleaved FP32 SpMV: the matrix
    entries are read as one 8-byte word of value and column instead of two
    4-byte loads (an extra packed copy of A's FP32 values and columns).  The
-   same bits either way. */
+   same bits either way.
+   ICCG_OPT_STAGE_ROWS (default 512, 32 to 8192): the staged sweep's batches
+   hold up to 16 unit groups and this many rows (a single larger group is one
+   batch); more rows give more chains per CTA and larger stage buffers.  The
+   same bits for any value. */
 #define ICCG_OPT_TILED 0
 #define ICCG_OPT_SWEEP 1
 #define ICCG_OPT_PDL 2
@@ -264,6 +268,7 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
 #define ICCG_OPT_FUSE_UPDATE 6
 #define ICCG_OPT_DEFER_X 7
 #define ICCG_OPT_SPMV_PACK 8
+#define ICCG_OPT_STAGE_ROWS 9
 int iccg_ctx_set_option(iccg_ctx* ctx, int option, long long value);
 
 /* Uploads A_run (the matrix conjugate_gradient runs on, cg_crs.cpp:442-447):

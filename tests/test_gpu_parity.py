@@ -736,3 +736,28 @@ def test_gpu_packed_spmv_gives_the_same_bits(which):
     assert np.array_equal(out[1][0], out[0][0])
     assert np.array_equal(out[1][1], out[0][1]) and out[1][2].iters == out[0][2].iters
     ctx.close()
+
+
+@pytest.mark.parametrize("which", ["abmc_lin", "d27_mc"])
+def test_gpu_stage_rows_give_the_same_bits(which):
+    """Staged batches of 256 to 2048 rows (ICCG_OPT_STAGE_ROWS): how rows are
+    grouped into CTAs changes, the arithmetic of every row does not."""
+    P = {"abmc_lin": lambda: pb.config_abmc_aniso(40, 16, "linear"),
+         "d27_mc": lambda: pb.config_diffusion27(24, "piccg")}[which]()
+    ctx = _ctx_for(P.A_run, P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    r = ib.gen_uniform(P.A_run.n, 47)
+    out = {}
+    for rows in (512, 256, 1024, 2048):
+        ctx.set_option(ib.OPT_STAGE_ROWS, rows)
+        res = []
+        for st in (ib.STORE_FP64, ib.STORE_FP32):
+            x = np.zeros(P.A_run.n)
+            rr = ctx.solve(P.b_run, x, 10000, 1e-8, storage=st)
+            res.append((ctx.apply(r, st), x, rr.iters))
+        out[rows] = res
+    ctx.set_option(ib.OPT_STAGE_ROWS, 512)
+    for rows in (256, 1024, 2048):
+        for a, b in zip(out[rows], out[512]):
+            assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
+    ctx.close()
