@@ -276,7 +276,7 @@ struct iccg_ctx {
     int sweep_kernel = 0;   // ICCG_OPT_SWEEP: 0 staged where it fits, 1 two-phase per-slice kernel
     bool pdl = true;        // ICCG_OPT_PDL: programmatic dependent launch
     int stage_kb = 0;       // ICCG_OPT_STAGE_KB: staged-sweep buffer budget (0: the opt-in maximum)
-    int stage_rows = 512;   // ICCG_OPT_STAGE_ROWS: rows of a staged batch at most (one group may exceed it)
+    int stage_rows = 256;   // ICCG_OPT_STAGE_ROWS: rows of a staged batch at most (one group may exceed it)
     int stage_bufs = 1;     // ICCG_OPT_STAGE_BUFS: staged-sweep buffers per CTA (1 or 2)
     int smem_optin = 0;     // largest dynamic shared memory per CTA
     bool persist = false;   // ICCG_OPT_PERSIST: the IC(0) apply as one persistent launch where planned

@@ -264,7 +264,7 @@ static bool plan_staged_type(iccg_ctx* c, int k)
 }
 
 // Batches of the staged sweeps: consecutive groups of one level, at most 16
-// groups and ICCG_OPT_STAGE_ROWS rows (512), and as many groups as keep two stage buffers of every
+// groups and ICCG_OPT_STAGE_ROWS rows (256), and as many groups as keep two stage buffers of every
 // type the staged kernel runs with (FP64 and FP32 forward, FP32 backward)
 // within the budget (ICCG_OPT_STAGE_KB, default the opt-in shared memory);
 // the default single buffer per CTA then takes half of it.  A level with a group that alone exceeds the budget runs on the

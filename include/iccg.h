@@ -255,10 +255,13 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
    entries are read as one 8-byte word of value and column instead of two
    4-byte loads (an extra packed copy of A's FP32 values and columns).  The
    same bits either way.
-   ICCG_OPT_STAGE_ROWS (default 512, 32 to 8192): the staged sweep's batches
+   ICCG_OPT_STAGE_ROWS (default 256, 32 to 8192): the staged sweep's batches
    hold up to 16 unit groups and this many rows (a single larger group is one
-   batch); more rows give more chains per CTA and larger stage buffers.  The
-   same bits for any value. */
+   batch); more rows give more chains per CTA and larger stage buffers, fewer
+   CTAs per SM.  The same bits for any value.  256 against 512: the 96^3
+   27-point multicolor solve 23.95 -> 22.12 ms mixed and 25.17 -> 23.95 ms
+   FP64, ABMC B=8 20.76 -> 20.47 and 40.63 -> 39.53 ms, the 128^3 7-point
+   ABMC B=16 solve unchanged (its batches are single 512-row groups). */
 #define ICCG_OPT_TILED 0
 #define ICCG_OPT_SWEEP 1
 #define ICCG_OPT_PDL 2

@@ -748,7 +748,7 @@ def test_gpu_stage_rows_give_the_same_bits(which):
     ctx.build(ib.PRECOND_IC0, 0.0)
     r = ib.gen_uniform(P.A_run.n, 47)
     out = {}
-    for rows in (512, 256, 1024, 2048):
+    for rows in (256, 512, 128, 1024, 2048):
         ctx.set_option(ib.OPT_STAGE_ROWS, rows)
         res = []
         for st in (ib.STORE_FP64, ib.STORE_FP32):
@@ -756,8 +756,8 @@ def test_gpu_stage_rows_give_the_same_bits(which):
             rr = ctx.solve(P.b_run, x, 10000, 1e-8, storage=st)
             res.append((ctx.apply(r, st), x, rr.iters))
         out[rows] = res
-    ctx.set_option(ib.OPT_STAGE_ROWS, 512)
-    for rows in (256, 1024, 2048):
-        for a, b in zip(out[rows], out[512]):
+    ctx.set_option(ib.OPT_STAGE_ROWS, 256)
+    for rows in (512, 128, 1024, 2048):
+        for a, b in zip(out[rows], out[256]):
             assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
     ctx.close()
