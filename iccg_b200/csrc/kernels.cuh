@@ -606,9 +606,10 @@ __global__ void __launch_bounds__(256) k_pack_sell(long long m, const float* __r
 }
 
 // y = A x over regular 32-row slices (slice s = Q rows [32 s, 32 s + 32)),
-// product and sum rounded separately as in spmv (cg_crs.cpp:73-75).
-template <class T, int FIN>
-__global__ void __launch_bounds__(256) k_spmv_q(int n, SellMat A, const double* __restrict__ x,
+// product and sum rounded separately as in spmv (cg_crs.cpp:73-75).  PK:
+// FP32 values read with their columns as one 8-byte word (A.pk).
+template <class T, int FIN, bool PK = false>
+__global__ void __launch_bounds__(256, PK ? 4 : 0) k_spmv_q(int n, SellMat A, const double* __restrict__ x,
                                                 double* __restrict__ y, SolverState* st, RedBuf red,
                                                 unsigned int* ticket)
 {
@@ -628,12 +629,13 @@ __global__ void __launch_bounds__(256) k_spmv_q(int n, SellMat A, const double* 
     int L = 0, c[K];
     T v[K];
     // FP32 values packed with their columns: one 8-byte load per entry
-    const int2* __restrict__ pk = sizeof(T) == 4 ? A.pk : nullptr;
+    static_assert(!PK || sizeof(T) == 4, "packed words hold FP32 values");
+    const int2* __restrict__ pk = A.pk;
     auto load = [&](int s) {
         const int i = (s << 5) + lane;
         L = i < n ? A.len[i] : 0;
         const int p0 = A.ptr[s] + lane;
-        if (pk) {
+        if (PK) {
 #pragma unroll
             for (int j = 0; j < K; ++j) {
                 const int2 e = j < L ? __ldcs(pk + p0 + 32 * j) : make_int2(0, 0);

@@ -240,9 +240,10 @@ static void spmv_path(iccg_ctx* c, int storage, const double* x, double* y, Solv
     const bool f32 = storage == ICCG_STORE_FP32;
     const int g = grid_for(c, c->n);
     if (c->use_q) {
-        SellMat A = c->Q.A.view(f32);
-        if (!c->spmv_pack) A.pk = nullptr;
-        if (f32) launch_n(c, 0, k_spmv_q<float, FIN>, (long long)c->n, c->n, A, x, y, st, red, c->ticket.get());
+        const SellMat A = c->Q.A.view(f32);
+        if (f32 && c->spmv_pack && A.pk)
+            launch_n(c, 0, k_spmv_q<float, FIN, true>, (long long)c->n, c->n, A, x, y, st, red, c->ticket.get());
+        else if (f32) launch_n(c, 0, k_spmv_q<float, FIN>, (long long)c->n, c->n, A, x, y, st, red, c->ticket.get());
         else launch_n(c, 0, k_spmv_q<double, FIN>, (long long)c->n, c->n, A, x, y, st, red, c->ticket.get());
         return;
     }

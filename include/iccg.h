@@ -385,7 +385,8 @@ int iccg_sweep_plan(iccg_ctx* ctx, int storage, int fwd, int* kinds, int* grids,
    substitution kernel (iccg_sweep_plan kind 1 or 0), which holds for the
    multicolor and ABMC schedules of the 7- and 27-point problems.
 
-   iccg_batch_solve runs nsolve solves: solve s is system system[s] (an index
+   iccg_batch_solve runs nsolve solves (no session solve may be in flight:
+   see iccg_batch_open below): solve s is system system[s] (an index
    returned by iccg_batch_add_system) with the right-hand side b[s] and the
    initial guess / solution x[s] (host arrays of that system's n doubles, A_run
    order).  Each solve gives the same iterations, status, residuals and the
