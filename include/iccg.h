@@ -261,7 +261,13 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
    CTAs per SM.  The same bits for any value.  256 against 512: the 96^3
    27-point multicolor solve 23.95 -> 22.12 ms mixed and 25.17 -> 23.95 ms
    FP64, ABMC B=8 20.76 -> 20.47 and 40.63 -> 39.53 ms, the 128^3 7-point
-   ABMC B=16 solve unchanged (its batches are single 512-row groups). */
+   ABMC B=16 solve unchanged (its batches are single 512-row groups).
+   ICCG_OPT_SPMV_TPR (default 1; 2 or 4), FP32 storage: threads per row of
+   the SpMV, for matrices with long rows.  Each of the TPR threads sums every
+   TPR-th entry of the row and the partial sums are added in a fixed order:
+   deterministic, but not the single CSR-order sum of 1 thread per row, so
+   FP32-storage results change in their last bits (FP64 storage always uses
+   one thread per row and the reference's order). */
 #define ICCG_OPT_TILED 0
 #define ICCG_OPT_SWEEP 1
 #define ICCG_OPT_PDL 2
@@ -272,6 +278,7 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
 #define ICCG_OPT_DEFER_X 7
 #define ICCG_OPT_SPMV_PACK 8
 #define ICCG_OPT_STAGE_ROWS 9
+#define ICCG_OPT_SPMV_TPR 10
 int iccg_ctx_set_option(iccg_ctx* ctx, int option, long long value);
 
 /* Uploads A_run (the matrix conjugate_gradient runs on, cg_crs.cpp:442-447):
