@@ -59,6 +59,7 @@ OPT_FUSE_UPDATE = 6
 OPT_DEFER_X = 7
 OPT_SPMV_PACK = 8
 OPT_STAGE_ROWS = 9
+OPT_SPMV_TPR = 10
 STATUS_NAMES = {0: "converged", 1: "breakdown", 2: "max_iter", 3: "nonfinite"}
 
 

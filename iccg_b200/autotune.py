@@ -37,7 +37,7 @@ from typing import Callable, Dict, List, Optional, Sequence, Tuple
 import numpy as np
 
 from . import (CRS, MODE_FUSED, OPT_DEFER_X, OPT_FUSE_UPDATE, OPT_PDL, OPT_PERSIST, OPT_SPMV_PACK, OPT_STAGE_BUFS,
-               OPT_STAGE_KB, OPT_STAGE_ROWS, OPT_SWEEP, PRECOND_IC0,
+               OPT_SPMV_TPR, OPT_STAGE_KB, OPT_STAGE_ROWS, OPT_SWEEP, PRECOND_IC0,
                STORE_FP32, Context)
 from .problems import Problem, make
 
@@ -57,12 +57,13 @@ KERNEL_OPTIONS: Tuple[Tuple[int, Tuple[int, ...]], ...] = (
     (OPT_STAGE_ROWS, (256, 512, 128)),
     (OPT_PDL, (1, 0)),
     (OPT_SPMV_PACK, (1, 0)),
+    (OPT_SPMV_TPR, (1, 2, 4)),
     (OPT_FUSE_UPDATE, (0, 1)),
     (OPT_DEFER_X, (0, 1)),
 )
 OPTION_NAMES = {OPT_PERSIST: "persist", OPT_SWEEP: "sweep", OPT_STAGE_BUFS: "stage_bufs", OPT_STAGE_KB: "stage_kb",
                 OPT_PDL: "pdl", OPT_SPMV_PACK: "spmv_pack", OPT_FUSE_UPDATE: "fuse_update", OPT_DEFER_X: "defer_x",
-                OPT_STAGE_ROWS: "stage_rows"}
+                OPT_STAGE_ROWS: "stage_rows", OPT_SPMV_TPR: "spmv_tpr"}
 
 
 @dataclass

@@ -283,6 +283,7 @@ struct iccg_ctx {
     bool fuse_update = false; // ICCG_OPT_FUSE_UPDATE: the CG update inside the forward sweep's launches
     bool defer_x = false;     // ICCG_OPT_DEFER_X: x += alpha p with the p update instead of the r update
     bool spmv_pack = true;    // ICCG_OPT_SPMV_PACK: FP32 SpMV reads (value, column) words
+    int spmv_tpr = 1;         // ICCG_OPT_SPMV_TPR: threads per row of the FP32 SpMV (1, 2 or 4)
     iccg::QSys Q;
     // preconditioner
     int pc_kind = -1;

@@ -160,6 +160,9 @@ int iccg_ctx_set_option(iccg_ctx* c, int option, long long value)
             c->defer_x = value != 0;
         } else if (option == ICCG_OPT_SPMV_PACK) {
             c->spmv_pack = value != 0;
+        } else if (option == ICCG_OPT_SPMV_TPR) {
+            if (value != 1 && value != 2 && value != 4) throw Error(ICCG_ERR_ARG, "ICCG_OPT_SPMV_TPR takes 1, 2 or 4");
+            c->spmv_tpr = (int)value;
         } else if (option == ICCG_OPT_STAGE_BUFS) {
             if (value != 1 && value != 2) throw Error(ICCG_ERR_ARG, "ICCG_OPT_STAGE_BUFS takes 1 or 2");
             c->stage_bufs = (int)value;

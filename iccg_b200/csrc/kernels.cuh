@@ -692,6 +692,73 @@ __global__ void __launch_bounds__(256, PK ? 4 : 0) k_spmv_q(int n, SellMat A, co
     if (FIN == FIN_PAP) reduce_finish<3, FIN_PAP>(a, red, st, ticket, blockIdx.x, gridDim.x);
 }
 
+// The FP32 SpMV with TPR threads per row (2 or 4) for matrices with long
+// rows: TPR warps share a slice, warp w of the slice takes the row entries
+// j = w, w + TPR, ... (coalesced: one 8-byte packed word per lane per j) and
+// sums them in that order; the TPR partial sums of a row are then added in
+// warp order.  The result is deterministic but not the single sum in CSR
+// order of k_spmv_q, so only the mixed form (FP32 storage) offers it.
+template <int TPR, int FIN>
+__global__ void __launch_bounds__(256) k_spmv_qt(int n, SellMat A, const double* __restrict__ x,
+                                                 double* __restrict__ y, SolverState* st, RedBuf red,
+                                                 unsigned int* ticket)
+{
+    grid_dep_begin();
+    if (st_done(st)) return;
+    constexpr int SPC = 8 / TPR;  // slices per CTA iteration
+    constexpr int K = 8;          // entries per warp in flight
+    __shared__ double part[8][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int sl = warp / TPR, w = warp % TPR;
+    const int nslices = (n + 31) >> 5;
+    const int2* __restrict__ pk = A.pk;
+    acc2 a[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    // every warp of the CTA runs the same number of iterations
+    for (int s0 = blockIdx.x * SPC; s0 < nslices; s0 += gridDim.x * SPC) {
+        const int s = s0 + sl;
+        const int i = (s << 5) + lane;
+        double sum = 0.0;
+        if (s < nslices && i < n) {
+            const int L = A.len[i];
+            const int p0 = A.ptr[s] + lane;
+            for (int j0 = w; j0 < L; j0 += K * TPR) {
+                int c[K];
+                float v[K];
+#pragma unroll
+                for (int u = 0; u < K; ++u) {
+                    const int j = j0 + u * TPR;
+                    const int2 e = j < L ? __ldcs(pk + p0 + 32 * j) : make_int2(0, 0);
+                    c[u] = e.y;
+                    v[u] = __int_as_float(e.x);
+                }
+                double xv[K];
+#pragma unroll
+                for (int u = 0; u < K; ++u) xv[u] = j0 + u * TPR < L ? __ldg(x + c[u]) : 0.0;
+#pragma unroll
+                for (int u = 0; u < K; ++u)
+                    if (j0 + u * TPR < L) sum = sum + (double)v[u] * xv[u];
+            }
+        }
+        part[warp][lane] = sum;
+        __syncthreads();
+        if (w == 0 && s < nslices && i < n) {
+            double t = part[warp][lane];
+#pragma unroll
+            for (int q = 1; q < TPR; ++q) t = t + part[warp + q][lane];
+            y[i] = t;
+            if (FIN == FIN_PAP) {
+                const double xi = __ldg(x + i);
+                acc2_fma(a[0], xi, t);
+                acc2_fma(a[1], xi, xi);
+                acc2_fma(a[2], t, t);
+            }
+        }
+        __syncthreads();
+    }
+    grid_dep_trigger();
+    if (FIN == FIN_PAP) reduce_finish<3, FIN_PAP>(a, red, st, ticket, blockIdx.x, gridDim.x);
+}
+
 // r = b - A x with the FP64 matrix in Q order (FIN_INIT: b.b and r.r;
 // FIN_TRUE: residual replacement when requested, r.r).
 template <int FIN>

@@ -499,7 +499,7 @@ static void ensure_q32(iccg_ctx* c)
     SetupPhase t("q.fp32_copies");
     QSys& Q = c->Q;
     sell_f32(c, Q.A);
-    if (c->spmv_pack && !Q.A.haspk) {
+    if ((c->spmv_pack || c->spmv_tpr > 1) && !Q.A.haspk) {
         Q.A.pk.alloc((size_t)Q.A.slots, &c->dev_bytes);
         if (Q.A.slots)
             launch(c, 3, k_pack_sell, grid_for(c, Q.A.slots), kThreads, (long long)Q.A.slots,

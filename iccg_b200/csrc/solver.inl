@@ -241,7 +241,20 @@ static void spmv_path(iccg_ctx* c, int storage, const double* x, double* y, Solv
     const int g = grid_for(c, c->n);
     if (c->use_q) {
         const SellMat A = c->Q.A.view(f32);
-        if (f32 && c->spmv_pack && A.pk)
+        // TPR threads per row: TPR times the threads, but every CTA writes its
+        // reduction slot, so the grid stays within the slots the partial-sum
+        // buffer holds (sized for one thread per row; the kernel strides)
+        const long long w = (long long)c->n * c->spmv_tpr;
+        auto qt_grid = [&](auto kern) {
+            return (int)std::max(1ll, std::min<long long>(occ_grid(c, kern, w), (long long)c->partial_slots));
+        };
+        if (f32 && A.pk && c->spmv_tpr == 2)
+            launch(c, 0, k_spmv_qt<2, FIN>, qt_grid(k_spmv_qt<2, FIN>), kThreads, c->n, A, x, y, st, red,
+                   c->ticket.get());
+        else if (f32 && A.pk && c->spmv_tpr == 4)
+            launch(c, 0, k_spmv_qt<4, FIN>, qt_grid(k_spmv_qt<4, FIN>), kThreads, c->n, A, x, y, st, red,
+                   c->ticket.get());
+        else if (f32 && c->spmv_pack && A.pk)
             launch_n(c, 0, k_spmv_q<float, FIN, true>, (long long)c->n, c->n, A, x, y, st, red, c->ticket.get());
         else if (f32) launch_n(c, 0, k_spmv_q<float, FIN>, (long long)c->n, c->n, A, x, y, st, red, c->ticket.get());
         else launch_n(c, 0, k_spmv_q<double, FIN>, (long long)c->n, c->n, A, x, y, st, red, c->ticket.get());

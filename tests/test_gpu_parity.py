@@ -761,3 +761,35 @@ def test_gpu_stage_rows_give_the_same_bits(which):
         for a, b in zip(out[rows], out[256]):
             assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[2] == b[2]
     ctx.close()
+
+
+@pytest.mark.parametrize("which", ["d27_mc", "knn_abmc", "abmc_lin"])
+def test_gpu_spmv_threads_per_row(which):
+    """The FP32 SpMV with 2 or 4 threads per row (ICCG_OPT_SPMV_TPR): the
+    product within FP32-storage rounding of the FP64 one, deterministic from
+    run to run, mixed solves to the true residual; FP64 storage keeps one
+    thread per row and its bits."""
+    P = {"d27_mc": lambda: pb.config_diffusion27(24, "piccg"),
+         "knn_abmc": lambda: pb.config_knn(8000, seed=5, block_size=16),
+         "abmc_lin": lambda: pb.config_abmc_aniso(40, 16, "linear")}[which]()
+    ctx = _ctx_for(P.A_run, P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    v = ib.gen_uniform(P.A_run.n, 53)
+    y64 = ctx.spmv(v, ib.STORE_FP64)
+    x64 = np.zeros(P.A_run.n)
+    r64 = ctx.solve(P.b_run, x64, 10000, 1e-8, storage=ib.STORE_FP64)
+    for tpr in (2, 4, 1):
+        ctx.set_option(ib.OPT_SPMV_TPR, tpr)
+        y = ctx.spmv(v, ib.STORE_FP32)
+        assert np.array_equal(y, ctx.spmv(v, ib.STORE_FP32))
+        assert rel_err(y, y64) < 1e-6
+        assert np.array_equal(ctx.spmv(v, ib.STORE_FP64), y64)
+        x = np.zeros(P.A_run.n)
+        r = ctx.solve(P.b_run, x, 10000, 1e-8, storage=ib.STORE_FP32)
+        assert r.converged and r.true_rel_resid <= 1e-8
+        # the mixed form's distance to the FP64 solution (conditioning x tol)
+        assert rel_err(x, x64) < 1e-5
+        x2 = np.zeros(P.A_run.n)
+        r2 = ctx.solve(P.b_run, x2, 10000, 1e-8, storage=ib.STORE_FP64)
+        assert r2.iters == r64.iters and np.array_equal(x2, x64)
+    ctx.close()
