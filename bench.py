@@ -124,7 +124,6 @@ def build_problem():
     t0 = time.perf_counter()
     P = pb.config_abmc_aniso(SIDE, BLOCK, BLOCKING, seed=0)
     return P, time.perf_counter() - t0
-    P, setup_s = build_problem()
 
 
 def bytes_model(P, storage_bytes: int):
@@ -645,6 +644,8 @@ def main():
     ap.add_argument("--variant", choices=["mc", "abmc8", "abmc16", "abmc32"], default="mc",
                     help="diffusion27 with --kernel-only: the ordering of the system")
     ap.add_argument("--systems", type=int, default=512, help="batched: number of systems")
+    ap.add_argument("--no-batch-tune", action="store_true",
+                    help="batched: greedy multicolor for every system instead of the tuned orderings")
     ap.add_argument("--threads", type=int, default=16, help="batched / serving: concurrent solves")
     ap.add_argument("--requests", type=int, default=400, help="serving: requests per arrival rate")
     ap.add_argument("--max-points", type=int, default=1000000, help="serving: largest kNN system")
@@ -665,33 +666,51 @@ def main():
         run_gpu(args)
 
 
-def _batched_problems(count: int, seed: int = 4):
-    """The batched workload's systems: 50/50 a 2D 5-point Poisson problem with
-    side U{32..256} and a 3D 7-point Laplacian with side U{16..48}, greedy
-    multicolor each."""
+def _batched_matrices(count: int, seed: int = 4):
+    """The batched workload's matrices: 50/50 a 2D 5-point Poisson problem
+    with side U{32..256} and a 3D 7-point Laplacian with side U{16..48}."""
     import iccg_b200.problems as pb
     rng = np.random.default_rng(seed)
-    probs = []
-    for i in range(count):
+    mats = []
+    for _ in range(count):
         if rng.random() < 0.5:
-            probs.append(pb.make(pb.poisson2d(int(rng.integers(32, 257))), "piccg", seed=i))
+            mats.append(pb.poisson2d(int(rng.integers(32, 257))))
         else:
-            probs.append(pb.make(pb.laplace3d_aniso(int(rng.integers(16, 49)), 1.0), "piccg", seed=i))
-    return probs
+            mats.append(pb.laplace3d_aniso(int(rng.integers(16, 49)), 1.0))
+    return mats
+
+
+def _batched_problems(count: int, seed: int = 4, tune: bool = False, device: int = 0):
+    """The batched workload's systems, greedy multicolor each; with `tune`
+    the ordering of each class of systems (autotune.tune_batch: entries per
+    row and power of two of the size) is the fastest of multicolor and ABMC
+    with 8, 16 and 32-row blocks, timed on the class's largest system.
+    Returns the problems and the tuner's table (None untuned)."""
+    import iccg_b200.problems as pb
+    mats = _batched_matrices(count, seed)
+    if not tune:
+        return [pb.make(A, "piccg", seed=i) for i, A in enumerate(mats)], None
+    import iccg_b200.autotune as at
+    probs, table = at.tune_batch(mats, seeds=list(range(count)), tol=TOL, device=device)
+    return probs, [{"class": list(r["class"]), "systems": r["systems"], "tuned_on_rows": r["tuned_on_rows"],
+                    "choice": r["choice"], "ms": {t["candidate"]: t["ms"] for t in r["trials"]}} for r in table]
 
 
 def batched_case(count: int, nrhs: int = 4, steps: int = 3, warmup: int = 1, device: int = 0,
-                 compare_streams: bool = True, sample: int = 32):
+                 compare_streams: bool = True, sample: int = 32, tune: bool = True):
     """All count x nrhs solves of the batched workload through the batched
     engine (ib.Batch: one launch per CG step for every solve), FP32 A and L,
     FP64 vectors and reductions, tol 1e-8.  Reports solves/s from the device
     time (CUDA events) and end to end (host arrays in and out, wall clock),
     per-solve latency percentiles (batch start to the solve's stop, device
     clock), the algorithmic GB/s of the iterations, and the same solves one
-    at a time (fused mixed path per system, and plain FP64) on a sample."""
+    at a time (fused mixed path per system, and plain FP64) on a sample.
+    `tune`: orderings per class of systems by the tuner (its time is
+    reported as setup_s.tune)."""
     import iccg_b200 as ib
     t0 = time.perf_counter()
-    probs = _batched_problems(count)
+    probs, table = _batched_problems(count, tune=tune, device=device)
+    tune_s = time.perf_counter() - t0
     import iccg_b200.problems as pb
     rhs = [[pb.with_rhs(P, seed=1000 * i + k).b_run.copy() for k in range(nrhs)] for i, P in enumerate(probs)]
     host_s = time.perf_counter() - t0
@@ -744,7 +763,11 @@ def batched_case(count: int, nrhs: int = 4, steps: int = 3, warmup: int = 1, dev
            "launches_per_batch": int(launches),
            "setup_s": {"host": round(host_s, 2), "upload_and_ic0": round(upload_s, 2),
                        "first_batch_with_layouts": round(first_s, 2)},
-           "steps": steps}
+           "steps": steps,
+           "orderings": "tuned per class" if tune else "greedy multicolor"}
+    if tune:
+        out["setup_s"]["tune"] = round(tune_s, 2)
+        out["tuning"] = table
     # the same solves one at a time: the per-system fused mixed path (its
     # own CUDA graphs) and the plain FP64 path, on a sample of the solves
     pick = list(range(0, nsolve, max(1, nsolve // sample)))
@@ -795,9 +818,12 @@ def run_batched(args):
     threads)."""
     import torch
     torch.cuda.set_device(0)
-    out = batched_case(args.systems, 4, steps=max(1, args.steps), warmup=max(1, args.warmup))
+    out = batched_case(args.systems, 4, steps=max(1, args.steps), warmup=max(1, args.warmup),
+                       tune=not args.no_batch_tune)
     line = {"workload": "batched", **out,
-            "storage": "fp32 A and L, fp64 vectors", "preconditioner": "IC(0), greedy multicolor",
+            "storage": "fp32 A and L, fp64 vectors",
+            "preconditioner": "IC(0), " + ("greedy multicolor" if args.no_batch_tune else
+                                           "multicolor or ABMC per class of systems (tuned)"),
             "data": "synthetic",
             "timing": "device: CUDA events around each batch on the batch's stream (median over steps); "
                       "e2e: wall clock of Batch.solve with host arrays in and out"}

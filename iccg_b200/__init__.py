@@ -60,6 +60,7 @@ OPT_DEFER_X = 7
 OPT_SPMV_PACK = 8
 OPT_STAGE_ROWS = 9
 OPT_SPMV_TPR = 10
+OPT_EARLY = 11
 STATUS_NAMES = {0: "converged", 1: "breakdown", 2: "max_iter", 3: "nonfinite"}
 
 

@@ -13,6 +13,11 @@ candidates on the matrix itself.
   fastest ``Problem`` with the table of timings. Candidates differ in
   iteration count as well as in speed per iteration; the tuner compares
   time to tolerance.
+* ``tune_batch(matrices, ...)`` picks the ordering of every system of a
+  batch: the systems are grouped into classes (by default the rounded
+  entries per row and the power of two of the row count), the ordering of
+  the largest system of each class is tuned as above, and every system of
+  the class is built with it.
 * ``tune_kernels(ctx, b_run, ...)`` chooses the context options of a built
   system by coordinate search: for each option in turn it keeps the value
   with the lowest median solve time, the others held at their best so far.
@@ -32,11 +37,11 @@ from __future__ import annotations
 
 import statistics
 from dataclasses import dataclass, field
-from typing import Callable, Dict, List, Optional, Sequence, Tuple
+from typing import Callable, Dict, Hashable, List, Optional, Sequence, Tuple
 
 import numpy as np
 
-from . import (CRS, MODE_FUSED, OPT_DEFER_X, OPT_FUSE_UPDATE, OPT_PDL, OPT_PERSIST, OPT_SPMV_PACK, OPT_STAGE_BUFS,
+from . import (CRS, MODE_FUSED, OPT_DEFER_X, OPT_EARLY, OPT_FUSE_UPDATE, OPT_PDL, OPT_PERSIST, OPT_SPMV_PACK, OPT_STAGE_BUFS,
                OPT_SPMV_TPR, OPT_STAGE_KB, OPT_STAGE_ROWS, OPT_SWEEP, PRECOND_IC0,
                STORE_FP32, Context)
 from .problems import Problem, make
@@ -48,6 +53,11 @@ ORDERINGS: Tuple[Tuple[str, int, str], ...] = (("piccg", 0, "bfs"), ("abmc", 8, 
                                                ("abmc", 32, "bfs"), ("abmc", 16, "linear"),
                                                ("abmc", 32, "linear"))
 
+# the candidates per class of a batch: small systems, so the 8-row blocks
+# (more parallel chains) are in and the linear blockings are not
+BATCH_ORDERINGS: Tuple[Tuple[str, int, str], ...] = (("piccg", 0, "bfs"), ("abmc", 8, "bfs"), ("abmc", 16, "bfs"),
+                                                     ("abmc", 32, "bfs"))
+
 # option -> candidate values, in the order they are tried (the first is the default)
 KERNEL_OPTIONS: Tuple[Tuple[int, Tuple[int, ...]], ...] = (
     (OPT_PERSIST, (0, 1)),
@@ -56,6 +66,7 @@ KERNEL_OPTIONS: Tuple[Tuple[int, Tuple[int, ...]], ...] = (
     (OPT_STAGE_KB, (0, 160, 112, 80)),
     (OPT_STAGE_ROWS, (256, 512, 128)),
     (OPT_PDL, (1, 0)),
+    (OPT_EARLY, (1, 0, 3)),
     (OPT_SPMV_PACK, (1, 0)),
     (OPT_SPMV_TPR, (1, 2, 4)),
     (OPT_FUSE_UPDATE, (0, 1)),
@@ -63,7 +74,7 @@ KERNEL_OPTIONS: Tuple[Tuple[int, Tuple[int, ...]], ...] = (
 )
 OPTION_NAMES = {OPT_PERSIST: "persist", OPT_SWEEP: "sweep", OPT_STAGE_BUFS: "stage_bufs", OPT_STAGE_KB: "stage_kb",
                 OPT_PDL: "pdl", OPT_SPMV_PACK: "spmv_pack", OPT_FUSE_UPDATE: "fuse_update", OPT_DEFER_X: "defer_x",
-                OPT_STAGE_ROWS: "stage_rows", OPT_SPMV_TPR: "spmv_tpr"}
+                OPT_STAGE_ROWS: "stage_rows", OPT_SPMV_TPR: "spmv_tpr", OPT_EARLY: "early"}
 
 
 @dataclass
@@ -177,3 +188,46 @@ def tune_kernels(ctx: Context, b_run: np.ndarray, storage: int = STORE_FP32, tol
     choice["ms"] = best_ms
     return TuneResult(best=",".join(f"{k}={v}" for k, v in choice.items() if k != "ms"), trials=trials,
                       choice=choice)
+
+
+def batch_class(A: CRS) -> Tuple[int, int]:
+    """Default class of a batch system: (rounded entries per row, bit length
+    of the row count), e.g. every 2D 5-point system of 2 049 to 4 096 rows."""
+    n = max(A.n, 1)
+    return int(round(A.nnz / n)), int(n - 1).bit_length()
+
+
+def tune_batch(matrices: Sequence[CRS], classes: Optional[Sequence[Hashable]] = None,
+               candidates: Sequence[Tuple] = BATCH_ORDERINGS, storage: int = STORE_FP32, tol: float = 1e-8,
+               seeds: Optional[Sequence[int]] = None, device: int = 0, reps: int = 1,
+               timer: Optional[Callable[[Problem], Tuple[float, int, bool]]] = None
+               ) -> Tuple[List[Problem], List[dict]]:
+    """Orderings for the systems of a batch (original, unpermuted matrices).
+    Systems with the same class (`classes[i]`, default `batch_class`) share
+    one choice: the one `tune_ordering` makes for the class's largest system.
+    Returns the built problems, in the order of `matrices`, and one row per
+    class: its key, members, the system tuned and the timings."""
+    m = len(matrices)
+    keys = list(classes) if classes is not None else [batch_class(A) for A in matrices]
+    if len(keys) != m:
+        raise ValueError("one class per matrix")
+    seeds = list(seeds) if seeds is not None else list(range(m))
+    if len(seeds) != m:
+        raise ValueError("one seed per matrix")
+    members: Dict[Hashable, List[int]] = {}
+    for i, k in enumerate(keys):
+        members.setdefault(k, []).append(i)
+    out: List[Optional[Problem]] = [None] * m
+    rows = []
+    for key, idx in members.items():
+        rep = max(idx, key=lambda i: (matrices[i].n, -i))
+        P, res = tune_ordering(matrices[rep], candidates, storage=storage, tol=tol, seed=seeds[rep], device=device,
+                               reps=reps, timer=timer)
+        best = next(c for c in candidates if _label(c[0], c[1], c[2] if len(c) > 2 else "bfs") == res.best)
+        blocking = best[2] if len(best) > 2 else "bfs"
+        for i in idx:
+            out[i] = P if i == rep else make(matrices[i], best[0], block_size=max(best[1], 1), blocking=blocking,
+                                             seed=seeds[i], name=res.best)
+        rows.append({"class": key, "systems": len(idx), "tuned_on_rows": matrices[rep].n, "choice": res.best,
+                     "trials": res.table()})
+    return [P for P in out if P is not None], rows

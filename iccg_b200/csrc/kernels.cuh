@@ -302,16 +302,43 @@ template <int FIN>
 __global__ void __launch_bounds__(256) k_update(int n, double alpha_arg, const double* __restrict__ p,
                                                 const double* __restrict__ Ap, double* __restrict__ x,
                                                 double* __restrict__ r, SolverState* st, RedBuf red,
-                                                unsigned int* ticket)
+                                                unsigned int* ticket, int early)
 {
-    grid_dep_begin();
-    if (st_done(st)) return;
     constexpr bool DOX = FIN != FIN_UPDX;
-    const double alpha = st ? st->alpha : alpha_arg;
-    acc2 a[1] = {{0.0, 0.0}};
     // pairs of elements as 16-byte accesses, two pairs in flight per thread
     // (all vectors 16-byte aligned; otherwise one element at a time)
     const bool vec = (((uintptr_t)Ap | (uintptr_t)r | (DOX ? ((uintptr_t)p | (uintptr_t)x) : 0)) & 15) == 0;
+    const int n2 = n >> 1;
+    const int stride = gridDim.x * blockDim.x;
+    const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const double2* __restrict__ p2 = reinterpret_cast<const double2*>(p);
+    const double2* __restrict__ q2 = reinterpret_cast<const double2*>(Ap);
+    double2* __restrict__ x2 = reinterpret_cast<double2*>(x);
+    double2* __restrict__ r2 = reinterpret_cast<double2*>(r);
+    // early: r, x and p of the thread's first two pairs were written before
+    // the launch just before this one (the SpMV), so they load before the
+    // wait on it, and the next launch is let in right after the wait
+    const bool ew = early && vec;
+    if (!ew) grid_dep_begin();
+    double2 pre[2][3];
+    if (ew) {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int ik = i0 + k * stride;
+            if (ik < n2) {
+                pre[k][0] = __ldcg(r2 + ik);
+                if (DOX) {
+                    pre[k][1] = __ldcg(p2 + ik);
+                    pre[k][2] = __ldcg(x2 + ik);
+                }
+            }
+        }
+        grid_dep_begin();
+        grid_dep_trigger();
+    }
+    if (st_done(st)) return;
+    const double alpha = st ? st->alpha : alpha_arg;
+    acc2 a[1] = {{0.0, 0.0}};
     if (!vec) {
         for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
             if (DOX) x[k] = fma(alpha, p[k], x[k]);
@@ -323,18 +350,13 @@ __global__ void __launch_bounds__(256) k_update(int n, double alpha_arg, const d
         if (FIN != FIN_NONE) reduce_finish<1, FIN>(a, red, st, ticket, blockIdx.x, gridDim.x);
         return;
     }
-    const int n2 = n >> 1;
-    const int stride = gridDim.x * blockDim.x;
-    const double2* __restrict__ p2 = reinterpret_cast<const double2*>(p);
-    const double2* __restrict__ q2 = reinterpret_cast<const double2*>(Ap);
-    double2* __restrict__ x2 = reinterpret_cast<double2*>(x);
-    double2* __restrict__ r2 = reinterpret_cast<double2*>(r);
-    auto pair = [&](int i) {
+    // k < 0: load the pair; k = 0, 1: the pair loaded before the wait
+    auto pair = [&](int i, int k) {
         const double2 qv = q2[i];
-        double2 rv = r2[i];
+        double2 rv = k < 0 ? r2[i] : pre[k][0];
         if (DOX) {
-            const double2 pv = p2[i];
-            double2 xv = x2[i];
+            const double2 pv = k < 0 ? p2[i] : pre[k][1];
+            double2 xv = k < 0 ? x2[i] : pre[k][2];
             xv.x = fma(alpha, pv.x, xv.x);
             xv.y = fma(alpha, pv.y, xv.y);
             x2[i] = xv;
@@ -347,12 +369,22 @@ __global__ void __launch_bounds__(256) k_update(int n, double alpha_arg, const d
             acc2_fma(a[0], rv.y, rv.y);
         }
     };
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    for (; i + stride < n2; i += 2 * stride) {
-        pair(i);
-        pair(i + stride);
+    int i = i0;
+    if (ew) {
+        if (i + stride < n2) {
+            pair(i, 0);
+            pair(i + stride, 1);
+            i += 2 * stride;
+        } else if (i < n2) {
+            pair(i, 0);
+            i = n2;
+        }
     }
-    if (i < n2) pair(i);
+    for (; i + stride < n2; i += 2 * stride) {
+        pair(i, -1);
+        pair(i + stride, -1);
+    }
+    if (i < n2) pair(i, -1);
     if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
         const int k = n - 1;
         if (DOX) x[k] = fma(alpha, p[k], x[k]);
@@ -360,7 +392,7 @@ __global__ void __launch_bounds__(256) k_update(int n, double alpha_arg, const d
         r[k] = rk;
         if (FIN != FIN_NONE) acc2_fma(a[0], rk, rk);
     }
-    grid_dep_trigger();
+    if (!ew) grid_dep_trigger();
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(a, red, st, ticket, blockIdx.x, gridDim.x);
 }
 
@@ -369,9 +401,35 @@ __global__ void __launch_bounds__(256) k_update(int n, double alpha_arg, const d
 // (the update fused into the forward sweep) x += alpha p comes first, with
 // the p of this iteration (cg_crs.cpp:137-138).
 __global__ void __launch_bounds__(256) k_xpay(int n, double beta_arg, const double* __restrict__ z,
-                                              double* __restrict__ p, SolverState* st, double* __restrict__ x)
+                                              double* __restrict__ p, SolverState* st, double* __restrict__ x,
+                                              int early)
 {
-    grid_dep_begin();
+    const bool vec = (((uintptr_t)z | (uintptr_t)p | (uintptr_t)x) & 15) == 0;
+    const int n2 = n >> 1;
+    const int stride = gridDim.x * blockDim.x;
+    const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const double2* __restrict__ z2 = reinterpret_cast<const double2*>(z);
+    double2* __restrict__ p2 = reinterpret_cast<double2*>(p);
+    double2* __restrict__ x2 = reinterpret_cast<double2*>(x);
+    // early: p and x of the thread's first two pairs were written before
+    // the launch just before this one (the preconditioner apply, which
+    // writes z), so they load before the wait on it, and the next launch is
+    // let in right after the wait
+    const bool ew = early && vec;
+    if (!ew) grid_dep_begin();
+    double2 pre[2][2];
+    if (ew) {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int ik = i0 + k * stride;
+            if (ik < n2) {
+                pre[k][0] = __ldcg(p2 + ik);
+                if (x) pre[k][1] = __ldcg(x2 + ik);
+            }
+        }
+        grid_dep_begin();
+        grid_dep_trigger();
+    }
     if (st) {
         // a stop the persistent apply deferred: make it the solve's status
         const int pd = *(volatile const int*)&st->pend;
@@ -383,22 +441,18 @@ __global__ void __launch_bounds__(256) k_xpay(int n, double beta_arg, const doub
     if (st_done(st)) return;
     const double beta = st ? st->beta : beta_arg;
     const double alpha = (st && x) ? st->alpha : 0.0;
-    if ((((uintptr_t)z | (uintptr_t)p | (uintptr_t)x) & 15) != 0) {
+    if (!vec) {
         for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
             if (x) x[k] = fma(alpha, p[k], x[k]);
             p[k] = fma(beta, p[k], z[k]);
         }
     } else {
-        const int n2 = n >> 1;
-        const int stride = gridDim.x * blockDim.x;
-        const double2* __restrict__ z2 = reinterpret_cast<const double2*>(z);
-        double2* __restrict__ p2 = reinterpret_cast<double2*>(p);
-        double2* __restrict__ x2 = reinterpret_cast<double2*>(x);
-        auto pair = [&](int i) {
+        // k < 0: load the pair; k = 0, 1: the pair loaded before the wait
+        auto pair = [&](int i, int k) {
             const double2 zv = z2[i];
-            double2 pv = p2[i];
+            double2 pv = k < 0 ? p2[i] : pre[k][0];
             if (x) {
-                double2 xv = x2[i];
+                double2 xv = k < 0 ? x2[i] : pre[k][1];
                 xv.x = fma(alpha, pv.x, xv.x);
                 xv.y = fma(alpha, pv.y, xv.y);
                 x2[i] = xv;
@@ -407,18 +461,28 @@ __global__ void __launch_bounds__(256) k_xpay(int n, double beta_arg, const doub
             pv.y = fma(beta, pv.y, zv.y);
             p2[i] = pv;
         };
-        int i = blockIdx.x * blockDim.x + threadIdx.x;
-        for (; i + stride < n2; i += 2 * stride) {
-            pair(i);
-            pair(i + stride);
+        int i = i0;
+        if (ew) {
+            if (i + stride < n2) {
+                pair(i, 0);
+                pair(i + stride, 1);
+                i += 2 * stride;
+            } else if (i < n2) {
+                pair(i, 0);
+                i = n2;
+            }
         }
-        if (i < n2) pair(i);
+        for (; i + stride < n2; i += 2 * stride) {
+            pair(i, -1);
+            pair(i + stride, -1);
+        }
+        if (i < n2) pair(i, -1);
         if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
             if (x) x[n - 1] = fma(alpha, p[n - 1], x[n - 1]);
             p[n - 1] = fma(beta, p[n - 1], z[n - 1]);
         }
     }
-    grid_dep_trigger();
+    if (!ew) grid_dep_trigger();
     if (st && blockIdx.x == 0 && threadIdx.x == 0) {
         const int k1 = st->k + 1;
         st->k = k1;
@@ -611,10 +675,8 @@ __global__ void __launch_bounds__(256) k_pack_sell(long long m, const float* __r
 template <class T, int FIN, bool PK = false>
 __global__ void __launch_bounds__(256, PK ? 4 : 0) k_spmv_q(int n, SellMat A, const double* __restrict__ x,
                                                 double* __restrict__ y, SolverState* st, RedBuf red,
-                                                unsigned int* ticket)
+                                                unsigned int* ticket, int early)
 {
-    grid_dep_begin();
-    if (st_done(st)) return;
     const T* __restrict__ val = (const T*)A.val;
     const int* __restrict__ col = A.col;
     acc2 a[3] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
@@ -650,8 +712,17 @@ __global__ void __launch_bounds__(256, PK ? 4 : 0) k_spmv_q(int n, SellMat A, co
             }
         }
     };
+    // early: the first slice's matrix words do not depend on the launch
+    // just before, so they load before the wait on it, and the next launch
+    // is let in right after the wait
+    if (!early) grid_dep_begin();
     int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (s < nslices) load(s);
+    if (early) {
+        grid_dep_begin();
+        grid_dep_trigger();
+    }
+    if (st_done(st)) return;
     for (; s < nslices; s += stride) {
         const int Lc = L;
         int cc[K];
@@ -688,7 +759,7 @@ __global__ void __launch_bounds__(256, PK ? 4 : 0) k_spmv_q(int n, SellMat A, co
             }
         }
     }
-    grid_dep_trigger();
+    if (!early) grid_dep_trigger();
     if (FIN == FIN_PAP) reduce_finish<3, FIN_PAP>(a, red, st, ticket, blockIdx.x, gridDim.x);
 }
 
@@ -1195,23 +1266,31 @@ __device__ __forceinline__ int stage_range(unsigned char* dst, const void* src, 
     return first - a0;
 }
 
+// Parts of a staged batch: the level's own arrays (slice words, pivots, row
+// words, columns, values: the same in every sweep), the input rows and r.
+enum StagePart { SP_MAT = 1, SP_IN = 2, SP_RD = 4, SP_ALL = 7, SP_EARLY = 8 };
+
 // STAGE_IN = false leaves the inputs to the caller (the persistent apply's
-// fused update writes them into the tile itself).
-template <class T, bool FWD, bool WITH_R, bool STAGE_IN = true>
+// fused update writes them into the tile itself).  `parts` selects what is
+// copied; COMMIT closes the copy group (a batch staged in two calls commits
+// with the second).
+template <class T, bool FWD, bool WITH_R, bool STAGE_IN = true, bool COMMIT = true>
 __device__ __forceinline__ void stage_batch(unsigned char* base, const StageLayout& Ly, const BatchDesc& d,
                                             const SliceMeta* meta, const SellMat& M, const T* dg,
-                                            const double* in, const double* rdot)
+                                            const double* in, const double* rdot, int parts = SP_ALL)
 {
     const int rows = d.qe - d.qb;
     const int p0 = FWD ? d.ps0 : d.pt0, p1 = FWD ? d.ps1 : d.pt1;
-    stage_range(base + Ly.meta, meta, 16, d.sb, d.se - d.sb);
-    if (STAGE_IN) stage_range(base + Ly.in, in, 8, d.qb, rows);
-    if (WITH_R) stage_range(base + Ly.rd, rdot, 8, d.qb, rows);
-    stage_range(base + Ly.piv, dg, (int)sizeof(T), d.qb, rows);
-    stage_range(base + Ly.len, M.len, 4, d.qb, rows);
-    stage_range(base + Ly.col, M.col, 4, p0, p1 - p0);
-    stage_range(base + Ly.val, M.val, (int)sizeof(T), p0, p1 - p0);
-    cp_async_commit();
+    if (parts & SP_MAT) {
+        stage_range(base + Ly.meta, meta, 16, d.sb, d.se - d.sb);
+        stage_range(base + Ly.piv, dg, (int)sizeof(T), d.qb, rows);
+        stage_range(base + Ly.len, M.len, 4, d.qb, rows);
+        stage_range(base + Ly.col, M.col, 4, p0, p1 - p0);
+        stage_range(base + Ly.val, M.val, (int)sizeof(T), p0, p1 - p0);
+    }
+    if (STAGE_IN && (parts & SP_IN)) stage_range(base + Ly.in, in, 8, d.qb, rows);
+    if (WITH_R && (parts & SP_RD)) stage_range(base + Ly.rd, rdot, 8, d.qb, rows);
+    if (COMMIT) cp_async_commit();
 }
 
 // Phase G of a staged batch (all threads): the earlier-level values of each
@@ -1565,30 +1644,56 @@ __device__ __forceinline__ void st_chain(const BatchDesc& cur, unsigned char* ba
     }
 }
 
-template <class T, bool FWD, int FIN, bool EXACT, int NB = 2>
+// EW (loads before the wait): the first batch's copy of the level's own
+// arrays, and of the input rows / r where `early` (SP_IN / SP_RD bits) says
+// the launch just before this one did not write them, is issued before the
+// wait on that launch (griddepcontrol.wait), and the next launch is let in
+// right after the wait; the rest of the batch follows the wait.  Every read
+// of data the launch before may write (earlier-level values, the solver
+// state) comes after the wait.  A template argument: as a run-time flag it
+// made the forward FP32 form spill.
+template <class T, bool FWD, int FIN, bool EXACT, int NB = 2, bool EW = false>
 __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDesc* __restrict__ bd, int rows_cap,
                                                   int slots_cap, int slices_cap, const int* __restrict__ sl0,
                                                   const int* __restrict__ glen, const SliceMeta* __restrict__ meta,
                                                   SellMat M, const T* __restrict__ dg, const double* in,
                                                   double* out, const double* __restrict__ rdot, int slot0,
                                                   int nslots, SolverState* st, RedBuf red, unsigned int* ticket,
-                                                  UpdArgs U)
+                                                  UpdArgs U, int early)
 {
-    grid_dep_begin();
-    if (st_done(st)) return;
     // FIN_UPDX (forward, one buffer): the fused CG update; each batch's r
     // and Ap are staged (Ap in the area of the backward sweep's r)
     constexpr bool UPD = FIN == FIN_UPDX;
     static_assert(!UPD || (FWD && NB == 1), "the fused update runs in single-buffered forward sweeps");
     constexpr bool with_r = FIN == FIN_RZ || FIN == FIN_RZ0;
     constexpr bool with_pv = !(FWD || !EXACT);
-    const double alpha = UPD ? st->alpha : 0.0;
     extern __shared__ __align__(16) unsigned char smem_st[];
     const StageLayout Ly = stage_layout(rows_cap, slots_cap, slices_cap, (int)sizeof(T), with_r || UPD, with_pv);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const double* prev = out;  // earlier-level values: read-only in this launch
     acc2 rz[1] = {{0.0, 0.0}};
     const double* stage2 = UPD ? U.Ap : rdot;
+    int b = b0 + blockIdx.x;
+    constexpr bool ew = EW;
+    // the parts of the first batch copied before the wait (none: wait first)
+    const int first = ew ? SP_MAT | (UPD ? 0 : early & (SP_IN | SP_RD)) : 0;
+    if (!ew) grid_dep_begin();
+    if (ew && b < b1) {
+        const BatchDesc d0 = bd[b];
+        stage_batch<T, FWD, with_r || UPD, true, false>(smem_st, Ly, d0, meta, M, dg, in, stage2, first);
+    }
+    if (ew) {
+        grid_dep_begin();
+        grid_dep_trigger();
+    }
+    if (st_done(st)) {
+        // the copies issued above are not in a group yet: close it, so the
+        // wait covers them, before the CTA (and its shared memory) goes
+        cp_async_commit();
+        cp_async_wait<0>();
+        return;
+    }
+    const double alpha = UPD ? st->alpha : 0.0;
 
     // the fused update of a staged batch's rows (after its copy landed):
     // r -= alpha Ap in the tile and back to r
@@ -1602,10 +1707,9 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
             acc2_fma(rz[0], rn, rn);
         }
     };
-    int b = b0 + blockIdx.x;
     if (b < b1) {
         BatchDesc cur = bd[b];
-        stage_batch<T, FWD, with_r || UPD>(smem_st, Ly, cur, meta, M, dg, in, stage2);
+        stage_batch<T, FWD, with_r || UPD>(smem_st, Ly, cur, meta, M, dg, in, stage2, SP_ALL & ~first);
         bool has_next = b + (int)gridDim.x < b1;
         BatchDesc nxt = cur;
         if (has_next) nxt = bd[b + gridDim.x];
@@ -1650,7 +1754,7 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
             has_next = has_nn;
         }
     }
-    grid_dep_trigger();
+    if (!ew) grid_dep_trigger();
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(rz, red, st, ticket, slot0 + blockIdx.x, nslots);
 }
 
@@ -1664,20 +1768,23 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
 // lane per unit; the steps' rows stream in chunks of CH, the next chunk's
 // loads in flight while the current one is chained; no shared memory.
 // ---------------------------------------------------------------------------
+// `early` as in k_sweep_st: the group words and, for FP32 storage, the first
+// chunk's level arrays and the inputs / r it names are loaded before the wait
+// on the launch just before.  (The FP64 chunks stay after the wait: held
+// across it they take the backward kernel from 114 to 142 registers, one CTA
+// per SM, and the level to two waves.)
 template <class T, bool FWD, int FIN, bool EXACT>
 __global__ void __launch_bounds__(256) k_sweep_chain(int g0, int g1, const int* __restrict__ glen,
                                                      const int* __restrict__ sl0, const SliceMeta* __restrict__ meta,
                                                      SellMat M, const T* __restrict__ dg,
                                                      const double* in, double* __restrict__ out,
                                                      const double* __restrict__ rdot, int slot0, int nslots,
-                                                     SolverState* st, RedBuf red, unsigned int* ticket, UpdArgs U)
+                                                     SolverState* st, RedBuf red, unsigned int* ticket, UpdArgs U,
+                                                     int early)
 {
-    grid_dep_begin();
-    if (st_done(st)) return;
     constexpr bool UPD = FIN == FIN_UPDX;  // forward: the fused CG update (r -= alpha Ap) on load
     constexpr bool with_r = FIN == FIN_RZ || FIN == FIN_RZ0;
     constexpr int CH = 4;
-    const double alpha = UPD ? st->alpha : 0.0;
     const T* __restrict__ val = (const T*)M.val;
     const int lane = threadIdx.x & 31;
     acc2 rz[1] = {{0.0, 0.0}};
@@ -1688,36 +1795,61 @@ __global__ void __launch_bounds__(256) k_sweep_chain(int g0, int g1, const int* 
     };
     const int wg = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     const int nwg = (int)((gridDim.x * blockDim.x) >> 5);
-    for (int g = g0 + wg; g < g1; g += nwg) {
-        const int len = glen[(size_t)g * 32];  // every unit of the group has this length
-        const int sb = sl0[g];
-        // lane r holds step r's first Q row, slot pointer and slice width
+    const bool ew = (early & SP_EARLY) != 0;
+    early = UPD ? 0 : early & (SP_IN | SP_RD);
+    int g = g0 + wg;
+    int len = 0, my_q = 0, my_p = 0, my_w = 0;
+    // lane r holds step r's first Q row, slot pointer and slice width
+    auto group = [&](int gg) {
+        len = glen[(size_t)gg * 32];  // every unit of the group has this length
+        const int sb = sl0[gg];
         const SliceMeta mine = lane < len ? meta[sb + lane] : SliceMeta{0, 0, 0, 0};
-        const int my_q = mine.q0;
-        const int my_p = FWD ? mine.pS : mine.pT;
-        const int my_w = FWD ? (mine.w >> 12) & 255 : (mine.w >> 20) & 255;
-        auto load = [&](int t0, Chunk& C) {
+        my_q = mine.q0;
+        my_p = FWD ? mine.pS : mine.pT;
+        my_w = FWD ? (mine.w >> 12) & 255 : (mine.w >> 20) & 255;
+    };
+    auto load = [&](int t0, Chunk& C, int parts) {
 #pragma unroll
-            for (int u = 0; u < CH; ++u) {
-                const int t = t0 + u;
-                const bool ok = t < len;
-                const int rs = ok ? (FWD ? t : len - 1 - t) : 0;
-                const int q = __shfl_sync(0xffffffffu, my_q, rs) + lane;
+        for (int u = 0; u < CH; ++u) {
+            const int t = t0 + u;
+            const bool ok = t < len;
+            const int rs = ok ? (FWD ? t : len - 1 - t) : 0;
+            const int q = __shfl_sync(0xffffffffu, my_q, rs) + lane;
+            if (parts & SP_MAT) {
                 const int p = __shfl_sync(0xffffffffu, my_p, rs) + lane;
                 const int w = __shfl_sync(0xffffffffu, my_w, rs);
                 C.q[u] = q;
-                C.a[u] = ok ? in[q] : 0.0;
                 C.p[u] = ok ? dg[q] : (T)1;
                 C.L[u] = ok ? M.len[q] & 0xffff : 0;
                 C.v[u] = (ok && w > 0) ? val[p] : (T)0;
-                C.rd[u] = ok ? (with_r ? rdot[q] : UPD ? U.Ap[q] : 0.0) : 0.0;
             }
-        };
+            if (parts & SP_IN) C.a[u] = ok ? __ldcg(in + q) : 0.0;
+            if (parts & SP_RD) C.rd[u] = ok ? (with_r ? __ldcg(rdot + q) : UPD ? __ldcg(U.Ap + q) : 0.0) : 0.0;
+        }
+    };
+    Chunk A, B;
+    const bool pre = ew && !EXACT;
+    if (!ew) grid_dep_begin();
+    if (g < g1) {
+        group(g);
+        if (pre) load(0, A, SP_MAT | early);
+    }
+    if (ew) {
+        grid_dep_begin();
+        grid_dep_trigger();
+    }
+    if (st_done(st)) return;
+    const double alpha = UPD ? st->alpha : 0.0;
+    for (bool first = true; g < g1; g += nwg, first = false) {
+        if (first) {
+            load(0, A, pre ? SP_ALL & ~(SP_MAT | early) : SP_ALL);
+        } else {
+            group(g);
+            load(0, A, SP_ALL);
+        }
         double last = 0.0;
-        Chunk A, B;
-        load(0, A);
         for (int t0 = 0; t0 < len; t0 += CH) {
-            if (t0 + CH < len) load(t0 + CH, B);
+            if (t0 + CH < len) load(t0 + CH, B, SP_ALL);
 #pragma unroll
             for (int u = 0; u < CH; ++u) {
                 if (t0 + u < len) {
@@ -1738,7 +1870,7 @@ __global__ void __launch_bounds__(256) k_sweep_chain(int g0, int g1, const int* 
             A = B;
         }
     }
-    grid_dep_trigger();
+    if (!ew) grid_dep_trigger();
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(rz, red, st, ticket, slot0 + blockIdx.x, nslots);
 }
 

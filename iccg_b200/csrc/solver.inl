@@ -76,6 +76,13 @@ static SweepLevel sweep_level(iccg_ctx* c, int l, bool fwd)
     return {3, Q.fgrid[l_]};
 }
 
+// 1 if this storage's solves load before the wait on the previous launch
+// (ICCG_OPT_EARLY)
+static int early_on(const iccg_ctx* c, int storage)
+{
+    return (c->early >> (storage == ICCG_STORE_FP32 ? 0 : 1)) & 1;
+}
+
 template <class T, int FIN, bool FWD, int NI, int KS>
 static void launch_q2_level(iccg_ctx* c, int l, int grid, const double* in, double* out, const double* rdot,
                             int slot0, int nslots, SolverState* st, const SellMat& M, const T* d)
@@ -92,9 +99,13 @@ static void launch_q2_level(iccg_ctx* c, int l, int grid, const double* in, doub
                 c->ticket.get());
 }
 
+// early (SP_IN / SP_RD): `in` / `rdot` were not written by the launch just
+// before this level's, so the chain-only and staged kernels may load them
+// before their wait on it
 template <class T, int FIN, bool FWD>
 static void launch_sweep_level(iccg_ctx* c, int l, const SweepLevel& sl, const double* in, double* out,
-                               const double* rdot, int slot0, int nslots, SolverState* st, UpdArgs U = UpdArgs{})
+                               const double* rdot, int slot0, int nslots, SolverState* st, UpdArgs U = UpdArgs{},
+                               int early = 0)
 {
     QSys& Q = c->Q;
     constexpr bool f32 = std::is_same<T, float>::value;
@@ -106,11 +117,12 @@ static void launch_sweep_level(iccg_ctx* c, int l, const SweepLevel& sl, const d
     const T* dg = f32 ? (const T*)(const void*)Q.r32.get() : (const T*)(const void*)Q.d64.get();
     const T* d = f32 ? (const T*)(const void*)Q.d32.get() : (const T*)(const void*)Q.d64.get();
     const int cls = FWD ? 1 : 2;
+    early = early_on(c, f32 ? ICCG_STORE_FP32 : ICCG_STORE_FP64) ? early | SP_EARLY : 0;
     switch (sl.kind) {
     case 0:
         launch(c, cls, k_sweep_chain<T, FWD, FIN, exact>, sl.grid, kThreads, Q.level_g[l_], Q.level_g[l_ + 1],
                (const int*)Q.glen.get(), (const int*)Q.sl0.get(), (const SliceMeta*)Q.meta.get(), M, dg, in, out,
-               rdot, slot0, nslots, st, red, c->ticket.get(), U);
+               rdot, slot0, nslots, st, red, c->ticket.get(), U, early);
         break;
     case 1: {
         const int slots = FWD ? Q.st_slotsS[l_] : Q.st_slotsT[l_];
@@ -120,21 +132,23 @@ static void launch_sweep_level(iccg_ctx* c, int l, const SweepLevel& sl, const d
         const size_t smem = nbuf * (size_t)stage_layout(Q.st_rows[l_], slots, Q.st_slices[l_], (int)sizeof(T),
                                                         with_r, !FWD && exact)
                                        .bytes;
+        const bool ew = (early & SP_EARLY) != 0;
         if constexpr (FIN == FIN_UPDX) {
             // the fused update runs single-buffered only (fused_update_ok)
-            auto kern = k_sweep_st<T, FWD, FIN, exact, 1>;
+            auto kern = ew ? k_sweep_st<T, FWD, FIN, exact, 1, true> : k_sweep_st<T, FWD, FIN, exact, 1>;
             allow_smem(c, kern);
             launch_smem(c, cls, kern, sl.grid, kThreads, smem, Q.lb[l_], Q.lb[l_ + 1],
                         (const BatchDesc*)Q.bdesc.get(), Q.st_rows[l_], slots, Q.st_slices[l_],
                         (const int*)Q.sl0.get(), (const int*)Q.glen.get(), (const SliceMeta*)Q.meta.get(), M, dg, in,
-                        out, rdot, slot0, nslots, st, red, c->ticket.get(), U);
+                        out, rdot, slot0, nslots, st, red, c->ticket.get(), U, early);
         } else {
-            auto kern = nbuf == 1 ? k_sweep_st<T, FWD, FIN, exact, 1> : k_sweep_st<T, FWD, FIN, exact, 2>;
+            auto kern = nbuf == 1 ? (ew ? k_sweep_st<T, FWD, FIN, exact, 1, true> : k_sweep_st<T, FWD, FIN, exact, 1>)
+                                  : (ew ? k_sweep_st<T, FWD, FIN, exact, 2, true> : k_sweep_st<T, FWD, FIN, exact, 2>);
             allow_smem(c, kern);
             launch_smem(c, cls, kern, sl.grid, kThreads, smem, Q.lb[l_], Q.lb[l_ + 1],
                         (const BatchDesc*)Q.bdesc.get(), Q.st_rows[l_], slots, Q.st_slices[l_],
                         (const int*)Q.sl0.get(), (const int*)Q.glen.get(), (const SliceMeta*)Q.meta.get(), M, dg, in,
-                        out, rdot, slot0, nslots, st, red, c->ticket.get(), U);
+                        out, rdot, slot0, nslots, st, red, c->ticket.get(), U, early);
         }
         break;
     }
@@ -195,8 +209,11 @@ static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, Solv
             s0 += fl[(size_t)l].grid;
         }
     } else {
+        // level 0's r may come from the launch just before (the update or a
+        // residual); the later levels' r does not
         for (int l = 0; l < Q.nlevels; ++l)
-            launch_sweep_level<T, FIN_NONE, true>(c, l, sweep_level<T>(c, l, true), r, y, nullptr, 0, 0, st);
+            launch_sweep_level<T, FIN_NONE, true>(c, l, sweep_level<T>(c, l, true), r, y, nullptr, 0, 0, st,
+                                                  UpdArgs{}, l > 0 ? SP_IN : 0);
     }
     std::vector<SweepLevel> bl((size_t)Q.nlevels);
     int nslots = 0;
@@ -205,8 +222,12 @@ static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, Solv
         nslots += bl[(size_t)l].grid;
     }
     int slot0 = 0;
+    // the backward level l reads the y rows the forward level l wrote (and,
+    // with the fused update, its r rows): the launch just before only for
+    // the last level; without the fused update r is older
     for (int l = Q.nlevels - 1; l >= 0; --l) {
-        launch_sweep_level<T, FIN, false>(c, l, bl[(size_t)l], y, z, r, slot0, nslots, st);
+        const int early = l < Q.nlevels - 1 ? SP_IN | SP_RD : UPD ? 0 : SP_RD;
+        launch_sweep_level<T, FIN, false>(c, l, bl[(size_t)l], y, z, r, slot0, nslots, st, UpdArgs{}, early);
         slot0 += bl[(size_t)l].grid;
     }
 }
@@ -241,6 +262,7 @@ static void spmv_path(iccg_ctx* c, int storage, const double* x, double* y, Solv
     const int g = grid_for(c, c->n);
     if (c->use_q) {
         const SellMat A = c->Q.A.view(f32);
+        const int ew = early_on(c, storage);
         // TPR threads per row: TPR times the threads, but every CTA writes its
         // reduction slot, so the grid stays within the slots the partial-sum
         // buffer holds (sized for one thread per row; the kernel strides)
@@ -255,9 +277,9 @@ static void spmv_path(iccg_ctx* c, int storage, const double* x, double* y, Solv
             launch(c, 0, k_spmv_qt<4, FIN>, qt_grid(k_spmv_qt<4, FIN>), kThreads, c->n, A, x, y, st, red,
                    c->ticket.get());
         else if (f32 && c->spmv_pack && A.pk)
-            launch_n(c, 0, k_spmv_q<float, FIN, true>, (long long)c->n, c->n, A, x, y, st, red, c->ticket.get());
-        else if (f32) launch_n(c, 0, k_spmv_q<float, FIN>, (long long)c->n, c->n, A, x, y, st, red, c->ticket.get());
-        else launch_n(c, 0, k_spmv_q<double, FIN>, (long long)c->n, c->n, A, x, y, st, red, c->ticket.get());
+            launch_n(c, 0, k_spmv_q<float, FIN, true>, (long long)c->n, c->n, A, x, y, st, red, c->ticket.get(), ew);
+        else if (f32) launch_n(c, 0, k_spmv_q<float, FIN>, (long long)c->n, c->n, A, x, y, st, red, c->ticket.get(), ew);
+        else launch_n(c, 0, k_spmv_q<double, FIN>, (long long)c->n, c->n, A, x, y, st, red, c->ticket.get(), ew);
         return;
     }
     const int* rp = c->rowptr.get();
@@ -351,7 +373,7 @@ static void solve_plain(iccg_ctx* c, const double* b, double* x, int max_iter, d
         }
         const double alpha = rz_old / pAp;
         launch_n(c, 3, k_update<FIN_NONE>, (long long)c->n, n, alpha, (const double*)p, (const double*)Ap, x, r,
-               (SolverState*)nullptr, red, c->ticket.get());
+               (SolverState*)nullptr, red, c->ticket.get(), early_on(c, ICCG_STORE_FP64));
         const double rel = std::sqrt(dot_dev(c, n, r, r)) / normb;
         res->iters = k + 1;
         res->rel_resid = rel;
@@ -363,7 +385,8 @@ static void solve_plain(iccg_ctx* c, const double* b, double* x, int max_iter, d
         apply_path<FIN_NONE>(c, ICCG_STORE_FP64, r, z, nullptr);
         const double rz_new = dot_dev(c, n, r, z);
         const double beta = rz_new / rz_old;
-        launch_n(c, 3, k_xpay, (long long)c->n, n, beta, (const double*)z, p, (SolverState*)nullptr, (double*)nullptr);
+        launch_n(c, 3, k_xpay, (long long)c->n, n, beta, (const double*)z, p, (SolverState*)nullptr, (double*)nullptr,
+                 early_on(c, ICCG_STORE_FP64));
         rz_old = rz_new;
     }
     res->status = kMaxIter;
@@ -383,7 +406,8 @@ static void fused_iteration(iccg_ctx* c, int storage, bool rr, const double* b, 
         // update, both sweeps and the two reductions in one launch
         if (storage == ICCG_STORE_FP32) launch_persist<float, true, FIN_RZ>(c, c->vr.get(), c->vy.get(), c->vz.get(), st, x);
         else launch_persist<double, true, FIN_RZ>(c, c->vr.get(), c->vy.get(), c->vz.get(), st, x);
-        launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st, (double*)nullptr);
+        launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st, (double*)nullptr,
+                 early_on(c, storage));
         return;
     }
     const bool f32 = storage == ICCG_STORE_FP32;
@@ -393,22 +417,24 @@ static void fused_iteration(iccg_ctx* c, int storage, bool rr, const double* b, 
         if (f32) apply_ic0_q<float, FIN_RZ, true>(c, c->vr.get(), c->vy.get(), c->vz.get(), st, U);
         else apply_ic0_q<double, FIN_RZ, true>(c, c->vr.get(), c->vy.get(), c->vz.get(), st, U);
         // x += alpha p, then p = z + beta p
-        launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st, x);
+        launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st, x,
+                 early_on(c, storage));
         return;
     }
     // x += alpha p with the p update (defer_x), except where the FP64
     // residual of this iteration needs the new x
     const bool dx = c->defer_x && !rr;
+    const int ew = early_on(c, storage);
     if (dx)
         launch_n(c, 3, k_update<FIN_UPDX>, (long long)c->n, n, 0.0, (const double*)c->vp.get(),
-                 (const double*)c->vAp.get(), x, c->vr.get(), st, red, c->ticket.get());
+                 (const double*)c->vAp.get(), x, c->vr.get(), st, red, c->ticket.get(), ew);
     else
         launch_n(c, 3, k_update<FIN_UPD>, (long long)c->n, n, 0.0, (const double*)c->vp.get(),
-                 (const double*)c->vAp.get(), x, c->vr.get(), st, red, c->ticket.get());
+                 (const double*)c->vAp.get(), x, c->vr.get(), st, red, c->ticket.get(), ew);
     if (rr) residual_path<FIN_TRUE>(c, (const double*)x, b, c->vr.get(), st);
     apply_path<FIN_RZ>(c, storage, c->vr.get(), c->vz.get(), st);
     launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st,
-             dx ? x : (double*)nullptr);
+             dx ? x : (double*)nullptr, ew);
 }
 
 // releases every captured iteration graph of the context
@@ -573,7 +599,8 @@ static void solve_fused(iccg_ctx* c, const double* b, double* x, int max_iter, d
         launch(c, 3, k_resume_true_check, 1, 1, st);
         residual_path<FIN_TRUE>(c, (const double*)x, b, c->vr.get(), st);
         apply_path<FIN_RZ>(c, storage, c->vr.get(), c->vz.get(), st);
-        launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st, (double*)nullptr);
+        launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st, (double*)nullptr,
+                 early_on(c, storage));
         CK(cudaMemcpyAsync(c->h_state, st, sizeof(SolverState), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
         if (c->h_state->status != kRunning) break;

@@ -267,7 +267,17 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
    TPR-th entry of the row and the partial sums are added in a fixed order:
    deterministic, but not the single CSR-order sum of 1 thread per row, so
    FP32-storage results change in their last bits (FP64 storage always uses
-   one thread per row and the reference's order). */
+   one thread per row and the reference's order).
+   ICCG_OPT_EARLY (default 1; 0 to 3): loads before the wait on the previous
+   launch, per storage (bit 0: FP32 storage, bit 1: FP64).  With programmatic
+   dependent launch each hot kernel lets the next launch in right after its
+   own wait, and before its wait loads what the launch just before cannot
+   write: the SpMV's first slice of A, the sweeps' first batch of L (and the
+   input rows / r where they are older), the update's r, x, p and the p
+   update's p, x for each thread's first two pairs.  The same bits either
+   way.  The 128^3 ABMC mixed solve 21.15 -> 19.95 ms and the 96^3 27-point
+   multicolor one 21.18 -> 19.54 ms; the FP64 fused solve 32.2 -> 33.3 ms, so
+   FP64 storage keeps it off by default. */
 #define ICCG_OPT_TILED 0
 #define ICCG_OPT_SWEEP 1
 #define ICCG_OPT_PDL 2
@@ -279,6 +289,7 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
 #define ICCG_OPT_SPMV_PACK 8
 #define ICCG_OPT_STAGE_ROWS 9
 #define ICCG_OPT_SPMV_TPR 10
+#define ICCG_OPT_EARLY 11
 int iccg_ctx_set_option(iccg_ctx* ctx, int option, long long value);
 
 /* Uploads A_run (the matrix conjugate_gradient runs on, cg_crs.cpp:442-447):

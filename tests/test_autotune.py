@@ -68,12 +68,12 @@ def test_tune_kernels_coordinate_search_leaves_best_options_set():
 
     res = at.tune_kernels(ctx, np.zeros(4), timer=timer)
     assert ctx.opts == {ib.OPT_PERSIST: 1, ib.OPT_SWEEP: 1, ib.OPT_STAGE_BUFS: 1, ib.OPT_STAGE_KB: 112,
-                        ib.OPT_STAGE_ROWS: 256, ib.OPT_PDL: 1, ib.OPT_SPMV_PACK: 1, ib.OPT_SPMV_TPR: 1,
+                        ib.OPT_STAGE_ROWS: 256, ib.OPT_PDL: 1, ib.OPT_EARLY: 1, ib.OPT_SPMV_PACK: 1, ib.OPT_SPMV_TPR: 1,
                         ib.OPT_FUSE_UPDATE: 0, ib.OPT_DEFER_X: 0}
     assert res.choice["persist"] == 1
     assert res.choice["sweep"] == 1 and res.choice["stage_kb"] == 112 and res.choice["pdl"] == 1
     assert abs(res.choice["ms"] - (10.0 - 2.0 - 1.0 - 0.5 - 0.4)) < 1e-12
-    assert len(res.trials) == 2 + 2 + 2 + 4 + 3 + 2 + 2 + 3 + 2 + 2
+    assert len(res.trials) == 2 + 2 + 2 + 4 + 3 + 2 + 3 + 2 + 3 + 2 + 2
 
 
 def test_tune_kernels_skips_unconverged_settings():
@@ -87,3 +87,38 @@ def test_tune_kernels_skips_unconverged_settings():
 
     at.tune_kernels(ctx, np.zeros(4), timer=timer)
     assert ctx.opts[ib.OPT_SWEEP] == 0
+
+
+def test_tune_batch_tunes_one_system_per_class_and_applies_its_choice():
+    mats = [pb.poisson2d(18), pb.poisson2d(20), pb.laplace3d_aniso(7, 1.0), pb.poisson2d(40), pb.laplace3d_aniso(8, 1.0)]
+    keys = [at.batch_class(A) for A in mats]
+    # 2D 5-point: 5 entries per row (rounded); 3D 7-point: 6
+    assert keys[0] == keys[1] == (5, 9) and keys[3] == (5, 11)
+    assert keys[2] == keys[4] and keys[2][0] == 6
+    timed = []
+
+    def timer(P):
+        timed.append((P.A.n, P.name))
+        # 2D: ABMC 16 wins; 3D: multicolor wins
+        best = "abmc16" if P.A.nnz / P.A.n < 6 else "mc"
+        return (1.0 if P.name == best else 2.0), 30, True
+
+    probs, rows = at.tune_batch(mats, timer=timer)
+    assert len(probs) == len(mats) and len(rows) == 3
+    # the largest system of each class is the one timed, once per candidate
+    assert sorted({n for n, _ in timed}) == sorted({mats[1].n, mats[3].n, mats[4].n})
+    assert len(timed) == 3 * len(at.BATCH_ORDERINGS)
+    for A, P, k in zip(mats, probs, keys):
+        assert P.A.n == A.n
+        assert P.variant == ("abmc" if k[0] < 6 else "piccg")
+        if P.variant == "abmc":
+            assert P.info["block_size"] == 16
+    by = {tuple(r["class"]): r for r in rows}
+    assert by[keys[0]]["systems"] == 2 and by[keys[0]]["tuned_on_rows"] == mats[1].n
+    assert by[keys[2]]["choice"] == "mc"
+    # explicit classes, and their length is checked
+    probs2, rows2 = at.tune_batch(mats[:2], classes=["a", "b"], timer=timer)
+    assert len(rows2) == 2
+    import pytest
+    with pytest.raises(ValueError):
+        at.tune_batch(mats, classes=["a"], timer=timer)

@@ -475,6 +475,46 @@ def test_gpu_pdl_launches_give_the_same_bits(which):
     ctx.close()
 
 
+@pytest.mark.parametrize("which", ["abmc_lin", "abmc_bfs", "d27_mc", "mc2d"])
+def test_gpu_early_loads_give_the_same_bits(which):
+    """Loads before the wait on the previous launch (ICCG_OPT_EARLY) only
+    move reads of data that launch cannot write ahead of the wait: solves
+    (FP64 and mixed, with the fused update and deferred x as well) and
+    applies are identical with them off, on for FP32 storage (the default)
+    and on for both storages, over several solves in a row."""
+    P = {"abmc_lin": lambda: pb.config_abmc_aniso(40, 16, "linear"),
+         "abmc_bfs": lambda: pb.config_abmc_aniso(40, 16, "bfs"),
+         "d27_mc": lambda: pb.config_diffusion27(24, "piccg"),
+         "mc2d": lambda: pb.config_small_mc(100, seed=1)}[which]()
+    ctx = _ctx_for(P.A_run, P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    r = ib.gen_uniform(P.A_run.n, 37)
+    out = {}
+    for early in (0, 1, 3):
+        ctx.set_option(ib.OPT_EARLY, early)
+        res = []
+        for opt in (None, ib.OPT_FUSE_UPDATE, ib.OPT_DEFER_X):
+            if opt is not None:
+                ctx.set_option(opt, 1)
+            for st, cap, rri in ((ib.STORE_FP64, 10000, 50), (ib.STORE_FP32, 10000, 50), (ib.STORE_FP32, 10000, 7),
+                                 (ib.STORE_FP64, 9, 50)):
+                for _ in range(2):
+                    x = np.zeros(P.A_run.n)
+                    rr = ctx.solve(P.b_run, x, cap, 1e-8, storage=st, rr_interval=rri)
+                    res.append((x, rr.iters, rr.status, rr.n_replacements))
+            if opt is not None:
+                ctx.set_option(opt, 0)
+        for st in (ib.STORE_FP64, ib.STORE_FP32):
+            res.append((ctx.apply(r, st), 0, "", 0))
+        out[early] = res
+    ctx.set_option(ib.OPT_EARLY, 1)
+    for e in (1, 3):
+        for a, b in zip(out[e], out[0]):
+            assert np.array_equal(a[0], b[0])
+            assert a[1:] == b[1:]
+    ctx.close()
+
+
 @pytest.mark.parametrize("which", ["abmc_lin", "d27_mc", "d27_abmc8"])
 def test_gpu_stage_budget_keeps_fp64_bits(which):
     """The staged kernel's batch budget (ICCG_OPT_STAGE_KB) only changes how
