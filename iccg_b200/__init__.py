@@ -61,6 +61,7 @@ OPT_SPMV_PACK = 8
 OPT_STAGE_ROWS = 9
 OPT_SPMV_TPR = 10
 OPT_EARLY = 11
+OPT_UPDATE_CHAIN = 12
 STATUS_NAMES = {0: "converged", 1: "breakdown", 2: "max_iter", 3: "nonfinite"}
 
 

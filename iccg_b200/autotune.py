@@ -41,7 +41,7 @@ from typing import Callable, Dict, Hashable, List, Optional, Sequence, Tuple
 
 import numpy as np
 
-from . import (CRS, MODE_FUSED, OPT_DEFER_X, OPT_EARLY, OPT_FUSE_UPDATE, OPT_PDL, OPT_PERSIST, OPT_SPMV_PACK, OPT_STAGE_BUFS,
+from . import (CRS, MODE_FUSED, OPT_DEFER_X, OPT_EARLY, OPT_FUSE_UPDATE, OPT_PDL, OPT_UPDATE_CHAIN, OPT_PERSIST, OPT_SPMV_PACK, OPT_STAGE_BUFS,
                OPT_SPMV_TPR, OPT_STAGE_KB, OPT_STAGE_ROWS, OPT_SWEEP, PRECOND_IC0,
                STORE_FP32, Context)
 from .problems import Problem, make
@@ -71,10 +71,12 @@ KERNEL_OPTIONS: Tuple[Tuple[int, Tuple[int, ...]], ...] = (
     (OPT_SPMV_TPR, (1, 2, 4)),
     (OPT_FUSE_UPDATE, (0, 1)),
     (OPT_DEFER_X, (0, 1)),
+    (OPT_UPDATE_CHAIN, (0, 1)),
 )
 OPTION_NAMES = {OPT_PERSIST: "persist", OPT_SWEEP: "sweep", OPT_STAGE_BUFS: "stage_bufs", OPT_STAGE_KB: "stage_kb",
                 OPT_PDL: "pdl", OPT_SPMV_PACK: "spmv_pack", OPT_FUSE_UPDATE: "fuse_update", OPT_DEFER_X: "defer_x",
-                OPT_STAGE_ROWS: "stage_rows", OPT_SPMV_TPR: "spmv_tpr", OPT_EARLY: "early"}
+                OPT_STAGE_ROWS: "stage_rows", OPT_SPMV_TPR: "spmv_tpr", OPT_EARLY: "early",
+                OPT_UPDATE_CHAIN: "update_chain"}
 
 
 @dataclass

@@ -284,6 +284,7 @@ struct iccg_ctx {
     bool defer_x = false;     // ICCG_OPT_DEFER_X: x += alpha p with the p update instead of the r update
     bool spmv_pack = true;    // ICCG_OPT_SPMV_PACK: FP32 SpMV reads (value, column) words
     int spmv_tpr = 1;         // ICCG_OPT_SPMV_TPR: threads per row of the FP32 SpMV (1, 2 or 4)
+    bool update_chain = false;  // ICCG_OPT_UPDATE_CHAIN: the update does the first (chain-only) forward level
     int early = 1;            // ICCG_OPT_EARLY: loads before the wait on the previous launch
                               // (bit 0: FP32 storage solves, bit 1: FP64)
     iccg::QSys Q;

@@ -163,6 +163,8 @@ int iccg_ctx_set_option(iccg_ctx* c, int option, long long value)
         } else if (option == ICCG_OPT_SPMV_TPR) {
             if (value != 1 && value != 2 && value != 4) throw Error(ICCG_ERR_ARG, "ICCG_OPT_SPMV_TPR takes 1, 2 or 4");
             c->spmv_tpr = (int)value;
+        } else if (option == ICCG_OPT_UPDATE_CHAIN) {
+            c->update_chain = value != 0;
         } else if (option == ICCG_OPT_EARLY) {
             if (value < 0 || value > 3) throw Error(ICCG_ERR_ARG, "ICCG_OPT_EARLY takes 0 to 3");
             c->early = (int)value;

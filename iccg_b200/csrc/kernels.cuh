@@ -1874,6 +1874,185 @@ __global__ void __launch_bounds__(256) k_sweep_chain(int g0, int g1, const int* 
     if (FIN != FIN_NONE) reduce_finish<1, FIN>(rz, red, st, ticket, slot0 + blockIdx.x, nslots);
 }
 
+// ---------------------------------------------------------------------------
+// The CG update with the first forward level folded in, for a first level
+// that is chain-only (k_sweep_chain's rows: at most one in-unit entry, on
+// the unit's previous step).  One launch does
+//   x += alpha p                       every row (a flat loop over pairs),
+//   r -= alpha Ap                      rows [n0, n) in the flat loop, and the
+//                                      first level's rows [0, n0) in the chains,
+//   y = (r - v y_prev) / d             the first level's chains (warp per group),
+// and reduces r.r over both parts (FIN_UPD).  Each element gets the fused
+// multiply-adds of k_update and k_sweep_chain, so x, r and y keep their
+// bits; the forward sweep then starts at level 1.  The chains run first in
+// each warp: their steps are serial, and the flat loop's loads fill the SM
+// behind them.  `early`: the flat loop's first two pairs of x, p and r
+// (written two or more launches back) and the group words load before the
+// wait on the SpMV.
+// ---------------------------------------------------------------------------
+template <class T, bool EXACT>
+__global__ void __launch_bounds__(256) k_update_chain(int g0, int g1, const int* __restrict__ glen,
+                                                      const int* __restrict__ sl0,
+                                                      const SliceMeta* __restrict__ meta, SellMat M,
+                                                      const T* __restrict__ dg, int n0, int n,
+                                                      const double* __restrict__ p, const double* __restrict__ Ap,
+                                                      double* __restrict__ x, double* __restrict__ r,
+                                                      double* __restrict__ y, SolverState* st, RedBuf red,
+                                                      unsigned int* ticket, int early)
+{
+    constexpr int CH = 4;
+    const T* __restrict__ val = (const T*)M.val;
+    const int lane = threadIdx.x & 31;
+    acc2 a[1] = {{0.0, 0.0}};
+    const int n2 = n >> 1;
+    const int stride = gridDim.x * blockDim.x;
+    const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const double2* __restrict__ p2 = reinterpret_cast<const double2*>(p);
+    const double2* __restrict__ q2 = reinterpret_cast<const double2*>(Ap);
+    double2* __restrict__ x2 = reinterpret_cast<double2*>(x);
+    double2* __restrict__ r2 = reinterpret_cast<double2*>(r);
+    const int wg = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nwg = (int)((gridDim.x * blockDim.x) >> 5);
+    int g = g0 + wg;
+    int len = 0, my_q = 0, my_p = 0, my_w = 0;
+    auto group = [&](int gg) {
+        len = glen[(size_t)gg * 32];
+        const int sb = sl0[gg];
+        const SliceMeta mine = lane < len ? meta[sb + lane] : SliceMeta{0, 0, 0, 0};
+        my_q = mine.q0;
+        my_p = mine.pS;
+        my_w = (mine.w >> 12) & 255;
+    };
+    // the pair's r update: whole (both rows >= n0), second row only, or none
+    auto rmask = [&](int i) { return (2 * i >= n0 ? 1 : 0) + (2 * i + 1 >= n0 ? 1 : 0); };
+    double2 pre[2][3];
+    if (early) {
+        if (g < g1) group(g);
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int ik = i0 + k * stride;
+            if (ik < n2) {
+                pre[k][0] = __ldcg(p2 + ik);
+                pre[k][1] = __ldcg(x2 + ik);
+                if (rmask(ik)) pre[k][2] = __ldcg(r2 + ik);
+            }
+        }
+        grid_dep_begin();
+        grid_dep_trigger();
+    } else {
+        grid_dep_begin();
+        if (g < g1) group(g);
+    }
+    if (st_done(st)) return;
+    const double alpha = st->alpha;
+
+    // x for every row, r for the rows from n0 on (k_update's pairs)
+    auto pair = [&](int i, int k) {
+        double2 pv, xv;
+        if (k < 0) {
+            pv = p2[i];
+            xv = x2[i];
+        } else {
+            pv = pre[k][0];
+            xv = pre[k][1];
+        }
+        xv.x = fma(alpha, pv.x, xv.x);
+        xv.y = fma(alpha, pv.y, xv.y);
+        x2[i] = xv;
+        const int m = rmask(i);
+        if (m == 2) {
+            const double2 qv = q2[i];
+            double2 rv = k < 0 ? r2[i] : pre[k][2];
+            rv.x = fma(-alpha, qv.x, rv.x);
+            rv.y = fma(-alpha, qv.y, rv.y);
+            r2[i] = rv;
+            acc2_fma(a[0], rv.x, rv.x);
+            acc2_fma(a[0], rv.y, rv.y);
+        } else if (m == 1) {
+            const int e = 2 * i + 1;
+            const double rk = fma(-alpha, Ap[e], r[e]);
+            r[e] = rk;
+            acc2_fma(a[0], rk, rk);
+        }
+    };
+    // the pairs loaded before the wait go first (their registers are then
+    // free for the chains)
+    int i = i0;
+    if (early) {
+        if (i + stride < n2) {
+            pair(i, 0);
+            pair(i + stride, 1);
+            i += 2 * stride;
+        } else if (i < n2) {
+            pair(i, 0);
+            i = n2;
+        }
+    }
+    // the first level's chains: r of the row, then the row of y
+    struct Chunk {
+        double r[CH], q[CH];
+        T v[CH], d[CH];
+        int L[CH], row[CH];
+    };
+    auto load = [&](int t0, Chunk& C) {
+#pragma unroll
+        for (int u = 0; u < CH; ++u) {
+            const int t = t0 + u;
+            const bool ok = t < len;
+            const int rs = ok ? t : 0;
+            const int q = __shfl_sync(0xffffffffu, my_q, rs) + lane;
+            const int pp = __shfl_sync(0xffffffffu, my_p, rs) + lane;
+            const int w = __shfl_sync(0xffffffffu, my_w, rs);
+            C.row[u] = q;
+            C.r[u] = ok ? r[q] : 0.0;
+            C.q[u] = ok ? Ap[q] : 0.0;
+            C.d[u] = ok ? dg[q] : (T)1;
+            C.L[u] = ok ? M.len[q] & 0xffff : 0;
+            C.v[u] = (ok && w > 0) ? val[pp] : (T)0;
+        }
+    };
+    for (bool first = true; g < g1; g += nwg, first = false) {
+        if (!first) group(g);
+        Chunk A, B;
+        load(0, A);
+        double last = 0.0;
+        for (int t0 = 0; t0 < len; t0 += CH) {
+            if (t0 + CH < len) load(t0 + CH, B);
+#pragma unroll
+            for (int u = 0; u < CH; ++u) {
+                if (t0 + u < len) {
+                    double rn = fma(-alpha, A.q[u], A.r[u]);
+                    r[A.row[u]] = rn;
+                    acc2_fma(a[0], rn, rn);
+                    const double xx = fma(-(double)A.v[u], last, rn);
+                    rn = A.L[u] ? xx : rn;
+                    const double v = EXACT ? rn / (double)A.d[u] : rn * (double)A.d[u];
+                    y[A.row[u]] = v;
+                    last = v;
+                }
+            }
+            A = B;
+        }
+    }
+
+    for (; i + stride < n2; i += 2 * stride) {
+        pair(i, -1);
+        pair(i + stride, -1);
+    }
+    if (i < n2) pair(i, -1);
+    if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        const int k = n - 1;
+        x[k] = fma(alpha, p[k], x[k]);
+        if (k >= n0) {
+            const double rk = fma(-alpha, Ap[k], r[k]);
+            r[k] = rk;
+            acc2_fma(a[0], rk, rk);
+        }
+    }
+    if (!early) grid_dep_trigger();
+    reduce_finish<1, FIN_UPD>(a, red, st, ticket, blockIdx.x, gridDim.x);
+}
+
 // out[q] = in[perm[q]] (gather into Q order) / out[perm[q]] = in[q] (scatter)
 __global__ void __launch_bounds__(256) k_gather_vec(int n, const int* __restrict__ perm,
                                                     const double* __restrict__ in, double* __restrict__ out)

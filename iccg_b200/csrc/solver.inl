@@ -125,6 +125,10 @@ static void launch_sweep_level(iccg_ctx* c, int l, const SweepLevel& sl, const d
                rdot, slot0, nslots, st, red, c->ticket.get(), U, early);
         break;
     case 1: {
+        // a staged level of fewer than two CTAs per SM runs without loads
+        // before the wait: with them the 96^3 27-point ABMC B=16 solve, whose
+        // levels hold about one 512-row batch per SM, went 50.1 -> 58.7 ms
+        if (sl.grid < 2 * c->nsm) early = 0;
         const int slots = FWD ? Q.st_slotsS[l_] : Q.st_slotsT[l_];
         const int nbuf = (c->stage_bufs == 1 || Q.st_one[l_]) ? 1 : 2;
         // the fused update stages Ap in the area of the backward sweep's r
@@ -188,8 +192,11 @@ static bool fused_update_ok(iccg_ctx* c)
 // Ap of their rows (U; x += alpha p waits for the p update) and reduce r.r
 // over all their launches (FIN_UPDX at the last CTA of the last forward
 // level).
+// f0 = 1: the first forward level was done by the update (k_update_chain),
+// which also wrote r; the forward sweep starts at level 1.
 template <class T, int FIN, bool UPD = false>
-static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, SolverState* st, UpdArgs U = UpdArgs{})
+static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, SolverState* st, UpdArgs U = UpdArgs{},
+                        int f0 = 0)
 {
     QSys& Q = c->Q;
     if (!UPD && use_persist(c, std::is_same<T, float>::value ? ICCG_STORE_FP32 : ICCG_STORE_FP64)) {
@@ -209,11 +216,11 @@ static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, Solv
             s0 += fl[(size_t)l].grid;
         }
     } else {
-        // level 0's r may come from the launch just before (the update or a
-        // residual); the later levels' r does not
-        for (int l = 0; l < Q.nlevels; ++l)
+        // the first level's r may come from the launch just before (the
+        // update or a residual); the later levels' r does not
+        for (int l = f0; l < Q.nlevels; ++l)
             launch_sweep_level<T, FIN_NONE, true>(c, l, sweep_level<T>(c, l, true), r, y, nullptr, 0, 0, st,
-                                                  UpdArgs{}, l > 0 ? SP_IN : 0);
+                                                  UpdArgs{}, l > f0 ? SP_IN : 0);
     }
     std::vector<SweepLevel> bl((size_t)Q.nlevels);
     int nslots = 0;
@@ -224,9 +231,10 @@ static void apply_ic0_q(iccg_ctx* c, const double* r, double* y, double* z, Solv
     int slot0 = 0;
     // the backward level l reads the y rows the forward level l wrote (and,
     // with the fused update, its r rows): the launch just before only for
-    // the last level; without the fused update r is older
+    // the last level; without the fused update r is older, unless no
+    // forward level ran after the update
     for (int l = Q.nlevels - 1; l >= 0; --l) {
-        const int early = l < Q.nlevels - 1 ? SP_IN | SP_RD : UPD ? 0 : SP_RD;
+        const int early = l < Q.nlevels - 1 ? SP_IN | SP_RD : (UPD || l < f0) ? 0 : SP_RD;
         launch_sweep_level<T, FIN, false>(c, l, bl[(size_t)l], y, z, r, slot0, nslots, st, UpdArgs{}, early);
         slot0 += bl[(size_t)l].grid;
     }
@@ -395,6 +403,44 @@ static void solve_plain(iccg_ctx* c, const double* b, double* x, int max_iter, d
 // ---------------------------------------------------------------------------
 // fused CG: device-side scalars, iterations replayed as a CUDA graph
 // ---------------------------------------------------------------------------
+
+// true if the update can take the first forward level (ICCG_OPT_UPDATE_CHAIN):
+// IC(0) in Q order whose first forward level runs on the chain-only kernel,
+// the plain update path (no persistent apply, fused update or deferred x) and
+// 16-byte aligned vectors
+template <class T>
+static bool update_chain_ok(iccg_ctx* c, const double* x)
+{
+    if (!c->update_chain || !c->use_q || c->pc_kind != ICCG_PRECOND_IC0 || c->fuse_update || c->defer_x) return false;
+    if (c->Q.nlevels < 1 || use_persist(c, std::is_same<T, float>::value ? ICCG_STORE_FP32 : ICCG_STORE_FP64))
+        return false;
+    if (sweep_level<T>(c, 0, true).kind != 0) return false;
+    const uintptr_t a = (uintptr_t)x | (uintptr_t)c->vp.get() | (uintptr_t)c->vAp.get() | (uintptr_t)c->vr.get();
+    return (a & 15) == 0;
+}
+
+template <class T>
+static void update_chain(iccg_ctx* c, double* x, SolverState* st)
+{
+    QSys& Q = c->Q;
+    constexpr bool f32 = std::is_same<T, float>::value;
+    constexpr bool exact = !f32;
+    auto kern = k_update_chain<T, exact>;
+    int per = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kThreads, 0));
+    const int groups = Q.level_g[1] - Q.level_g[0];
+    // a full wave; the chains want one warp per group
+    int grid = std::max(1, per) * c->nsm;
+    grid = std::max(grid, std::min((groups + 7) / 8, 8 * c->nsm));
+    grid = std::min(grid, (int)c->partial_slots);
+    const int n0 = Q.h_gbase[(size_t)Q.level_g[1]];
+    const T* dg = f32 ? (const T*)(const void*)Q.r32.get() : (const T*)(const void*)Q.d64.get();
+    RedBuf red{c->partials.get(), c->scalars.get()};
+    launch(c, 3, kern, grid, kThreads, Q.level_g[0], Q.level_g[1], (const int*)Q.glen.get(), (const int*)Q.sl0.get(),
+           (const SliceMeta*)Q.meta.get(), Q.S.view(f32), dg, n0, c->n, (const double*)c->vp.get(),
+           (const double*)c->vAp.get(), x, c->vr.get(), c->vy.get(), st, red, c->ticket.get(),
+           early_on(c, f32 ? ICCG_STORE_FP32 : ICCG_STORE_FP64));
+}
 static void fused_iteration(iccg_ctx* c, int storage, bool rr, const double* b, double* x)
 {
     const int n = c->n;
@@ -418,6 +464,16 @@ static void fused_iteration(iccg_ctx* c, int storage, bool rr, const double* b, 
         else apply_ic0_q<double, FIN_RZ, true>(c, c->vr.get(), c->vy.get(), c->vz.get(), st, U);
         // x += alpha p, then p = z + beta p
         launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st, x,
+                 early_on(c, storage));
+        return;
+    }
+    if (!rr && (f32 ? update_chain_ok<float>(c, x) : update_chain_ok<double>(c, x))) {
+        // the update with the first forward level (chain-only) in its launch
+        if (f32) update_chain<float>(c, x, st);
+        else update_chain<double>(c, x, st);
+        if (f32) apply_ic0_q<float, FIN_RZ>(c, c->vr.get(), c->vy.get(), c->vz.get(), st, UpdArgs{}, 1);
+        else apply_ic0_q<double, FIN_RZ>(c, c->vr.get(), c->vy.get(), c->vz.get(), st, UpdArgs{}, 1);
+        launch_n(c, 3, k_xpay, (long long)c->n, n, 0.0, (const double*)c->vz.get(), c->vp.get(), st, (double*)nullptr,
                  early_on(c, storage));
         return;
     }

@@ -277,7 +277,14 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
    update's p, x for each thread's first two pairs.  The same bits either
    way.  The 128^3 ABMC mixed solve 21.15 -> 19.95 ms and the 96^3 27-point
    multicolor one 21.18 -> 19.54 ms; the FP64 fused solve 32.2 -> 33.3 ms, so
-   FP64 storage keeps it off by default. */
+   FP64 storage keeps it off by default.
+   ICCG_OPT_UPDATE_CHAIN (default 0): where the first forward level is
+   chain-only (every row's one in-unit entry is the previous step of its
+   unit), the CG update kernel also does that level: x += alpha p for every
+   row, r -= alpha Ap, and the level's chains from the new r, in one launch
+   (k_update_chain).  The same bits.  Slower on the systems measured (128^3
+   ABMC mixed 19.91 -> 20.39 ms, FP64 32.00 -> 32.38; 96^3 27-point
+   multicolor mixed 19.56 -> 19.72), so off by default; the tuner tries it. */
 #define ICCG_OPT_TILED 0
 #define ICCG_OPT_SWEEP 1
 #define ICCG_OPT_PDL 2
@@ -290,6 +297,7 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
 #define ICCG_OPT_STAGE_ROWS 9
 #define ICCG_OPT_SPMV_TPR 10
 #define ICCG_OPT_EARLY 11
+#define ICCG_OPT_UPDATE_CHAIN 12
 int iccg_ctx_set_option(iccg_ctx* ctx, int option, long long value);
 
 /* Uploads A_run (the matrix conjugate_gradient runs on, cg_crs.cpp:442-447):

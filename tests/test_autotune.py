@@ -69,11 +69,11 @@ def test_tune_kernels_coordinate_search_leaves_best_options_set():
     res = at.tune_kernels(ctx, np.zeros(4), timer=timer)
     assert ctx.opts == {ib.OPT_PERSIST: 1, ib.OPT_SWEEP: 1, ib.OPT_STAGE_BUFS: 1, ib.OPT_STAGE_KB: 112,
                         ib.OPT_STAGE_ROWS: 256, ib.OPT_PDL: 1, ib.OPT_EARLY: 1, ib.OPT_SPMV_PACK: 1, ib.OPT_SPMV_TPR: 1,
-                        ib.OPT_FUSE_UPDATE: 0, ib.OPT_DEFER_X: 0}
+                        ib.OPT_FUSE_UPDATE: 0, ib.OPT_DEFER_X: 0, ib.OPT_UPDATE_CHAIN: 0}
     assert res.choice["persist"] == 1
     assert res.choice["sweep"] == 1 and res.choice["stage_kb"] == 112 and res.choice["pdl"] == 1
     assert abs(res.choice["ms"] - (10.0 - 2.0 - 1.0 - 0.5 - 0.4)) < 1e-12
-    assert len(res.trials) == 2 + 2 + 2 + 4 + 3 + 2 + 3 + 2 + 3 + 2 + 2
+    assert len(res.trials) == 2 + 2 + 2 + 4 + 3 + 2 + 3 + 2 + 3 + 2 + 2 + 2
 
 
 def test_tune_kernels_skips_unconverged_settings():

@@ -515,6 +515,41 @@ def test_gpu_early_loads_give_the_same_bits(which):
     ctx.close()
 
 
+@pytest.mark.parametrize("which", ["abmc_lin", "abmc_bfs", "d27_mc", "mc2d", "knn_abmc"])
+def test_gpu_update_chain_gives_the_same_bits(which):
+    """The update with the first (chain-only) forward level in its launch
+    (ICCG_OPT_UPDATE_CHAIN) does each element's fused multiply-adds of the
+    update and the chain-only sweep: solves keep their bits, iterations and
+    statuses in FP64 and mixed storage, with replacement, iteration caps and
+    early loads on and off.  (Systems whose first level is not chain-only
+    take the usual path.)"""
+    P = {"abmc_lin": lambda: pb.config_abmc_aniso(40, 16, "linear"),
+         "abmc_bfs": lambda: pb.config_abmc_aniso(40, 16, "bfs"),
+         "d27_mc": lambda: pb.config_diffusion27(24, "piccg"),
+         "mc2d": lambda: pb.config_small_mc(100, seed=1),
+         "knn_abmc": lambda: pb.config_knn(8000, seed=5, block_size=16)}[which]()
+    ctx = _ctx_for(P.A_run, P.sched)
+    ctx.build(ib.PRECOND_IC0, 0.0)
+    out = {}
+    for uc in (1, 0):
+        ctx.set_option(ib.OPT_UPDATE_CHAIN, uc)
+        res = []
+        for early in (1, 3):
+            ctx.set_option(ib.OPT_EARLY, early)
+            for st, cap, rri in ((ib.STORE_FP64, 10000, 50), (ib.STORE_FP32, 10000, 50), (ib.STORE_FP32, 10000, 7),
+                                 (ib.STORE_FP64, 9, 50)):
+                x = np.zeros(P.A_run.n)
+                rr = ctx.solve(P.b_run, x, cap, 1e-8, storage=st, rr_interval=rri)
+                res.append((x, rr.iters, rr.status, rr.n_replacements, rr.true_rel_resid))
+        out[uc] = res
+    ctx.set_option(ib.OPT_UPDATE_CHAIN, 0)
+    ctx.set_option(ib.OPT_EARLY, 1)
+    for a, b in zip(out[1], out[0]):
+        assert np.array_equal(a[0], b[0])
+        assert a[1:] == b[1:]
+    ctx.close()
+
+
 @pytest.mark.parametrize("which", ["abmc_lin", "d27_mc", "d27_abmc8"])
 def test_gpu_stage_budget_keeps_fp64_bits(which):
     """The staged kernel's batch budget (ICCG_OPT_STAGE_KB) only changes how
