@@ -715,9 +715,10 @@ def batched_case(count: int, nrhs: int = 4, steps: int = 3, warmup: int = 1, dev
     rhs = [[pb.with_rhs(P, seed=1000 * i + k).b_run.copy() for k in range(nrhs)] for i, P in enumerate(probs)]
     host_s = time.perf_counter() - t0
     t0 = time.perf_counter()
+    import iccg_b200.batch as bt
     ctxs = []
     for P in probs:
-        c = ib.Context(device)
+        c = bt.batch_context(device)
         c.upload(P.A_run)
         c.set_schedule(P.sched)
         c.build(ib.PRECOND_IC0, 0.0)
