@@ -139,8 +139,24 @@ __global__ void __launch_bounds__(kThreadsB) k_bat_spmv(const BItem* __restrict_
             if (i < S.n) {
                 const int L = A.len[i];
                 const int p0 = A.ptr[s] + lane;
+                // the row's first K entries: every column and value load,
+                // then every gather, in flight before the sum (in CSR
+                // order, as k_spmv_q)
+                constexpr int K = 8;
+                int c[K];
+                double v[K], xv[K];
+#pragma unroll
+                for (int j = 0; j < K; ++j) {
+                    c[j] = j < L ? __ldg(A.col + p0 + 32 * j) : 0;
+                    v[j] = j < L ? (double)__ldg(val + p0 + 32 * j) : 0.0;
+                }
+#pragma unroll
+                for (int j = 0; j < K; ++j) xv[j] = j < L ? __ldg(S.p + c[j]) : 0.0;
                 double sum = 0.0;
-                for (int j = 0; j < L; ++j) {
+#pragma unroll
+                for (int j = 0; j < K; ++j)
+                    if (j < L) sum = sum + v[j] * xv[j];
+                for (int j = K; j < L; ++j) {
                     const int pa = p0 + 32 * j;
                     sum = sum + (double)__ldg(val + pa) * __ldg(S.p + __ldg(A.col + pa));
                 }
