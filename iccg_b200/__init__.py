@@ -590,7 +590,7 @@ class Context:
 
     def solve(self, b: np.ndarray, x: np.ndarray, max_iter: int = 10000, tol: float = 1e-8,
               mode: int = MODE_FUSED, storage: int = STORE_FP64, rr_interval: int = 50,
-              graph_iters: int = 8) -> CGResult:
+              graph_iters: int = 16) -> CGResult:
         """conjugate_gradient on the uploaded A_run; x (float64, in/out)."""
         b = _f64(b)
         if x.dtype != np.float64 or not x.flags.c_contiguous:
@@ -602,7 +602,7 @@ class Context:
 
     def solve_dev(self, b_ptr: int, x_ptr: int, max_iter: int = 10000, tol: float = 1e-8,
                   mode: int = MODE_FUSED, storage: int = STORE_FP64, rr_interval: int = 50,
-                  graph_iters: int = 8) -> CGResult:
+                  graph_iters: int = 16) -> CGResult:
         """Same with device pointers (e.g. torch tensors' data_ptr())."""
         opts = _Opts(mode, storage, rr_interval, graph_iters)
         res = _Result()

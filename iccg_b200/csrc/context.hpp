@@ -233,6 +233,11 @@ struct QSys {
 // What a captured iteration graph was recorded for: a graph is replayed
 // only for a solve whose key equals it field by field (the graphs bake in
 // the system, its kernels and the x / b device pointers).
+// iterations per graph launch of a single-system solve when the caller does
+// not choose: the 128^3 mixed solve took 20.10 / 19.92 / 19.80 / 19.79 ms
+// with 4 / 8 / 16 / 32 (the replay loop shrinks the last graphs to 4, 2, 1)
+constexpr int kGraphIters = 16;
+
 struct GraphKey {
     int sched_version = -1, factor_version = -1, storage = -1, rri = -1, use_q = -1, m = -1, pc_kind = -1,
         sweep_kernel = -1;

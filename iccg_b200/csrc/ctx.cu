@@ -597,7 +597,7 @@ int iccg_batch_solve(iccg_batch* B, int nsolve, const int* system, const double*
         for (int s = 0; s < nsolve; ++s)
             if (!b[s] || !x[s]) throw Error(ICCG_ERR_ARG, "null right-hand side or solution");
         if (B->sys.empty()) throw Error(ICCG_ERR_STATE, "the batch holds no system");
-        iccg_solve_opts o{ICCG_MODE_FUSED, ICCG_STORE_FP64, 50, 8};
+        iccg_solve_opts o{ICCG_MODE_FUSED, ICCG_STORE_FP64, 50, kGraphIters};
         if (opts) o = *opts;
         if (o.storage == ICCG_STORE_FP32) bat::run<float>(B, nsolve, system, b, x, max_iter, tol, o, res);
         else bat::run<double>(B, nsolve, system, b, x, max_iter, tol, o, res);
@@ -607,7 +607,7 @@ int iccg_batch_solve(iccg_batch* B, int nsolve, const int* system, const double*
 int iccg_batch_open(iccg_batch* B, int slots, const iccg_solve_opts* opts)
 {
     return bguard(B, [&] {
-        iccg_solve_opts o{ICCG_MODE_FUSED, ICCG_STORE_FP64, 50, 8};
+        iccg_solve_opts o{ICCG_MODE_FUSED, ICCG_STORE_FP64, 50, kGraphIters};
         if (opts) o = *opts;
         bat::open_session(B, slots, o);
     });

@@ -1255,14 +1255,20 @@ __device__ __forceinline__ void cp_async_wait()
 // Copies elements [first, first + count) of src (esize bytes each) into dst
 // in 16-byte chunks, starting at the chunk that holds `first`; returns the
 // element offset of `first` in dst.
-__device__ __forceinline__ int stage_range(unsigned char* dst, const void* src, int esize, int first, int count)
+// Threads tid = 0 .. nthr - 1 of the CTA share the copy (by default all).
+__device__ __forceinline__ int stage_range(unsigned char* dst, const void* src, int esize, int first, int count,
+                                           int tid = -1, int nthr = 0)
 {
+    if (tid < 0) {
+        tid = threadIdx.x;
+        nthr = blockDim.x;
+    }
     const int per = 16 / esize;
     const int a0 = first & ~(per - 1);
     const int a1 = (first + count + per - 1) & ~(per - 1);
     const int chunks = (a1 - a0) / per;
     const unsigned char* s = (const unsigned char*)src + (size_t)a0 * esize;
-    for (int k = threadIdx.x; k < chunks; k += blockDim.x) cp_async16(dst + 16 * k, s + 16 * k);
+    for (int k = tid; k < chunks; k += nthr) cp_async16(dst + 16 * k, s + 16 * k);
     return first - a0;
 }
 
@@ -1274,22 +1280,31 @@ enum StagePart { SP_MAT = 1, SP_IN = 2, SP_RD = 4, SP_ALL = 7, SP_EARLY = 8 };
 // fused update writes them into the tile itself).  `parts` selects what is
 // copied; COMMIT closes the copy group (a batch staged in two calls commits
 // with the second).
+// SP_MAT split in two: SP_GEO, the row words, columns and values, which a
+// regular chain phase does not read, and SP_HEAD, the slice words and
+// pivots, which it does (with the inputs, r and the packed in-unit words).
+constexpr int SP_GEO = 16;
+constexpr int SP_HEAD = 32;
+
 template <class T, bool FWD, bool WITH_R, bool STAGE_IN = true, bool COMMIT = true>
 __device__ __forceinline__ void stage_batch(unsigned char* base, const StageLayout& Ly, const BatchDesc& d,
                                             const SliceMeta* meta, const SellMat& M, const T* dg,
-                                            const double* in, const double* rdot, int parts = SP_ALL)
+                                            const double* in, const double* rdot, int parts = SP_ALL,
+                                            int tid = -1, int nthr = 0)
 {
     const int rows = d.qe - d.qb;
     const int p0 = FWD ? d.ps0 : d.pt0, p1 = FWD ? d.ps1 : d.pt1;
-    if (parts & SP_MAT) {
-        stage_range(base + Ly.meta, meta, 16, d.sb, d.se - d.sb);
-        stage_range(base + Ly.piv, dg, (int)sizeof(T), d.qb, rows);
-        stage_range(base + Ly.len, M.len, 4, d.qb, rows);
-        stage_range(base + Ly.col, M.col, 4, p0, p1 - p0);
-        stage_range(base + Ly.val, M.val, (int)sizeof(T), p0, p1 - p0);
+    if (parts & (SP_MAT | SP_HEAD)) {
+        stage_range(base + Ly.meta, meta, 16, d.sb, d.se - d.sb, tid, nthr);
+        stage_range(base + Ly.piv, dg, (int)sizeof(T), d.qb, rows, tid, nthr);
     }
-    if (STAGE_IN && (parts & SP_IN)) stage_range(base + Ly.in, in, 8, d.qb, rows);
-    if (WITH_R && (parts & SP_RD)) stage_range(base + Ly.rd, rdot, 8, d.qb, rows);
+    if (parts & (SP_MAT | SP_GEO)) {
+        stage_range(base + Ly.len, M.len, 4, d.qb, rows, tid, nthr);
+        stage_range(base + Ly.col, M.col, 4, p0, p1 - p0, tid, nthr);
+        stage_range(base + Ly.val, M.val, (int)sizeof(T), p0, p1 - p0, tid, nthr);
+    }
+    if (STAGE_IN && (parts & SP_IN)) stage_range(base + Ly.in, in, 8, d.qb, rows, tid, nthr);
+    if (WITH_R && (parts & SP_RD)) stage_range(base + Ly.rd, rdot, 8, d.qb, rows, tid, nthr);
     if (COMMIT) cp_async_commit();
 }
 
@@ -1744,10 +1759,24 @@ __global__ void __launch_bounds__(256) k_sweep_st(int b0, int b1, const BatchDes
             st_gather<T, FWD, EXACT, false>(cur, base, Ly, rows_cap, prev);
             __syncthreads();
 
+            // backward, single buffer, regular chain: the warps with no group
+            // to chain copy the next batch's row words, columns and values
+            // (read only by the gather) while the chains run.  (Not forward:
+            // there it took the FP32 kernel from 48 to 60 registers, 5 to 4
+            // CTAs per SM.)
+            constexpr bool ext_first = FWD || !EXACT;
+            const int busy = cur.ng < 8 ? cur.ng : 8;
+            const bool geo = !FWD && NB == 1 && !UPD && ext_first && has_next && busy < 8 && (cur.flags & 2);
+            if (geo && warp >= busy) {
+                stage_batch<T, FWD, with_r || UPD>(smem_st, Ly, nxt, meta, M, dg, in, stage2, SP_GEO,
+                                                   (int)threadIdx.x - 32 * busy, (int)blockDim.x - 32 * busy);
+            }
             st_chain<T, FWD, EXACT, with_r>(cur, base, Ly, rows_cap, gl, gs, out, rz[0]);
             __syncthreads();
             if (!has_next) break;
-            if (NB == 1) stage_batch<T, FWD, with_r || UPD>(smem_st, Ly, nxt, meta, M, dg, in, stage2);
+            if (NB == 1)
+                stage_batch<T, FWD, with_r || UPD>(smem_st, Ly, nxt, meta, M, dg, in, stage2,
+                                                   geo ? SP_HEAD | SP_IN | SP_RD : SP_ALL);
             b += gridDim.x;
             cur = nxt;
             nxt = nn;

@@ -689,9 +689,9 @@ static void solve_dev(iccg_ctx* c, const double* b, double* x, int max_iter, dou
                       iccg_result* res)
 {
     require_precond(c);
-    iccg_solve_opts o{ICCG_MODE_FUSED, ICCG_STORE_FP64, 50, 8};
+    iccg_solve_opts o{ICCG_MODE_FUSED, ICCG_STORE_FP64, 50, kGraphIters};
     if (opts) o = *opts;
-    if (o.graph_iters <= 0) o.graph_iters = 8;
+    if (o.graph_iters <= 0) o.graph_iters = kGraphIters;
     if (o.mode == ICCG_MODE_PLAIN && o.storage != ICCG_STORE_FP64)
         throw Error(ICCG_ERR_ARG, "the plain path computes in FP64 storage only");
     std::memset(res, 0, sizeof(*res));

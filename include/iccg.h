@@ -69,7 +69,7 @@ typedef struct {
     int storage;       /* ICCG_STORE_FP64 or ICCG_STORE_FP32                  */
     int rr_interval;   /* FP64 residual replacement every k iterations
                           (FP32 storage only; 0 = off; default 50)           */
-    int graph_iters;   /* FUSED: iterations per graph launch (default 8)     */
+    int graph_iters;   /* FUSED: iterations per graph launch (default 16)    */
 } iccg_solve_opts;
 
 typedef struct iccg_ctx iccg_ctx;
