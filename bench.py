@@ -173,12 +173,64 @@ def _solve_case(P, device: int, with_plain: bool = True) -> dict:
     return out
 
 
+def serving_case(device: int, requests: int = 48, max_points: float = 1e5, rate: float = 30.0,
+                 builders: int = 16) -> dict:
+    """A short serving stream for the headline line: `requests` kNN-Laplacian
+    solves (N log-uniform in [1e3, max_points]) arriving as a Poisson
+    process at `rate` per second, through the continuous-batching loop
+    (batch.ServingLoop) under the 100 GB budget; solves/s and p50 / p99
+    latency, arrival to result with host set-up included.  Two requests
+    are also solved alone and through a batch session, to check the bits."""
+    import iccg_b200 as ib
+    import iccg_b200.batch as bt
+    import iccg_b200.problems as pb
+    rng = np.random.default_rng(11)
+    sizes = [int(np.exp(rng.uniform(np.log(1e3), np.log(max_points)))) for _ in range(requests)]
+    arr = np.random.default_rng(13)
+    t, reqs = 0.0, []
+    for i, npts in enumerate(sizes):
+        t += arr.exponential(1.0 / rate)
+        reqs.append(bt.Request(i, t, (lambda npts=npts, i=i: pb.config_knn(npts, seed=i)),
+                               bt.estimate_device_bytes(npts, 18 * npts)))
+    loop = bt.ServingLoop(budget_bytes=100 * 10**9, device=device, builders=builders, slots=256, graph_iters=4,
+                          rr_interval=RR)
+    st = bt.serve_sharded(reqs, loop, dist=None)
+    same, plain = True, []
+    B = ib.Batch(device)
+    B.open(1, ib.STORE_FP32, rr_interval=RR, graph_iters=4)
+    for i, npts in enumerate(sizes[:2]):
+        P = pb.config_knn(npts, seed=i)
+        c = bt.batch_context(device)
+        bt.load_system(c, P, ib.STORE_FP32)
+        x = np.zeros(P.A_run.n)
+        r = c.solve(P.b_run, x, 10000, TOL, storage=ib.STORE_FP32, rr_interval=RR, graph_iters=4)
+        k = B.add_system(c)
+        B.submit(k, P.b_run, None, 10000, TOL)
+        while True:
+            stopped, _ = B.step()
+            if stopped:
+                break
+        xb, rb = B.retire(stopped)
+        B.remove_system(k)
+        same = same and np.array_equal(xb[0], x) and rb[0].iters == r.iters
+        xp = np.zeros(P.A_run.n)
+        plain.append(c.solve(P.b_run, xp, 10000, TOL, storage=ib.STORE_FP64, mode=ib.MODE_PLAIN).solve_ms)
+        c.close()
+    B.close()
+    return {"requests": requests, "points": {"min": min(sizes), "max": max(sizes), "distribution": "log-uniform"},
+            "arrival_rate_per_s": rate, "solves_per_s": st.get("solves_per_s"), "p50_ms": st.get("p50_ms"),
+            "p99_ms": st.get("p99_ms"), "failed": st.get("failed"), "mean_iters": st.get("mean_iters"),
+            "peak_device_bytes": (st.get("peak_device_bytes_per_rank") or [None])[0],
+            "plain_fp64_solve_ms_alone": [round(v, 3) for v in plain],
+            "batch_session_same_bits_as_alone": bool(same)}
+
+
 def sub_results(device: int) -> dict:
     """Short results of the other workloads, carried on the headline line:
     C1 the 2D 5-point 128^2 Poisson problem with greedy multicolor IC(0);
     C3 the 27-point variable-coefficient 96^3 problem, multicolor and ABMC
     B=8; the batched engine on 64 of the batched workload's systems x 4
-    right-hand sides."""
+    right-hand sides; a short serving stream (serving_case)."""
     import iccg_b200.problems as pb
     out = {}
     t0 = time.perf_counter()
@@ -187,6 +239,7 @@ def sub_results(device: int) -> dict:
         for key, (v, B) in {"c3_diffusion27_96_mc": ("piccg", 16), "c3_diffusion27_96_abmc8": ("abmc", 8)}.items():
             out[key] = _solve_case(pb.config_diffusion27(96, v, block_size=B, seed=0), device, with_plain=False)
         out["batched_64x4"] = batched_case(64, 4, steps=2, warmup=1, device=device, compare_streams=False, sample=8)
+        out["serving_48"] = serving_case(device)
     except Exception as e:   # the headline number stands; the failure is shown, not hidden
         out["error"] = repr(e)
     out["wall_s"] = round(time.perf_counter() - t0, 1)
