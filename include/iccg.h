@@ -274,7 +274,8 @@ long long iccg_ctx_device_bytes(const iccg_ctx* ctx);
    own wait, and before its wait loads what the launch just before cannot
    write: the SpMV's first slice of A, the sweeps' first batch of L (and the
    input rows / r where they are older), the update's r, x, p and the p
-   update's p, x for each thread's first two pairs.  The same bits either
+   update's p, x for each thread's first two pairs.  Staged sweep levels of
+   fewer than two CTAs per SM run without it.  The same bits either
    way.  The 128^3 ABMC mixed solve 21.15 -> 19.95 ms and the 96^3 27-point
    multicolor one 21.18 -> 19.54 ms; the FP64 fused solve 32.2 -> 33.3 ms, so
    FP64 storage keeps it off by default.
